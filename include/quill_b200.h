@@ -1,0 +1,158 @@
+/*
+ * quill_b200 — B200-native per-timestep particle-in-cell loop of QUILL
+ * (QUILL-PIC/Quill), one GPU, one spatial region (n_sr = 1).
+ *
+ * C ABI of libquill_b200.so.  Plain pointers and sizes only; every call
+ * returns a qp_status and leaves a message for qp_last_error().  One handle
+ * owns one region on one GPU; a handle is not thread-safe.
+ *
+ * The reference has no plugin or FFI: its seam is the C++ object
+ * `spatial_region` (include/main.h:17-170) driven by main() in
+ * src/main.cpp:2319-2432.  Each entry point below cites the member function
+ * or code it replaces.
+ *
+ * Units are the reference's: time in 1/omega, lengths in c/omega, particle
+ * positions in cell units (x = i at node i), momenta u = p/(mc), fields in
+ * m c omega / e.  Field planes are indexed (i, j, k) with k fastest, as
+ * field3d (src/containers.cpp:4-22).
+ */
+#ifndef QUILL_B200_H
+#define QUILL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QP_MAX_SPECIES 8
+
+typedef enum {
+    QP_OK = 0,
+    QP_ERR_CONFIG = 1,   /* bad parameters or input data */
+    QP_ERR_CAPACITY = 2, /* a particle store is full (device append overflow) */
+    QP_ERR_NAN = 3,      /* non-finite particle state detected */
+    QP_ERR_TIMEOUT = 4,  /* a bounded device wait gave up */
+    QP_ERR_CUDA = 5,     /* CUDA runtime error */
+    QP_ERR_STATE = 6,    /* call not valid in the handle's current state */
+    QP_ERR_ARG = 7       /* null pointer or out-of-range argument */
+} qp_status;
+
+/* maxwell_solver_enum, include/containers.h:82-84 */
+typedef enum { QP_SOLVER_FDTD = 0, QP_SOLVER_NDFX = 1, QP_SOLVER_FIVE_POINT = 2 } qp_solver;
+/* pusher_enum, include/containers.h:86-88 */
+typedef enum { QP_PUSHER_VAY = 0, QP_PUSHER_BORIS = 1 } qp_pusher;
+/* FP64: the reference arithmetic.  MIXED: positions as int cell + f32
+ * offset, FP32 push, gather, deposition and stencils; FP64 diagnostics. */
+typedef enum { QP_PREC_FP64 = 0, QP_PREC_MIXED = 1 } qp_precision;
+
+typedef struct {
+    int nx, ny, nz;              /* cells per axis (spatial_region::create_arrays) */
+    double dx, dy, dz, dt;       /* c/omega and 1/omega (spatial_region::init) */
+    double lambda_cm;            /* wavelength in cm: e_s = lambda/2.4263086e-10 (main.cpp:2276)
+                                    and the N / energy normalisations (main.cpp:2324-2327) */
+    int solver;                  /* qp_solver */
+    int pusher;                  /* qp_pusher */
+    int qed;                     /* 0/1: photon emission, Breit-Wheeler pairs, vacuum pairs */
+    int precision;               /* qp_precision */
+    uint64_t seed;               /* counter-based random stream seed (QED) */
+    int n_species;
+    double cmr[QP_MAX_SPECIES];  /* charge/mass: -1 electrons, +1 positrons, 0 photons,
+                                    anything else an ion population (icmr, main.cpp:3251-3330),
+                                    ion populations numbered in table order */
+    int64_t capacity[QP_MAX_SPECIES]; /* particle slots per species (0 = grow on load only) */
+    int device;                  /* CUDA device ordinal */
+} qp_params;
+
+/* Per-step diagnostics: spatial_region::compute_N and compute_energy
+ * (fout.cpp:41-138) with the normalisations of main.cpp:2326-2327. */
+typedef struct {
+    double N_e, N_p, N_ph;               /* weighted counts */
+    int64_t N_qp_e, N_qp_p, N_qp_g;      /* macro-particle counts */
+    double energy_f, energy_e, energy_p, energy_ph; /* Joules */
+    int n_ion;
+    int64_t N_qp_i[QP_MAX_SPECIES];
+    double ienergy[QP_MAX_SPECIES];
+    int64_t n_macro[QP_MAX_SPECIES];     /* live particles per species (table order) */
+    int32_t status;                      /* qp_status raised on the device in this step */
+    int32_t pad_;
+} qp_diag;
+
+typedef struct qp_handle qp_handle;
+
+/* Library version string. */
+const char* qp_version(void);
+
+/* Message of the last failing call on h (or of the last failed qp_create
+ * when h is NULL). */
+const char* qp_last_error(const qp_handle* h);
+
+/* spatial_region::init + create_arrays (low-level.cpp:61-150): allocate the
+ * fields and particle stores of one region on params->device. */
+int qp_create(const qp_params* params, qp_handle** out);
+
+/* ~spatial_region (low-level.cpp:152-184). */
+int qp_destroy(qp_handle* h);
+
+/* Copy E and B from host planes (nx*ny*nz doubles each, k fastest); the
+ * device copy is converted to the handle's precision.  Replaces the field
+ * initialisers writing spatial_region::ce/cb (init.cpp:6-400). */
+int qp_load_fields(qp_handle* h, const double* ex, const double* ey, const double* ez,
+                   const double* bx, const double* by, const double* bz);
+
+/* f_init_boundaries + interpolate_be, called once after loading
+ * (main.cpp:2288-2289, advance.cpp:85-88, maxwell.cpp:135/338/532). */
+int qp_init_boundaries(qp_handle* h);
+
+/* Append n particles of one species from host arrays (cell units; chi may
+ * be NULL).  Within a cell the given order becomes the traversal order;
+ * particles of a later call precede those already in the cell, as head
+ * insertion by spatial_region::place (plist.cpp:22-39) would put them.
+ * Positions must lie in [0, n) per axis.  Replaces new_particle + place
+ * in fill_cell_by_particles (init.cpp:402-478). */
+int qp_load_particles(qp_handle* h, int species, int64_t n, const double* x, const double* y,
+                      const double* z, const double* ux, const double* uy, const double* uz,
+                      const double* g, const double* q, const double* chi);
+
+/* nsteps timesteps, each in the order of main.cpp:2321-2331:
+ *   birth_from_vacuum -> padvance(external_bz) -> compute_N/compute_energy
+ *   -> fadvance.
+ * diag (nullable) receives one record per step. */
+int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag);
+
+/* Diagnostics of the last completed step. */
+int qp_get_diag(qp_handle* h, qp_diag* out);
+
+/* Copy fields to host: 12 planes E(3) B(3) J(3) Bbar(3), FP64. */
+int qp_dump_fields(qp_handle* h, double* out12);
+
+/* Live particle count of one species. */
+int qp_count_particles(qp_handle* h, int species, int64_t* n);
+
+/* Copy one species to host in traversal order (cells lexicographic, list
+ * order inside a cell).  Each pointer may be NULL; cell receives the linear
+ * cell index (i*ny + j)*nz + k.  cap is the capacity of every array. */
+int qp_dump_particles(qp_handle* h, int species, int64_t cap, double* x, double* y, double* z,
+                      double* ux, double* uy, double* uz, double* g, double* q, double* chi,
+                      int64_t* cell);
+
+/* Device-resident snapshot of the full state (fields, particles, random
+ * counters, step) into slot 0..3 / restore from it.  No reference
+ * counterpart (the reference has no checkpointing). */
+int qp_checkpoint(qp_handle* h, int slot);
+int qp_restore(qp_handle* h, int slot);
+
+/* Wait for all work of the handle's stream. */
+int qp_synchronize(qp_handle* h);
+
+/* Run all work of h on the given cudaStream_t (NULL = the handle's own). */
+int qp_set_stream(qp_handle* h, void* cuda_stream);
+
+/* Number of this library's kernel launches issued since the handle was
+ * created (for launch accounting). */
+int qp_launch_count(qp_handle* h, int64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUILL_B200_H */

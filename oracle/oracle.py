@@ -1,0 +1,228 @@
+"""ORACLE / TEST INFRASTRUCTURE — ctypes loader for the CPU checkers.
+
+Two interchangeable back ends with one interface:
+
+* ``kind="ref"``  — the reference's own sources (QUILL src/*.cpp minus
+  main.cpp) compiled with oracle/ref_shim.cpp into oracle/_ref/ by
+  ``make -C oracle ref``;
+* ``kind="port"`` — the plain-C restatement oracle/qp_oracle.c built by
+  ``make -C oracle``.
+
+Each comes in a ``parity`` flavour (-ffp-contract=off: plain IEEE operation
+sequence, comparable bit for bit with the CUDA FP64 path built with
+--fmad=false) and a ``fast`` flavour (Release flags, for CPU timing).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only to check or time against it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+_D = C.c_double
+_DP = C.POINTER(C.c_double)
+_LP = C.POINTER(C.c_long)
+
+
+def lib_path(kind: str = "port", flavour: str = "parity") -> str:
+    if kind == "ref":
+        return os.path.join(HERE, "_ref", f"libquill_ref_{flavour}.so")
+    return os.path.join(HERE, f"liboracle_{flavour}.so")
+
+
+def available(kind: str = "port", flavour: str = "parity") -> bool:
+    return os.path.exists(lib_path(kind, flavour))
+
+
+_LIBS: dict = {}
+
+
+def _load(kind: str, flavour: str):
+    key = (kind, flavour)
+    if key in _LIBS:
+        return _LIBS[key]
+    path = lib_path(kind, flavour)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle{' ref' if kind == 'ref' else ''}`)")
+    lib = C.CDLL(path)
+    p = "qref_" if kind == "ref" else "qor_"
+
+    def fn(name, res, *args):
+        f = getattr(lib, p + name)
+        f.restype = res
+        f.argtypes = list(args)
+        return f
+
+    api = {
+        "create": fn("create", C.c_void_p, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D, _D,
+                     C.c_int, C.c_int, C.c_int, C.c_int, _DP, C.c_int),
+        "destroy": fn("destroy", None, C.c_void_p),
+        "set_fields": fn("set_fields", None, C.c_void_p, _DP, _DP, _DP, _DP, _DP, _DP),
+        "get_fields": fn("get_fields", None, C.c_void_p, _DP),
+        "init_boundaries": fn("init_boundaries", None, C.c_void_p),
+        "add_particles": fn("add_particles", None, C.c_void_p, C.c_long, _DP, _DP, _DP, _DP, _DP,
+                            _DP, _DP, _DP, _DP, _DP),
+        "count_particles": fn("count_particles", C.c_long, C.c_void_p),
+        "get_particles": fn("get_particles", C.c_long, C.c_void_p, C.c_long, _DP, _LP),
+        "diag_len": fn("diag_len", C.c_int, C.c_void_p),
+        "step": fn("step", None, C.c_void_p, C.c_int, _D, _DP),
+        "padvance": fn("padvance", None, C.c_void_p, _D),
+        "fadvance": fn("fadvance", None, C.c_void_p),
+        "compute_diag": fn("compute_diag", None, C.c_void_p, _DP),
+        "push": fn("push", None, C.c_int, _D, _DP, _DP, _DP, _D),
+        "jdeposition": fn("jdeposition", None, C.c_void_p, _DP, _DP, _D),
+        "zero_j": fn("zero_j", None, C.c_void_p),
+        "gather": fn("gather", None, C.c_void_p, _D, _D, _D, _DP, _DP),
+        "chi": fn("chi", _D, C.c_void_p, _DP, _DP, _DP, _D),
+        "w": fn("w", _D, C.c_void_p, _D, _DP, _D),
+        "tilde_w": fn("tilde_w", _D, C.c_void_p, _D, _D, _D),
+        "mathcal_W": fn("mathcal_W", _D, C.c_void_p, _DP, _DP),
+        "get_rand": fn("get_rand", _D, C.c_void_p),
+    }
+    _LIBS[key] = api
+    return api
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+PARTICLE_KEYS = ("x", "y", "z", "ux", "uy", "uz", "g", "q", "cmr", "chi")
+FIELD_KEYS = ("ex", "ey", "ez", "bx", "by", "bz", "jx", "jy", "jz", "bex", "bey", "bez")
+
+
+class Region:
+    """One simulation region on the CPU checker (reference or restatement)."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, dt, *, lambda_cm=1e-4, solver=0, pusher=1,
+                 qed=False, icmr=(), seed=0, kind="port", flavour="parity"):
+        self.api = _load(kind, flavour)
+        self.kind = kind
+        self.shape = (nx, ny, nz)
+        self.dx, self.dy, self.dz, self.dt = dx, dy, dz, dt
+        ic = np.ascontiguousarray(np.asarray(icmr, dtype=np.float64).reshape(-1))
+        if ic.size == 0:
+            ic = np.zeros(1)
+            n_ion = 0
+        else:
+            n_ion = ic.size
+        self._icmr = ic
+        self.h = self.api["create"](nx, ny, nz, dx, dy, dz, dt, lambda_cm, solver, pusher,
+                                    int(bool(qed)), n_ion, _dp(ic), int(seed))
+
+    def close(self):
+        if self.h:
+            self.api["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nc(self):
+        nx, ny, nz = self.shape
+        return nx * ny * nz
+
+    def set_fields(self, ex, ey, ez, bx, by, bz):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (ex, ey, ez, bx, by, bz)]
+        self.api["set_fields"](self.h, *[_dp(a) for a in arrs])
+
+    def get_fields(self) -> np.ndarray:
+        out = np.empty((12,) + self.shape, dtype=np.float64)
+        self.api["get_fields"](self.h, _dp(out))
+        return out
+
+    def init_boundaries(self):
+        self.api["init_boundaries"](self.h)
+
+    def add_particles(self, parts: dict):
+        n = len(parts["x"])
+        arrs = []
+        for k in PARTICLE_KEYS:
+            a = parts.get(k)
+            if a is None:
+                a = np.zeros(n)
+            arrs.append(np.ascontiguousarray(a, dtype=np.float64))
+        self.api["add_particles"](self.h, n, *[_dp(a) for a in arrs])
+
+    def count(self) -> int:
+        return self.api["count_particles"](self.h)
+
+    def get_particles(self):
+        n = self.count()
+        cap = max(n, 1)
+        out = np.empty((10, cap), dtype=np.float64)
+        cell = np.empty(cap, dtype=np.int64)
+        self.api["get_particles"](self.h, cap, _dp(out), cell.ctypes.data_as(_LP))
+        d = {k: out[i, :n].copy() for i, k in enumerate(PARTICLE_KEYS)}
+        d["cell"] = cell[:n].copy()
+        return d
+
+    def diag_len(self) -> int:
+        return self.api["diag_len"](self.h)
+
+    def step(self, nsteps=1, external_bz=0.0) -> np.ndarray:
+        d = np.zeros((nsteps, self.diag_len()), dtype=np.float64)
+        self.api["step"](self.h, nsteps, external_bz, _dp(d))
+        return d
+
+    def padvance(self, external_bz=0.0):
+        self.api["padvance"](self.h, external_bz)
+
+    def fadvance(self):
+        self.api["fadvance"](self.h)
+
+    def compute_diag(self) -> np.ndarray:
+        d = np.zeros(self.diag_len())
+        self.api["compute_diag"](self.h, _dp(d))
+        return d
+
+    def zero_j(self):
+        self.api["zero_j"](self.h)
+
+    def jdeposition(self, pos, d, q):
+        p = np.ascontiguousarray(pos, dtype=np.float64).copy()
+        dd = np.ascontiguousarray(d, dtype=np.float64)
+        self.api["jdeposition"](self.h, _dp(p), _dp(dd), q)
+        return p
+
+    def gather(self, x, y, z):
+        e = np.zeros(3)
+        b = np.zeros(3)
+        self.api["gather"](self.h, x, y, z, _dp(e), _dp(b))
+        return e, b
+
+    def chi(self, e, b, u, g):
+        e, b, u = (np.ascontiguousarray(v, dtype=np.float64) for v in (e, b, u))
+        return self.api["chi"](self.h, _dp(e), _dp(b), _dp(u), g)
+
+    def w(self, g, r, chi):
+        rr = np.array([r], dtype=np.float64)
+        v = self.api["w"](self.h, g, _dp(rr), chi)
+        return v, float(rr[0])
+
+    def tilde_w(self, g, r, chi):
+        return self.api["tilde_w"](self.h, g, r, chi)
+
+    def mathcal_W(self, e, b):
+        e, b = (np.ascontiguousarray(v, dtype=np.float64) for v in (e, b))
+        return self.api["mathcal_W"](self.h, _dp(e), _dp(b))
+
+    def get_rand(self):
+        return self.api["get_rand"](self.h)
+
+
+def push(pusher, cmr, state, e, b, dt, kind="port", flavour="parity"):
+    api = _load(kind, flavour)
+    s = np.ascontiguousarray(state, dtype=np.float64).copy()
+    e, b = (np.ascontiguousarray(v, dtype=np.float64) for v in (e, b))
+    api["push"](pusher, cmr, _dp(s), _dp(e), _dp(b), dt)
+    return s

@@ -1,0 +1,235 @@
+"""ctypes binding of libquill_b200.so (the C ABI in include/quill_b200.h).
+
+`Region` mirrors the reference's step contract on `spatial_region`
+(include/main.h:17-170): load fields and particles, `init_boundaries`
+(f_init_boundaries + interpolate_be), `step` (birth_from_vacuum -> padvance
+-> compute_N / compute_energy -> fadvance, main.cpp:2321-2331), and dumps.
+
+There is no CPU fallback: constructing a Region without the built library
+or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libquill_b200.so")
+
+QP_MAX_SPECIES = 8
+SOLVERS = {"fdtd": 0, "ndfx": 1, "five_point": 2}
+PUSHERS = {"vay": 0, "boris": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+STATUS = {0: "QP_OK", 1: "QP_ERR_CONFIG", 2: "QP_ERR_CAPACITY", 3: "QP_ERR_NAN", 4: "QP_ERR_TIMEOUT",
+          5: "QP_ERR_CUDA", 6: "QP_ERR_STATE", 7: "QP_ERR_ARG"}
+
+
+class QPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
+        ("lambda_cm", C.c_double),
+        ("solver", C.c_int), ("pusher", C.c_int), ("qed", C.c_int), ("precision", C.c_int),
+        ("seed", C.c_uint64),
+        ("n_species", C.c_int),
+        ("cmr", C.c_double * QP_MAX_SPECIES),
+        ("capacity", C.c_int64 * QP_MAX_SPECIES),
+        ("device", C.c_int),
+    ]
+
+
+class Diag(C.Structure):
+    _fields_ = [
+        ("N_e", C.c_double), ("N_p", C.c_double), ("N_ph", C.c_double),
+        ("N_qp_e", C.c_int64), ("N_qp_p", C.c_int64), ("N_qp_g", C.c_int64),
+        ("energy_f", C.c_double), ("energy_e", C.c_double), ("energy_p", C.c_double),
+        ("energy_ph", C.c_double),
+        ("n_ion", C.c_int),
+        ("N_qp_i", C.c_int64 * QP_MAX_SPECIES),
+        ("ienergy", C.c_double * QP_MAX_SPECIES),
+        ("n_macro", C.c_int64 * QP_MAX_SPECIES),
+        ("status", C.c_int32), ("pad_", C.c_int32),
+    ]
+
+    def as_array(self) -> np.ndarray:
+        """Same layout as the CPU checkers' diagnostic rows: N_e N_p N_ph
+        N_qp_e N_qp_p N_qp_g energy_f energy_e energy_p energy_ph, then
+        (N_qp_i, ienergy) per ion population."""
+        v = [self.N_e, self.N_p, self.N_ph, self.N_qp_e, self.N_qp_p, self.N_qp_g,
+             self.energy_f, self.energy_e, self.energy_p, self.energy_ph]
+        for m in range(self.n_ion):
+            v += [self.N_qp_i[m], self.ienergy[m]]
+        return np.array(v, dtype=np.float64)
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load libquill_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"libquill_b200.so not built at {p}: run `python -m quill_b200.build`")
+    lib = C.CDLL(p)
+    D, DP, I64, I64P, VP = C.c_double, C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_int64), C.c_void_p
+    sig = {
+        "qp_version": (C.c_char_p, []),
+        "qp_last_error": (C.c_char_p, [VP]),
+        "qp_create": (C.c_int, [C.POINTER(Params), C.POINTER(VP)]),
+        "qp_destroy": (C.c_int, [VP]),
+        "qp_load_fields": (C.c_int, [VP] + [DP] * 6),
+        "qp_init_boundaries": (C.c_int, [VP]),
+        "qp_load_particles": (C.c_int, [VP, C.c_int, I64] + [DP] * 9),
+        "qp_step": (C.c_int, [VP, C.c_int, D, C.POINTER(Diag)]),
+        "qp_get_diag": (C.c_int, [VP, C.POINTER(Diag)]),
+        "qp_dump_fields": (C.c_int, [VP, DP]),
+        "qp_count_particles": (C.c_int, [VP, C.c_int, I64P]),
+        "qp_dump_particles": (C.c_int, [VP, C.c_int, I64] + [DP] * 9 + [I64P]),
+        "qp_checkpoint": (C.c_int, [VP, C.c_int]),
+        "qp_restore": (C.c_int, [VP, C.c_int]),
+        "qp_synchronize": (C.c_int, [VP]),
+        "qp_set_stream": (C.c_int, [VP, VP]),
+        "qp_launch_count": (C.c_int, [VP, I64P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+PARTICLE_KEYS = ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")
+
+
+class Region:
+    """One simulation region on one GPU."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, dt, *, species_cmr=(-1.0,), lambda_cm=1e-4,
+                 solver="fdtd", pusher="boris", qed=False, precision="fp64", seed=0,
+                 capacity=None, device=0):
+        lib = load_library()
+        self.lib = lib
+        p = Params()
+        p.nx, p.ny, p.nz = nx, ny, nz
+        p.dx, p.dy, p.dz, p.dt = dx, dy, dz, dt
+        p.lambda_cm = lambda_cm
+        p.solver = SOLVERS[solver] if isinstance(solver, str) else int(solver)
+        p.pusher = PUSHERS[pusher] if isinstance(pusher, str) else int(pusher)
+        p.qed = int(bool(qed))
+        p.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        p.seed = seed
+        p.n_species = len(species_cmr)
+        for i, c in enumerate(species_cmr):
+            p.cmr[i] = c
+            p.capacity[i] = int(capacity[i]) if capacity is not None else 0
+        p.device = device
+        h = C.c_void_p()
+        r = lib.qp_create(C.byref(p), C.byref(h))
+        if r != 0:
+            raise QPError(r, lib.qp_last_error(None).decode())
+        self.h = h
+        self.params = p
+        self.shape = (nx, ny, nz)
+        self.n_species = len(species_cmr)
+
+    def _check(self, r):
+        if r != 0:
+            raise QPError(r, self.lib.qp_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nc(self):
+        nx, ny, nz = self.shape
+        return nx * ny * nz
+
+    def set_fields(self, ex, ey, ez, bx, by, bz):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (ex, ey, ez, bx, by, bz)]
+        for a in arrs:
+            if a.size != self.nc:
+                raise ValueError("field plane size mismatch")
+        self._check(self.lib.qp_load_fields(self.h, *[_dp(a) for a in arrs]))
+
+    def init_boundaries(self):
+        self._check(self.lib.qp_init_boundaries(self.h))
+
+    def add_particles(self, species: int, parts: dict):
+        n = len(parts["x"])
+        arrs = []
+        for k in PARTICLE_KEYS:
+            a = parts.get(k)
+            arrs.append(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
+        self._check(self.lib.qp_load_particles(self.h, species, n, *[_dp(a) for a in arrs]))
+
+    def step(self, nsteps=1, external_bz=0.0) -> list:
+        d = (Diag * max(nsteps, 1))()
+        self._check(self.lib.qp_step(self.h, nsteps, external_bz, d))
+        return [d[i] for i in range(nsteps)]
+
+    def get_diag(self) -> Diag:
+        d = Diag()
+        self._check(self.lib.qp_get_diag(self.h, C.byref(d)))
+        return d
+
+    def get_fields(self) -> np.ndarray:
+        out = np.empty((12,) + self.shape, dtype=np.float64)
+        self._check(self.lib.qp_dump_fields(self.h, _dp(out)))
+        return out
+
+    def count(self, species: int) -> int:
+        n = C.c_int64()
+        self._check(self.lib.qp_count_particles(self.h, species, C.byref(n)))
+        return n.value
+
+    def get_particles(self, species: int) -> dict:
+        n = self.count(species)
+        cap = max(n, 1)
+        out = {k: np.zeros(cap) for k in PARTICLE_KEYS}
+        cell = np.zeros(cap, dtype=np.int64)
+        self._check(self.lib.qp_dump_particles(self.h, species, cap, *[_dp(out[k]) for k in PARTICLE_KEYS],
+                                               cell.ctypes.data_as(C.POINTER(C.c_int64))))
+        d = {k: v[:n] for k, v in out.items()}
+        d["cell"] = cell[:n]
+        return d
+
+    def checkpoint(self, slot=0):
+        self._check(self.lib.qp_checkpoint(self.h, slot))
+
+    def restore(self, slot=0):
+        self._check(self.lib.qp_restore(self.h, slot))
+
+    def synchronize(self):
+        self._check(self.lib.qp_synchronize(self.h))
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._check(self.lib.qp_launch_count(self.h, C.byref(n)))
+        return n.value

@@ -1,0 +1,630 @@
+// C ABI of libquill_b200 (include/quill_b200.h): host-side orchestration of
+// one region on one GPU.  Each call maps onto the spatial_region member or
+// main() code it replaces (cited per function).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qp_internal.h"
+#include "qp_fields.cuh"
+
+#define QP_VERSION_STRING "quill_b200 0.1 (sm_100a)"
+
+namespace qp {
+
+SolverCoef solver_coef(const qp_params& p) {
+    const double PI = 3.141592653589793;
+    SolverCoef c;
+    // maxwell.cpp:6-8
+    c.dtdx = p.dt / p.dx;
+    c.dtdy = p.dt / p.dy;
+    c.dtdz = p.dt / p.dz;
+    c.dx = p.dx; c.dy = p.dy; c.dz = p.dz;
+    // five-point, maxwell.cpp:24-33
+    c.fax = 0.25 * (1 - p.dx / p.dt * std::sin(0.5 * PI * std::min(1.0, p.dt / p.dx)));
+    c.fay = 0.25 * (1 - p.dy / p.dt * std::sin(0.5 * PI * std::min(1.0, p.dt / p.dy)));
+    c.faz = 0.25 * (1 - p.dz / p.dt * std::sin(0.5 * PI * std::min(1.0, p.dt / p.dz)));
+    c.fbx = 1 - 2 * c.fax;
+    c.fby = 1 - 2 * c.fay;
+    c.fbz = 1 - 2 * c.faz;
+    // NDFX, maxwell.cpp:238-249
+    const double kappa = 1.25 * (std::sqrt(3.0) - 1) * 0.5 / std::sqrt(3.0);
+    c.nbx = (1 - kappa);
+    c.nax = 0.5 * (1 - c.nbx);
+    c.nby = 1 - kappa * p.dx * p.dx / (p.dy * p.dy);
+    c.nbz = 1 - kappa * p.dx * p.dx / (p.dz * p.dz);
+    c.nay = 0.5 * (1 - c.nby);
+    c.naz = 0.5 * (1 - c.nbz);
+    return c;
+}
+
+void zero_planes_fp64(State& s, const ZeroPlane* zp, int n);
+void zero_planes_mixed(State& s, const ZeroPlane* zp, int n);
+int load_merge(State& s, int si, int64_t n_old, const int32_t* d_new_start, int32_t* d_perm_out);
+
+static int n_arrays(const State& s) { return s.fp64 ? 9 : 10; }
+static size_t arr_elem(const State& s, int a) { return s.fp64 ? 8 : 4; }
+
+// Allocate (or grow, keeping contents) the particle arrays of a species.
+static int ensure_capacity(State& s, int si, int64_t need) {
+    Species& sp = s.sp[si];
+    if (need <= sp.cap) return QP_OK;
+    if (need >= (int64_t)INT32_MAX) {
+        s.err = "particle count exceeds 2^31-1 per species";
+        return QP_ERR_CAPACITY;
+    }
+    int64_t cap = std::max<int64_t>(need, sp.cap + sp.cap / 2);
+    cap = std::min<int64_t>(cap, (int64_t)INT32_MAX - 1);
+    const int na = n_arrays(s);
+    for (int b = 0; b < 2; b++)
+        for (int a = 0; a < na; a++) {
+            if (s.fp64 && a == 8 && !s.prm.qed) continue;   // chi only with QED
+            if (!s.fp64 && a == 9 && !s.prm.qed) continue;
+            void* p = nullptr;
+            QP_CUDA_CHECK(s, cudaMalloc(&p, cap * arr_elem(s, a)));
+            if (sp.buf[b][a]) {
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(p, sp.buf[b][a], sp.cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
+                QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+                cudaFree(sp.buf[b][a]);
+            }
+            sp.buf[b][a] = p;
+        }
+    int32_t* np = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&np, cap * sizeof(int32_t)));
+    if (sp.perm) {
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(np, sp.perm, sp.cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        cudaFree(sp.perm);
+    }
+    sp.perm = np;
+    if (sp.newcell) cudaFree(sp.newcell);
+    QP_CUDA_CHECK(s, cudaMalloc(&sp.newcell, cap * sizeof(int32_t)));
+    sp.cap = cap;
+    return QP_OK;
+}
+
+// Release every device and pinned allocation of a region.
+static void free_state(State* s) {
+    if (!s) return;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    cudaFree(s->fields);
+    for (auto& sp : s->sp) {
+        for (int b = 0; b < 2; b++)
+            for (int a = 0; a < 10; a++) cudaFree(sp.buf[b][a]);
+        cudaFree(sp.perm);
+        cudaFree(sp.newcell);
+        cudaFree(sp.cell_start);
+        cudaFree(sp.cell_next);
+        cudaFree(sp.count);
+    }
+    for (auto& sn : s->snap) {
+        cudaFree(sn.fields);
+        for (auto& v : sn.arrays)
+            for (void* p : v) cudaFree(p);
+        for (auto* p : sn.cell_start) cudaFree(p);
+    }
+    cudaFree(s->d_diag);
+    cudaFreeHost(s->h_diag);
+    cudaFree(s->d_status);
+    cudaFree(s->scan_tmp);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    s->stream = nullptr;
+}
+
+}  // namespace qp
+
+struct qp_handle {
+    qp::State st;
+};
+
+using namespace qp;
+
+static thread_local std::string g_create_error;
+
+#define QP_H_CHECK(h)                              \
+    do {                                           \
+        if (!(h)) return QP_ERR_ARG;               \
+        cudaError_t e0 = cudaSetDevice((h)->st.prm.device); \
+        if (e0 != cudaSuccess) {                   \
+            (h)->st.err = cudaGetErrorString(e0);  \
+            return QP_ERR_CUDA;                    \
+        }                                          \
+    } while (0)
+
+extern "C" {
+
+const char* qp_version(void) { return QP_VERSION_STRING; }
+
+const char* qp_last_error(const qp_handle* h) {
+    if (!h) return g_create_error.c_str();
+    return h->st.err.c_str();
+}
+
+int qp_create(const qp_params* prm, qp_handle** out) {
+    if (!prm || !out) { g_create_error = "null argument"; return QP_ERR_ARG; }
+    *out = nullptr;
+    const qp_params& p = *prm;
+    auto bad = [&](const char* m) { g_create_error = m; return QP_ERR_CONFIG; };
+    if (p.nx < 5 || p.ny < 5 || p.nz < 5) return bad("grid must have at least 5 cells per axis");
+    if ((int64_t)p.nx * p.ny * p.nz >= (int64_t)INT32_MAX - 1) return bad("grid exceeds 2^31 cells");
+    if (!(p.dx > 0 && p.dy > 0 && p.dz > 0 && p.dt > 0)) return bad("dx, dy, dz, dt must be positive");
+    // a particle must not move more than one cell per axis and step
+    if (!(p.dt < p.dx && p.dt < p.dy && p.dt < p.dz)) return bad("dt must be smaller than dx, dy and dz");
+    if (p.solver < 0 || p.solver > 2) return bad("unknown solver");
+    if (p.pusher < 0 || p.pusher > 1) return bad("unknown pusher");
+    if (p.precision < 0 || p.precision > 1) return bad("unknown precision");
+    if (p.n_species < 0 || p.n_species > QP_MAX_SPECIES) return bad("n_species out of range");
+    if (!(p.lambda_cm > 0)) return bad("lambda_cm must be positive");
+    if (p.qed) return bad("QED is not available in this build of the library");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        g_create_error = "no CUDA device";
+        return QP_ERR_CUDA;
+    }
+    if (p.device < 0 || p.device >= ndev) return bad("device ordinal out of range");
+    qp_handle* h = new qp_handle();
+    State& s = h->st;
+    s.prm = p;
+    s.fp64 = p.precision == QP_PREC_FP64;
+    s.grid.nx = p.nx; s.grid.ny = p.ny; s.grid.nz = p.nz;
+    s.grid.nynz = p.ny * p.nz;
+    s.grid.nc = p.nx * p.ny * p.nz;
+    s.field_elem = s.fp64 ? 8 : 4;
+    cudaError_t e = cudaSetDevice(p.device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+    s.own_stream = true;
+    const size_t nc = (size_t)s.grid.nc;
+    if (e == cudaSuccess) e = cudaMalloc(&s.fields, 12 * nc * s.field_elem);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.fields, 0, 12 * nc * s.field_elem, s.stream);
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_diag, sizeof(DiagAccum));
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_diag, sizeof(DiagAccum), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(unsigned int), s.stream);
+    s.scan_tmp_bytes = ((nc + 4095) / 4096 + 2) * sizeof(int32_t);
+    if (e == cudaSuccess) e = cudaMalloc(&s.scan_tmp, s.scan_tmp_bytes);
+    int ion = 0;
+    s.sp.resize(p.n_species);
+    for (int i = 0; i < p.n_species && e == cudaSuccess; i++) {
+        Species& sp = s.sp[i];
+        sp.cmr = p.cmr[i];
+        sp.kind = p.cmr[i] == 0 ? KIND_PHOTON : (std::fabs(p.cmr[i]) == 1 ? KIND_LEPTON : KIND_ION);
+        sp.ion_index = sp.kind == KIND_ION ? ion++ : -1;
+        e = cudaMalloc(&sp.cell_start, (nc + 1) * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMemsetAsync(sp.cell_start, 0, (nc + 1) * sizeof(int32_t), s.stream);
+        if (e == cudaSuccess) e = cudaMalloc(&sp.cell_next, (nc + 1) * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc(&sp.count, nc * sizeof(int32_t));
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("qp_create: ") + cudaGetErrorString(e);
+        free_state(&h->st);
+        delete h;
+        return QP_ERR_CUDA;
+    }
+    for (int i = 0; i < p.n_species; i++) {
+        int64_t c = p.capacity[i];
+        if (c > 0) {
+            int r = ensure_capacity(s, i, c);
+            if (r != QP_OK) {
+                g_create_error = s.err;
+                free_state(&h->st);
+                delete h;
+                return r;
+            }
+        }
+    }
+    *out = h;
+    return QP_OK;
+}
+
+int qp_destroy(qp_handle* h) {
+    if (!h) return QP_OK;
+    cudaSetDevice(h->st.prm.device);
+    free_state(&h->st);
+    delete h;
+    return QP_OK;
+}
+
+int qp_set_stream(qp_handle* h, void* stream) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    if (stream) {
+        if (s.own_stream) cudaStreamDestroy(s.stream);
+        s.stream = (cudaStream_t)stream;
+        s.own_stream = false;
+    }
+    return QP_OK;
+}
+
+int qp_synchronize(qp_handle* h) {
+    QP_H_CHECK(h);
+    QP_CUDA_CHECK(h->st, cudaStreamSynchronize(h->st.stream));
+    return QP_OK;
+}
+
+int qp_launch_count(qp_handle* h, int64_t* out) {
+    if (!h || !out) return QP_ERR_ARG;
+    *out = h->st.launches;
+    return QP_OK;
+}
+
+int qp_load_fields(qp_handle* h, const double* ex, const double* ey, const double* ez, const double* bx,
+                   const double* by, const double* bz) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (!ex || !ey || !ez || !bx || !by || !bz) { s.err = "null field plane"; return QP_ERR_ARG; }
+    const size_t nc = (size_t)s.grid.nc;
+    const double* src[6] = {ex, ey, ez, bx, by, bz};
+    if (s.fp64) {
+        for (int a = 0; a < 6; a++)
+            QP_CUDA_CHECK(s, cudaMemcpyAsync((double*)s.fields + a * nc, src[a], nc * 8, cudaMemcpyHostToDevice, s.stream));
+    } else {
+        std::vector<float> tmp(nc);
+        for (int a = 0; a < 6; a++) {
+            for (size_t c = 0; c < nc; c++) tmp[c] = (float)src[a][c];
+            QP_CUDA_CHECK(s, cudaMemcpyAsync((float*)s.fields + a * nc, tmp.data(), nc * 4, cudaMemcpyHostToDevice, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        }
+    }
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    s.boundaries_done = false;
+    return QP_OK;
+}
+
+int qp_init_boundaries(qp_handle* h) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    const int nx = s.grid.nx, ny = s.grid.ny, nz = s.grid.nz;
+    const int ALL = 63, EX = 1, EY = 2, EZ = 4, BX = 8, BY = 16, BZ = 32;
+    std::vector<ZeroPlane> zp;
+    if (s.prm.solver == QP_SOLVER_FDTD) {  // maxwell.cpp:532-597
+        zp = {{0, 0, EY | EZ | BX}, {0, nx - 1, ALL}, {1, 0, EX | EZ | BY}, {1, ny - 1, ALL},
+              {2, 0, EY | EX | BZ}, {2, nz - 1, ALL}};
+    } else if (s.prm.solver == QP_SOLVER_NDFX) {  // maxwell.cpp:338-438
+        zp = {{0, 0, ALL}, {0, 1, EY | EZ | BX}, {0, nx - 1, ALL}, {1, 0, ALL}, {1, 1, EX | EZ | BY},
+              {1, ny - 1, ALL}, {2, 0, ALL}, {2, 1, EY | EX | BZ}, {2, nz - 1, ALL}};
+    } else {  // maxwell.cpp:135-236
+        zp = {{0, 0, ALL}, {1, 0, ALL}, {2, 0, ALL}, {0, nx - 1, ALL}, {1, ny - 1, ALL}, {2, nz - 1, ALL},
+              {0, nx - 2, BY | BZ}, {0, 1, EZ | EY}, {1, ny - 2, BX | BZ}, {1, 1, EX | EZ},
+              {2, nz - 2, BX | BY}, {2, 1, EX | EY}};
+    }
+    if (s.fp64) {
+        zero_planes_fp64(s, zp.data(), (int)zp.size());
+        launch_fields_fp64(s, 3);
+    } else {
+        zero_planes_mixed(s, zp.data(), (int)zp.size());
+        launch_fields_mixed(s, 3);
+    }
+    QP_CUDA_CHECK(s, cudaGetLastError());
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    s.boundaries_done = true;
+    return QP_OK;
+}
+
+int qp_load_particles(qp_handle* h, int si, int64_t n, const double* x, const double* y, const double* z,
+                      const double* ux, const double* uy, const double* uz, const double* g, const double* q,
+                      const double* chi) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (si < 0 || si >= (int)s.sp.size()) { s.err = "species index out of range"; return QP_ERR_ARG; }
+    if (n < 0) { s.err = "negative particle count"; return QP_ERR_ARG; }
+    if (n == 0) return QP_OK;
+    if (!x || !y || !z || !ux || !uy || !uz || !g || !q) { s.err = "null particle array"; return QP_ERR_ARG; }
+    Species& sp = s.sp[si];
+    const Grid gr = s.grid;
+    const int64_t n_old = sp.n;
+    if (n_old + n >= (int64_t)INT32_MAX) { s.err = "particle count exceeds 2^31-1"; return QP_ERR_CAPACITY; }
+    // cells and a stable counting sort on the host
+    std::vector<int32_t> cell(n);
+    for (int64_t p = 0; p < n; p++) {
+        const double px = x[p], py = y[p], pz = z[p];
+        if (!(px >= 0 && px < gr.nx && py >= 0 && py < gr.ny && pz >= 0 && pz < gr.nz) ||
+            !std::isfinite(ux[p]) || !std::isfinite(uy[p]) || !std::isfinite(uz[p]) || !std::isfinite(g[p]) ||
+            !std::isfinite(q[p])) {
+            char b[160];
+            snprintf(b, sizeof b, "particle %lld outside the grid or not finite", (long long)p);
+            s.err = b;
+            return QP_ERR_CONFIG;
+        }
+        cell[p] = ((int)px * gr.ny + (int)py) * gr.nz + (int)pz;
+    }
+    std::vector<int32_t> start(gr.nc + 1, 0);
+    for (int64_t p = 0; p < n; p++) start[cell[p] + 1]++;
+    for (int c = 0; c < gr.nc; c++) start[c + 1] += start[c];
+    std::vector<int32_t> order(n);
+    {
+        std::vector<int32_t> fill(start.begin(), start.end() - 1);
+        for (int64_t p = 0; p < n; p++) order[fill[cell[p]]++] = (int32_t)p;
+    }
+    int r = ensure_capacity(s, si, n_old + n);
+    if (r != QP_OK) return r;
+    const int cur = sp.cur;
+    if (s.fp64) {
+        const double* src[9] = {x, y, z, ux, uy, uz, g, q, chi};
+        std::vector<double> tmp(n);
+        for (int a = 0; a < 9; a++) {
+            if (!sp.buf[cur][a]) continue;
+            for (int64_t t = 0; t < n; t++) tmp[t] = src[a] ? src[a][order[t]] : 0.0;
+            QP_CUDA_CHECK(s, cudaMemcpyAsync((double*)sp.buf[cur][a] + n_old, tmp.data(), n * 8, cudaMemcpyHostToDevice, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        }
+    } else {
+        std::vector<int32_t> tc(n);
+        std::vector<float> tmp(n);
+        for (int64_t t = 0; t < n; t++) tc[t] = cell[order[t]];
+        QP_CUDA_CHECK(s, cudaMemcpyAsync((int32_t*)sp.buf[cur][0] + n_old, tc.data(), n * 4, cudaMemcpyHostToDevice, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        const double* pos[3] = {x, y, z};
+        for (int a = 0; a < 3; a++) {
+            for (int64_t t = 0; t < n; t++) {
+                const double v = pos[a][order[t]];
+                float o = (float)(v - std::floor(v));
+                if (o >= 1.0f) o = 0.99999994f;
+                tmp[t] = o;
+            }
+            QP_CUDA_CHECK(s, cudaMemcpyAsync((float*)sp.buf[cur][1 + a] + n_old, tmp.data(), n * 4, cudaMemcpyHostToDevice, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        }
+        const double* src[6] = {ux, uy, uz, g, q, chi};
+        for (int a = 0; a < 6; a++) {
+            if (!sp.buf[cur][4 + a]) continue;
+            for (int64_t t = 0; t < n; t++) tmp[t] = src[a] ? (float)src[a][order[t]] : 0.0f;
+            QP_CUDA_CHECK(s, cudaMemcpyAsync((float*)sp.buf[cur][4 + a] + n_old, tmp.data(), n * 4, cudaMemcpyHostToDevice, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        }
+    }
+    // merge in front of the old particles of each cell
+    int32_t* d_new_start = nullptr;
+    int32_t* d_perm = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&d_new_start, (gr.nc + 1) * sizeof(int32_t)));
+    QP_CUDA_CHECK(s, cudaMalloc(&d_perm, sp.cap * sizeof(int32_t)));
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(d_new_start, start.data(), (gr.nc + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s.stream));
+    load_merge(s, si, n_old, d_new_start, d_perm);
+    QP_CUDA_CHECK(s, cudaGetLastError());
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    cudaFree(sp.perm);
+    sp.perm = d_perm;
+    cudaFree(d_new_start);
+    sp.n = n_old + n;
+    return QP_OK;
+}
+
+static void fill_diag(State& s, qp_diag* d) {
+    const qp_params& p = s.prm;
+    const double PI = 3.141592653589793;
+    const double dV = p.dx * p.dy * p.dz;
+    // normalisations of main.cpp:2326-2327
+    const double aN = dV * 1.11485e13 * p.lambda_cm / (8 * PI * PI * PI);
+    const double aE = 0.5 * dV * 3.691e4 * p.lambda_cm / 1e7;
+    const double bE = 8.2e-14 * dV * 1.11485e13 * p.lambda_cm / (8 * PI * PI * PI);
+    memset(d, 0, sizeof(*d));
+    const DiagAccum& a = *s.h_diag;
+    double Ne = 0, Np = 0, Nph = 0, ee = 0, ep = 0, eph = 0;
+    for (size_t i = 0; i < s.sp.size(); i++) {
+        const Species& sp = s.sp[i];
+        d->n_macro[i] = (int64_t)a.cnt[i];
+        // compute_N / compute_energy species tests (fout.cpp:62-77, 105-126)
+        if (sp.cmr == -1) { Ne -= a.sum_q[i]; ee -= a.sum_e[i]; d->N_qp_e += a.cnt[i]; }
+        else if (sp.cmr == 1) { Np += a.sum_q[i]; ep += a.sum_e[i]; d->N_qp_p += a.cnt[i]; }
+        else if (sp.cmr == 0) { Nph += a.sum_q[i]; eph += a.sum_e[i]; d->N_qp_g += a.cnt[i]; }
+        else if (sp.ion_index >= 0) {
+            d->N_qp_i[sp.ion_index] += a.cnt[i];
+            d->ienergy[sp.ion_index] += a.sum_e[i] / sp.cmr * bE;
+        }
+    }
+    int nion = 0;
+    for (const auto& sp : s.sp) nion += sp.kind == KIND_ION;
+    d->n_ion = nion;
+    d->N_e = Ne * aN; d->N_p = Np * aN; d->N_ph = Nph * aN;
+    d->energy_f = a.field * aE;
+    d->energy_e = ee * bE; d->energy_p = ep * bE; d->energy_ph = eph * bE;
+}
+
+int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (nsteps < 0) { s.err = "negative step count"; return QP_ERR_ARG; }
+    const size_t nc = (size_t)s.grid.nc;
+    for (int l = 0; l < nsteps; l++) {
+        // padvance (advance.cpp:90-387): J = 0, push and deposit every species
+        QP_CUDA_CHECK(s, cudaMemsetAsync((char*)s.fields + 6 * nc * s.field_elem, 0, 3 * nc * s.field_elem, s.stream));
+        QP_CUDA_CHECK(s, cudaMemsetAsync(s.d_diag, 0, sizeof(DiagAccum), s.stream));
+        for (size_t i = 0; i < s.sp.size(); i++) {
+            if (s.fp64) launch_push_fp64(s, (int)i, external_bz);
+            else launch_push_mixed(s, (int)i, external_bz);
+        }
+        QP_CUDA_CHECK(s, cudaGetLastError());
+        for (size_t i = 0; i < s.sp.size(); i++)
+            if (s.sp[i].n > 0) rebin(s, (int)i);
+        QP_CUDA_CHECK(s, cudaGetLastError());
+        // compute_energy field term on E, B before fadvance (main.cpp:2327)
+        if (s.fp64) launch_field_energy_fp64(s);
+        else launch_field_energy_mixed(s);
+        // fadvance: half B, E, half B, Bbar (maxwell.cpp:10-22, advance.cpp:13-18)
+        for (int ph = 0; ph < 4; ph++) {
+            if (s.fp64) launch_fields_fp64(s, ph == 2 ? 0 : ph);
+            else launch_fields_mixed(s, ph == 2 ? 0 : ph);
+        }
+        QP_CUDA_CHECK(s, cudaGetLastError());
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(s.h_diag, s.d_diag, sizeof(DiagAccum), cudaMemcpyDeviceToHost, s.stream));
+        unsigned int st = 0;
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(&st, s.d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        fill_diag(s, &s.last_diag);
+        s.last_diag.status = st ? (st & ST_NAN ? QP_ERR_NAN : (st & ST_CAPACITY ? QP_ERR_CAPACITY : QP_ERR_CONFIG)) : QP_OK;
+        s.have_diag = true;
+        s.step_index++;
+        if (diag) diag[l] = s.last_diag;
+        if (st) {
+            s.err = st & ST_NAN ? "non-finite particle momentum" :
+                    (st & ST_CAPACITY ? "particle store full" : "particle left the grid bounds");
+            return s.last_diag.status;
+        }
+    }
+    return QP_OK;
+}
+
+int qp_get_diag(qp_handle* h, qp_diag* out) {
+    QP_H_CHECK(h);
+    if (!out) return QP_ERR_ARG;
+    if (!h->st.have_diag) { h->st.err = "no step has run"; return QP_ERR_STATE; }
+    *out = h->st.last_diag;
+    return QP_OK;
+}
+
+int qp_dump_fields(qp_handle* h, double* out) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (!out) return QP_ERR_ARG;
+    const size_t nc = (size_t)s.grid.nc;
+    if (s.fp64) {
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(out, s.fields, 12 * nc * 8, cudaMemcpyDeviceToHost, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    } else {
+        std::vector<float> tmp(12 * nc);
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), s.fields, 12 * nc * 4, cudaMemcpyDeviceToHost, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        for (size_t c = 0; c < 12 * nc; c++) out[c] = tmp[c];
+    }
+    return QP_OK;
+}
+
+int qp_count_particles(qp_handle* h, int si, int64_t* n) {
+    QP_H_CHECK(h);
+    if (!n || si < 0 || si >= (int)h->st.sp.size()) return QP_ERR_ARG;
+    *n = h->st.sp[si].n;
+    return QP_OK;
+}
+
+int qp_dump_particles(qp_handle* h, int si, int64_t cap, double* x, double* y, double* z, double* ux,
+                      double* uy, double* uz, double* g, double* q, double* chi, int64_t* cell) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (si < 0 || si >= (int)s.sp.size()) return QP_ERR_ARG;
+    Species& sp = s.sp[si];
+    const int64_t n = sp.n;
+    if (cap < n) { s.err = "dump capacity smaller than the particle count"; return QP_ERR_ARG; }
+    if (n == 0) return QP_OK;
+    std::vector<int32_t> perm(n), cs(s.grid.nc + 1);
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(perm.data(), sp.perm, n * 4, cudaMemcpyDeviceToHost, s.stream));
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(cs.data(), sp.cell_start, (s.grid.nc + 1) * 4, cudaMemcpyDeviceToHost, s.stream));
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    // slots in use: [0, max perm]
+    int32_t used = 0;
+    for (int64_t t = 0; t < n; t++) used = std::max(used, perm[t] + 1);
+    std::vector<int32_t> cl(n);
+    for (int c = 0; c < s.grid.nc; c++)
+        for (int t = cs[c]; t < cs[c + 1]; t++) cl[t] = c;
+    if (cell)
+        for (int64_t t = 0; t < n; t++) cell[t] = cl[t];
+    const int cur = sp.cur;
+    if (s.fp64) {
+        double* dst[9] = {x, y, z, ux, uy, uz, g, q, chi};
+        std::vector<double> tmp(used);
+        for (int a = 0; a < 9; a++) {
+            if (!dst[a]) continue;
+            if (!sp.buf[cur][a]) { std::fill(dst[a], dst[a] + n, 0.0); continue; }
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), sp.buf[cur][a], (size_t)used * 8, cudaMemcpyDeviceToHost, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            for (int64_t t = 0; t < n; t++) dst[a][t] = tmp[perm[t]];
+        }
+    } else {
+        std::vector<float> tmp(used);
+        std::vector<int32_t> tci(used);
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(tci.data(), sp.buf[cur][0], (size_t)used * 4, cudaMemcpyDeviceToHost, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        double* pos[3] = {x, y, z};
+        for (int a = 0; a < 3; a++) {
+            if (!pos[a]) continue;
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), sp.buf[cur][1 + a], (size_t)used * 4, cudaMemcpyDeviceToHost, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            for (int64_t t = 0; t < n; t++) {
+                const int c = tci[perm[t]];
+                const int ii = c / s.grid.nynz, jj = (c / s.grid.nz) % s.grid.ny, kk = c % s.grid.nz;
+                const int base = a == 0 ? ii : (a == 1 ? jj : kk);
+                pos[a][t] = (double)base + (double)tmp[perm[t]];
+            }
+        }
+        double* dst[6] = {ux, uy, uz, g, q, chi};
+        for (int a = 0; a < 6; a++) {
+            if (!dst[a]) continue;
+            if (!sp.buf[cur][4 + a]) { std::fill(dst[a], dst[a] + n, 0.0); continue; }
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), sp.buf[cur][4 + a], (size_t)used * 4, cudaMemcpyDeviceToHost, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            for (int64_t t = 0; t < n; t++) dst[a][t] = tmp[perm[t]];
+        }
+    }
+    return QP_OK;
+}
+
+int qp_checkpoint(qp_handle* h, int slot) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (slot < 0 || slot > 3) return QP_ERR_ARG;
+    auto& sn = s.snap[slot];
+    const size_t nc = (size_t)s.grid.nc;
+    if (!sn.fields) QP_CUDA_CHECK(s, cudaMalloc(&sn.fields, 12 * nc * s.field_elem));
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.fields, s.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    for (auto& v : sn.arrays)
+        for (void* p : v) cudaFree(p);
+    sn.arrays.assign(s.sp.size(), std::vector<void*>(11, nullptr));
+    sn.n.assign(s.sp.size(), 0);
+    sn.cap.assign(s.sp.size(), 0);
+    sn.cell_start.resize(s.sp.size(), nullptr);
+    for (size_t i = 0; i < s.sp.size(); i++) {
+        Species& sp = s.sp[i];
+        const int64_t cap = sp.cap;
+        sn.cap[i] = cap;
+        sn.n[i] = sp.n;
+        if (cap > 0) {
+            for (int a = 0; a < 10; a++) {
+                if (!sp.buf[sp.cur][a]) continue;
+                QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][a], cap * arr_elem(s, a)));
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][a], sp.buf[sp.cur][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
+            }
+            QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][10], cap * 4));
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][10], sp.perm, cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+        }
+        if (!sn.cell_start[i]) QP_CUDA_CHECK(s, cudaMalloc(&sn.cell_start[i], (nc + 1) * 4));
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.cell_start[i], sp.cell_start, (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
+    }
+    sn.step_index = s.step_index;
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    sn.valid = true;
+    return QP_OK;
+}
+
+int qp_restore(qp_handle* h, int slot) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (slot < 0 || slot > 3) return QP_ERR_ARG;
+    auto& sn = s.snap[slot];
+    if (!sn.valid) { s.err = "checkpoint slot is empty"; return QP_ERR_STATE; }
+    const size_t nc = (size_t)s.grid.nc;
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(s.fields, sn.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
+    for (size_t i = 0; i < s.sp.size(); i++) {
+        Species& sp = s.sp[i];
+        const int64_t cap = sn.cap[i];
+        int r = ensure_capacity(s, (int)i, cap);
+        if (r != QP_OK) return r;
+        if (cap > 0) {
+            for (int a = 0; a < 10; a++) {
+                if (!sp.buf[sp.cur][a] || !sn.arrays[i][a]) continue;
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.buf[sp.cur][a], sn.arrays[i][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
+            }
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.perm, sn.arrays[i][10], cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+        }
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.cell_start, sn.cell_start[i], (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
+        sp.n = sn.n[i];
+    }
+    s.step_index = sn.step_index;
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    return QP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// Internal declarations of libquill_b200: device state of one region and the
+// kernel entry points shared between translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/quill_b200.h"
+
+namespace qp {
+
+// Particle kinds, from the charge-to-mass test chain of padvance
+// (advance.cpp:155 photon cmr == 0, :253 |cmr| == 1 lepton, :360 ion).
+enum Kind { KIND_PHOTON = 0, KIND_LEPTON = 1, KIND_ION = 2 };
+
+// Device error word bits, OR-ed by kernels into State::d_status.
+enum StatusBits {
+    ST_NAN = 1u << 0,       // non-finite gamma after a push
+    ST_BOUNDS = 1u << 1,    // an access would have left the grid (skipped)
+    ST_CAPACITY = 1u << 2,  // append beyond a store's capacity (dropped)
+};
+
+struct Grid {
+    int nx, ny, nz;
+    int nynz;
+    int nc;  // nx*ny*nz < 2^31
+};
+
+// Fields: 12 planes of nc elements (E, B, J, Bbar), element type T.
+template <typename T>
+struct Fields {
+    T* ex; T* ey; T* ez;
+    T* bx; T* by; T* bz;
+    T* jx; T* jy; T* jz;
+    T* bex; T* bey; T* bez;
+};
+
+// FP64 particle store, structure of arrays, one slot per particle.
+struct PStore64 {
+    double *x, *y, *z, *ux, *uy, *uz, *g, *q, *chi;
+};
+
+// Mixed particle store: linear cell index plus FP32 offset in [0, 1).
+struct PStore32 {
+    int32_t* cell;
+    float *ox, *oy, *oz, *ux, *uy, *uz, *g, *q, *chi;
+};
+
+struct Species {
+    double cmr = -1;
+    int kind = KIND_LEPTON;
+    int ion_index = -1;
+    int64_t n = 0;       // live particles
+    int64_t cap = 0;     // slots
+    // two buffers of each array; `cur` holds the particles in the layout of
+    // the previous push, read through `perm` in traversal order
+    void* buf[2][10] = {{nullptr}};
+    int cur = 0;
+    int32_t* perm = nullptr;       // traversal position -> slot in buf[cur]
+    int32_t* newcell = nullptr;    // cell after this push (-1 = erased), by traversal position
+    int32_t* cell_start = nullptr; // nc+1, traversal order at the start of a step
+    int32_t* cell_next = nullptr;  // nc+1, traversal order after the rebin
+    int32_t* count = nullptr;      // nc, rebin histogram
+};
+
+struct DiagAccum {
+    // per species: live count, sum q, sum of (g-1)q (or g q for photons)
+    double sum_q[QP_MAX_SPECIES];
+    double sum_e[QP_MAX_SPECIES];
+    unsigned long long cnt[QP_MAX_SPECIES];
+    double field;  // sum over cells of E^2 + B^2
+};
+
+struct State {
+    qp_params prm;
+    Grid grid;
+    int fp64 = 1;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    void* fields = nullptr;       // 12 planes
+    size_t field_elem = 8;
+    std::vector<Species> sp;
+    DiagAccum* d_diag = nullptr;  // device accumulators
+    DiagAccum* h_diag = nullptr;  // pinned host copy
+    unsigned int* d_status = nullptr;
+    void* scan_tmp = nullptr;     // block sums for the exclusive scans
+    size_t scan_tmp_bytes = 0;
+    qp_diag last_diag{};
+    bool have_diag = false;
+    int64_t launches = 0;
+    int64_t step_index = 0;
+    bool boundaries_done = false;
+    std::string err;
+    // checkpoints (device-resident copies)
+    struct Snap {
+        bool valid = false;
+        void* fields = nullptr;
+        std::vector<std::vector<void*>> arrays;  // per species, 10 arrays
+        std::vector<int64_t> n, cap;
+        std::vector<int32_t*> cell_start;
+        int64_t step_index = 0;
+    } snap[4];
+};
+
+// ---- kernels / launchers (FP64, qp_fp64.cu) ----
+void launch_fields_fp64(State& s, int phase);          // phase: 0 half B, 1 E, 2 half B, 3 Bbar
+void launch_init_boundaries_fp64(State& s);
+void launch_push_fp64(State& s, int species, double external_bz);
+void launch_field_energy_fp64(State& s);
+
+// ---- mixed precision (qp_mixed.cu) ----
+void launch_fields_mixed(State& s, int phase);
+void launch_init_boundaries_mixed(State& s);
+void launch_push_mixed(State& s, int species, double external_bz);
+void launch_field_energy_mixed(State& s);
+
+// ---- rebin and scans (qp_rebin.cu) ----
+// Rebin after a push: count -> scan -> assign; leaves the new traversal
+// order in sp.perm / sp.cell_next and swaps buffers.  Returns the new count.
+int64_t rebin(State& s, int species);
+// Sort freshly loaded particles (n_new appended at the tail of buf[cur],
+// cell ids in newcell) into traversal order; returns QP_OK or an error.
+int load_sort(State& s, int species, int64_t n_old, int64_t n_new, const int32_t* d_cells_new);
+void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n);
+
+}  // namespace qp
+
+#define QP_CUDA_CHECK(s, call)                                                  \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            (s).err = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+            return QP_ERR_CUDA;                                                  \
+        }                                                                        \
+    } while (0)

@@ -1,0 +1,122 @@
+// Kernel bodies shared by the FP64 translation unit (qp_fp64.cu, built with
+// --fmad=false) and the mixed-precision one (qp_mixed.cu, FMA allowed).
+#pragma once
+
+#include "qp_fields.cuh"
+
+namespace qp {
+
+// One thread per cell, (k, j, i) = (x, y, z) launch axes.
+template <typename T, int SOLVER, int PHASE>
+__global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = blockIdx.z;
+    if (k >= g.nz || j >= g.ny) return;
+    if (PHASE == 0) {
+        if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
+        else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
+        else fp_b(f, g, c, i, j, k);
+    } else if (PHASE == 1) {
+        if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
+        else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
+        else fp_e(f, g, c, i, j, k);
+    } else {
+        bbar(f, g, i, j, k);
+    }
+}
+
+// Zero the components in mask `comps` (bits ex ey ez bx by bz) on plane
+// `plane` of axis `axis`, over [0, n-1) of the two other axes.
+template <typename T>
+__global__ void k_zero_plane(Fields<T> f, Grid g, int axis, int plane, int comps) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = blockIdx.y;
+    int i, j, k;
+    int nu, nv;
+    if (axis == 0) { nu = g.nz; nv = g.ny; i = plane; j = v; k = u; }
+    else if (axis == 1) { nu = g.nz; nv = g.nx; i = v; j = plane; k = u; }
+    else { nu = g.ny; nv = g.nx; i = v; j = u; k = plane; }
+    if (u >= nu - 1 || v >= nv - 1) return;
+    const int x = cidx(g, i, j, k);
+    if (comps & 1) f.ex[x] = T(0);
+    if (comps & 2) f.ey[x] = T(0);
+    if (comps & 4) f.ez[x] = T(0);
+    if (comps & 8) f.bx[x] = T(0);
+    if (comps & 16) f.by[x] = T(0);
+    if (comps & 32) f.bz[x] = T(0);
+}
+
+template <typename V>
+__device__ __forceinline__ V warp_sum(V v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sums of three values, one atomic per block into the species'
+// diagnostic accumulators.
+__device__ __forceinline__ void block_diag(DiagAccum* acc, int sp, double dq, double de,
+                                           unsigned long long dc) {
+    __shared__ double s_q[32], s_e[32];
+    __shared__ unsigned long long s_c[32];
+    dq = warp_sum(dq);
+    de = warp_sum(de);
+    dc = warp_sum(dc);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { s_q[wid] = dq; s_e[wid] = de; s_c[wid] = dc; }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        dq = lane < nw ? s_q[lane] : 0.0;
+        de = lane < nw ? s_e[lane] : 0.0;
+        dc = lane < nw ? s_c[lane] : 0ull;
+        dq = warp_sum(dq);
+        de = warp_sum(de);
+        dc = warp_sum(dc);
+        if (lane == 0 && dc) {
+            atomicAdd(&acc->sum_q[sp], dq);
+            atomicAdd(&acc->sum_e[sp], de);
+            atomicAdd(&acc->cnt[sp], dc);
+        }
+    }
+}
+
+// Sum of E^2 + B^2 over all cells (compute_energy's field term,
+// fout.cpp:101-102), FP64 accumulation.
+template <typename T>
+__global__ void __launch_bounds__(256) k_field_energy(Fields<T> f, int nc, DiagAccum* acc) {
+    double s = 0.0;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nc; x += gridDim.x * blockDim.x) {
+        const double ex = f.ex[x], ey = f.ey[x], ez = f.ez[x], bx = f.bx[x], by = f.by[x], bz = f.bz[x];
+        s += ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
+    }
+    __shared__ double sh[32];
+    s = warp_sum(s);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = s;
+    __syncthreads();
+    if (wid == 0) {
+        s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        s = warp_sum(s);
+        if (lane == 0) atomicAdd(&acc->field, s);
+    }
+}
+
+// Erased by p_boundary (plist.cpp:73-102): layers {0, n-2, n-1} of each axis.
+__device__ __forceinline__ bool kill_layer(const Grid& g, int i, int j, int k) {
+    return i <= 0 || i >= g.nx - 2 || j <= 0 || j >= g.ny - 2 || k <= 0 || k >= g.nz - 2;
+}
+// is_inside (plist.cpp:42-48)
+__device__ __forceinline__ bool inside(const Grid& g, int i, int j, int k) {
+    return i > 0 && i < g.nx - 2 && j > 0 && j < g.ny - 2 && k > 0 && k < g.nz - 2;
+}
+
+struct PushArgs {
+    double cmr, dt, dx, dy, dz, ext_bz;
+    int n, sp, kind;
+    unsigned int* status;
+    DiagAccum* diag;
+};
+
+}  // namespace qp

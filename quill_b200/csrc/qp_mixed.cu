@@ -1,0 +1,157 @@
+// Mixed-precision path: positions as a linear cell index plus an FP32 offset
+// in [0, 1), FP32 push, gather, current deposition and Maxwell stencils.
+// Diagnostics are accumulated in FP64.  The algorithms are the reference's;
+// the deposition runs in the particle's cell frame (offsets), which is the
+// reference's absolute-coordinate algorithm shifted by an integer.
+#include "qp_kernels.cuh"
+
+namespace qp {
+
+struct PushArgs32 {
+    float cmr, dt, idx, idy, idz, ext_bz;
+    int n, sp, kind;
+    unsigned int* status;
+    DiagAccum* diag;
+};
+
+__device__ __forceinline__ float wrap_offset(float o, int& shift) {
+    const float fl = floorf(o);
+    shift = (int)fl;
+    float r = o - fl;
+    // keep the offset in [0, 1) after rounding
+    if (r >= 1.0f) r = 0.99999994f;
+    if (r < 0.0f) r = 0.0f;
+    return r;
+}
+
+template <int PUSHER, int KIND>
+__global__ void __launch_bounds__(256) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
+                                                const int32_t* __restrict__ perm,
+                                                int32_t* __restrict__ newcell, PushArgs32 a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    double dq = 0.0, de = 0.0;
+    unsigned long long dc = 0;
+    if (s < a.n) {
+        const int p = perm[s];
+        const int c0 = src.cell[p];
+        const int i0 = c0 / g.nynz, j0 = (c0 / g.nz) % g.ny, k0 = c0 - (c0 / g.nz) * g.nz;
+        float o[3] = {src.ox[p], src.oy[p], src.oz[p]};
+        float ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
+        const float q = src.q[p];
+        int nc = -1;
+        int i1 = i0, j1 = j0, k1 = k0;
+        if (!kill_layer(g, i0, j0, k0)) {
+            float E[3], B[3];
+            gather(f, g, i0, j0, k0, o[0], o[1], o[2], E, B);
+            B[2] += a.ext_bz;
+            if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
+            const float t = a.dt / gm;
+            float d[3] = {ux * t * a.idx, uy * t * a.idy, uz * t * a.idz};
+            if (KIND == KIND_PHOTON) {
+                o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
+            } else {
+                jdeposition(f, g, o, d, q, i0, j0, k0, a.status);
+            }
+            if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+            int si, sj, sk;
+            o[0] = wrap_offset(o[0], si);
+            o[1] = wrap_offset(o[1], sj);
+            o[2] = wrap_offset(o[2], sk);
+            i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
+            const bool moved = si | sj | sk;
+            if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
+        }
+        newcell[s] = nc;
+        if (nc >= 0) {
+            dst.cell[s] = nc;
+            dst.ox[s] = o[0]; dst.oy[s] = o[1]; dst.oz[s] = o[2];
+            dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
+            dst.g[s] = gm; dst.q[s] = q;
+            if (dst.chi) dst.chi[s] = src.chi[p];
+            dq = (double)q;
+            de = KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
+            dc = 1;
+        }
+    }
+    block_diag(a.diag, a.sp, dq, de, dc);
+}
+
+static Fields<float> fields32(State& s) {
+    float* b = (float*)s.fields;
+    const size_t nc = (size_t)s.grid.nc;
+    Fields<float> f;
+    float** p[12] = {&f.ex, &f.ey, &f.ez, &f.bx, &f.by, &f.bz, &f.jx, &f.jy, &f.jz, &f.bex, &f.bey, &f.bez};
+    for (int a = 0; a < 12; a++) *p[a] = b + a * nc;
+    return f;
+}
+
+SolverCoef solver_coef(const qp_params& p);
+
+void launch_fields_mixed(State& s, int phase) {
+    Fields<float> f = fields32(s);
+    Coef<float> c(solver_coef(s.prm));
+    dim3 blk(32, 8, 1);
+    dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, s.grid.nx);
+    const int sol = s.prm.solver;
+#define QP_LF(SOL, PH) k_field<float, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c)
+    if (phase == 0 || phase == 2) {
+        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 0);
+        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 0);
+        else QP_LF(QP_SOLVER_FIVE_POINT, 0);
+    } else if (phase == 1) {
+        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 1);
+        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 1);
+        else QP_LF(QP_SOLVER_FIVE_POINT, 1);
+    } else {
+        QP_LF(QP_SOLVER_FDTD, 3);
+    }
+#undef QP_LF
+    s.launches++;
+}
+
+void zero_planes_mixed(State& s, const ZeroPlane* zp, int n) {
+    Fields<float> f = fields32(s);
+    for (int a = 0; a < n; a++) {
+        int nu = zp[a].axis == 2 ? s.grid.ny : s.grid.nz;
+        int nv = zp[a].axis == 0 ? s.grid.ny : s.grid.nx;
+        dim3 grd((nu + 127) / 128, nv);
+        k_zero_plane<float><<<grd, 128, 0, s.stream>>>(f, s.grid, zp[a].axis, zp[a].plane, zp[a].comps);
+        s.launches++;
+    }
+}
+
+void launch_push_mixed(State& s, int si, double external_bz) {
+    Species& sp = s.sp[si];
+    if (sp.n == 0) return;
+    PStore32 src, dst;
+    src.cell = (int32_t*)sp.buf[sp.cur][0];
+    dst.cell = (int32_t*)sp.buf[1 - sp.cur][0];
+    float** ps[9] = {&src.ox, &src.oy, &src.oz, &src.ux, &src.uy, &src.uz, &src.g, &src.q, &src.chi};
+    float** pd[9] = {&dst.ox, &dst.oy, &dst.oz, &dst.ux, &dst.uy, &dst.uz, &dst.g, &dst.q, &dst.chi};
+    for (int a = 0; a < 9; a++) {
+        *ps[a] = (float*)sp.buf[sp.cur][1 + a];
+        *pd[a] = (float*)sp.buf[1 - sp.cur][1 + a];
+    }
+    PushArgs32 a;
+    a.cmr = (float)sp.cmr; a.dt = (float)s.prm.dt;
+    a.idx = (float)(1.0 / s.prm.dx); a.idy = (float)(1.0 / s.prm.dy); a.idz = (float)(1.0 / s.prm.dz);
+    a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
+    a.status = s.d_status; a.diag = s.d_diag;
+    const int nb = (int)((sp.n + 255) / 256);
+    Fields<float> f = fields32(s);
+    const bool vay = s.prm.pusher == QP_PUSHER_VAY;
+#define QP_LP(P, K) k_push32<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a)
+    if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
+    else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
+    else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
+#undef QP_LP
+    s.launches++;
+}
+
+void launch_field_energy_mixed(State& s) {
+    Fields<float> f = fields32(s);
+    k_field_energy<float><<<148 * 4, 256, 0, s.stream>>>(f, s.grid.nc, s.d_diag);
+    s.launches++;
+}
+
+}  // namespace qp

@@ -1,0 +1,240 @@
+// Device arithmetic of QUILL's per-timestep loop, templated on the real type
+// T (double for the FP64 path, float for the mixed path).
+//
+// Expression trees follow the reference operation by operation (same operand
+// association) so that the FP64 instantiation, compiled with --fmad=false,
+// performs the same IEEE operation sequence as the reference CPU build with
+// -ffp-contract=off.  Citations are to the reference's source files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qp_internal.h"
+
+namespace qp {
+
+template <typename T>
+__device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+__device__ __forceinline__ int cidx(const Grid& g, int i, int j, int k) {
+    return (i * g.ny + j) * g.nz + k;
+}
+
+// ----------------------------------------------------------------------------
+// Pushers (pusher.cpp)
+// ----------------------------------------------------------------------------
+
+// Vay (2008), pusher.cpp:5-42.  Uses the stored gamma g for the first
+// rotation, so g must be consistent with u on entry.
+template <typename T>
+__device__ __forceinline__ void push_vay(T cmr, T& ux, T& uy, T& uz, T& g, const T E[3],
+                                         const T B[3], T dt) {
+    T t = dt * cmr;
+    T ex = E[0] * t, ey = E[1] * t, ez = E[2] * t;
+    t = T(0.5) * t;
+    T bx = B[0] * t, by = B[1] * t, bz = B[2] * t;
+    T wx = ux + ex + (uy * bz - uz * by) / g;
+    T wy = uy + ey + (uz * bx - ux * bz) / g;
+    T wz = uz + ez + (ux * by - uy * bx) / g;
+    t = bx * bx + by * by + bz * bz;
+    T bw = bx * wx + by * wy + bz * wz;
+    T gg = T(1) + wx * wx + wy * wy + wz * wz - t;
+    gg = sqrt(T(0.5) * (gg + sqrt(gg * gg + T(4) * (t + bw * bw))));
+    t = T(1) / (T(1) + t / (gg * gg));
+    bw = bw / (gg * gg);
+    ux = (wx + (wy * bz - wz * by) / gg + bx * bw) * t;
+    uy = (wy + (wz * bx - wx * bz) / gg + by * bw) * t;
+    uz = (wz + (wx * by - wy * bx) / gg + bz * bw) * t;
+    g = gg;
+}
+
+// Boris, pusher.cpp:44-97.
+template <typename T>
+__device__ __forceinline__ void push_boris(T cmr, T& ux, T& uy, T& uz, T& g, const T E[3],
+                                           const T B[3], T dt) {
+    T t = T(0.5) * dt * cmr;
+    T ex = E[0] * t, ey = E[1] * t, ez = E[2] * t;
+    T u1x = ux + ex, u1y = uy + ey, u1z = uz + ez;
+    T gg = sqrt(T(1) + u1x * u1x + u1y * u1y + u1z * u1z);
+    t /= gg;
+    T bx = B[0] * t, by = B[1] * t, bz = B[2] * t;
+    T wx = u1x + (u1y * bz - u1z * by);
+    T wy = u1y + (u1z * bx - u1x * bz);
+    T wz = u1z + (u1x * by - u1y * bx);
+    t = T(2) / (T(1) + bx * bx + by * by + bz * bz);
+    u1x += (wy * bz - wz * by) * t;
+    u1y += (wz * bx - wx * bz) * t;
+    u1z += (wx * by - wy * bx) * t;
+    ux = u1x + ex;
+    uy = u1y + ey;
+    uz = u1z + ez;
+    g = sqrt(T(1) + ux * ux + uy * uy + uz * uz);
+}
+
+template <int PUSHER, typename T>
+__device__ __forceinline__ void push(T cmr, T& ux, T& uy, T& uz, T& g, const T E[3], const T B[3],
+                                     T dt) {
+    if (PUSHER == QP_PUSHER_VAY) push_vay(cmr, ux, uy, uz, g, E, B, dt);
+    else push_boris(cmr, ux, uy, uz, g, E, B, dt);
+}
+
+// ----------------------------------------------------------------------------
+// Field gather (deposition.cpp:431-471): Ex is interpolated in (y, z) at the
+// particle's i, Ey in (x, z), Ez in (x, y); B the same on Bbar.
+// (i, j, k) is the particle's cell, (xa, ya, za) its offset in the cell.
+// ----------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void gather(const Fields<T>& f, const Grid& gr, int i, int j, int k, T xa,
+                                       T ya, T za, T E[3], T B[3]) {
+    const T xb = T(1) - xa, yb = T(1) - ya, zb = T(1) - za;
+    const int c = cidx(gr, i, j, k);
+    const int cj1 = c + gr.nz, ck1 = c + 1, ci1 = c + gr.nynz;
+    E[0] = ld(f.ex + c) * yb * zb + ld(f.ex + cj1) * ya * zb + ld(f.ex + ck1) * yb * za + ld(f.ex + cj1 + 1) * ya * za;
+    E[1] = ld(f.ey + c) * xb * zb + ld(f.ey + ci1) * xa * zb + ld(f.ey + ck1) * xb * za + ld(f.ey + ci1 + 1) * xa * za;
+    E[2] = ld(f.ez + c) * xb * yb + ld(f.ez + ci1) * xa * yb + ld(f.ez + cj1) * xb * ya + ld(f.ez + ci1 + gr.nz) * xa * ya;
+    B[0] = ld(f.bex + c) * yb * zb + ld(f.bex + cj1) * ya * zb + ld(f.bex + ck1) * yb * za + ld(f.bex + cj1 + 1) * ya * za;
+    B[1] = ld(f.bey + c) * xb * zb + ld(f.bey + ci1) * xa * zb + ld(f.bey + ck1) * xb * za + ld(f.bey + ci1 + 1) * xa * za;
+    B[2] = ld(f.bez + c) * xb * yb + ld(f.bez + ci1) * xa * yb + ld(f.bez + cj1) * xb * ya + ld(f.bez + ci1 + gr.nz) * xa * ya;
+}
+
+// ----------------------------------------------------------------------------
+// Current deposition (deposition.cpp:13-356)
+// ----------------------------------------------------------------------------
+
+// 12 contributions of one straight segment d starting at p, lying in the cell
+// with lower corner w (deposition.cpp:13-39).  p and w are in the particle's
+// frame; the global cell of the corner is base + w.  Out-of-grid targets are
+// skipped and flagged (cannot happen for dt < dx, dy, dz).
+template <typename T>
+__device__ __forceinline__ void seg_dep(const Fields<T>& f, const Grid& gr, const T p[3], const T d[3],
+                                        T q, const int w[3], int bi, int bj, int bk,
+                                        unsigned int* status) {
+    const T xa = p[0] - T(w[0]), xb = T(1) - xa;
+    const T ya = p[1] - T(w[1]), yb = T(1) - ya;
+    const T za = p[2] - T(w[2]), zb = T(1) - za;
+    const int wi = bi + w[0], wj = bj + w[1], wk = bk + w[2];
+    const T dx = d[0], dy = d[1], dz = d[2];
+    if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= gr.nx || wj + 1 >= gr.ny || wk + 1 >= gr.nz) {
+        atomicOr(status, (unsigned int)ST_BOUNDS);
+        return;
+    }
+    const int c = cidx(gr, wi, wj, wk);
+    const int cj1 = c + gr.nz, ck1 = c + 1, ci1 = c + gr.nynz;
+    const T third = T(3);
+    atomicAdd(f.jx + cj1 + 1, dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third));
+    atomicAdd(f.jx + ck1, dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - dy * dz / third));
+    atomicAdd(f.jx + cj1, dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - dy * dz / third));
+    atomicAdd(f.jx + c, dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + dy * dz / third));
+    atomicAdd(f.jy + ci1 + 1, dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + dx * dz / third));
+    atomicAdd(f.jy + ck1, dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - dx * dz / third));
+    atomicAdd(f.jy + ci1, dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - dx * dz / third));
+    atomicAdd(f.jy + c, dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + dx * dz / third));
+    atomicAdd(f.jz + ci1 + gr.nz, dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + dx * dy / third));
+    atomicAdd(f.jz + cj1, dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third));
+    atomicAdd(f.jz + ci1, dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third));
+    atomicAdd(f.jz + c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third));
+}
+
+// Three ratios sorted descending with the reference's tie handling
+// (`regulate`, low-level.cpp:316-366).
+template <typename T>
+__device__ __forceinline__ void sort3_desc(T a, T b, T c, T& vx, T& vy, T& vz) {
+    if (a > b) {
+        if (b > c) { vx = a; vy = b; vz = c; }
+        else { vz = b; if (a > c) { vx = a; vy = c; } else { vx = c; vy = a; } }
+    } else {
+        if (c > b) { vx = c; vy = b; vz = a; }
+        else { vx = b; if (a > c) { vy = a; vz = c; } else { vy = c; vz = a; } }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ int ifloor(T v) { return (int)floor(v); }
+
+// Split the straight path p -> p + d at the cell faces it crosses (1..4
+// segments), deposit each segment in its cell and advance p segment by
+// segment (deposition.cpp:41-356).  p is in a frame whose integer lattice is
+// the cell lattice shifted by base (base = 0 for absolute FP64 positions).
+template <typename T>
+__device__ __forceinline__ void jdeposition(const Fields<T>& f, const Grid& gr, T p[3], const T d[3], T q,
+                                            int bi, int bj, int bk, unsigned int* status) {
+    int c1[3], c2[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) { c1[a] = ifloor(p[a]); c2[a] = ifloor(p[a] + d[a]); }
+    const int cx = c1[0] != c2[0], cy = c1[1] != c2[1], cz = c1[2] != c2[2];
+    const int ncross = cx + cy + cz;
+    T s[3];
+    int w[3] = {c1[0], c1[1], c1[2]};
+    if (ncross == 0) {
+        seg_dep(f, gr, p, d, q, w, bi, bj, bk, status);
+#pragma unroll
+        for (int o = 0; o < 3; o++) p[o] = p[o] + d[o];
+    } else if (ncross == 1) {
+        const int a = cx ? 0 : (cy ? 1 : 2);
+        s[a] = T(max(c1[a], c2[a])) - p[a];
+#pragma unroll
+        for (int o = 0; o < 3; o++) if (o != a) s[o] = d[o] * s[a] / d[a];
+        seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
+#pragma unroll
+        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+#pragma unroll
+        for (int o = 0; o < 3; o++) s[o] = d[o] - s[o];
+        w[a] = c2[a];
+        seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
+#pragma unroll
+        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+    } else if (ncross == 2) {
+        // axis A carries the reference's path1 (y for (y,z) and (x,y), x for
+        // (x,z)), axis B its path2; B goes first only if path1 > path2
+        int A, B;
+        if (!cx) { A = 1; B = 2; }
+        else if (!cy) { A = 0; B = 2; }
+        else { A = 1; B = 0; }
+        const T pa = (T(max(c1[A], c2[A])) - p[A]) / d[A];
+        const T pb = (T(max(c1[B], c2[B])) - p[B]) / d[B];
+        int first = A, second = B;
+        T p1 = pa, p2 = pb;
+        if (pa > pb) { first = B; second = A; p1 = pb; p2 = pa; }
+#pragma unroll
+        for (int o = 0; o < 3; o++) s[o] = d[o] * p1;
+        seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
+#pragma unroll
+        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        const T pm = p2 - p1;
+#pragma unroll
+        for (int o = 0; o < 3; o++) s[o] = d[o] * pm;
+        w[first] = c2[first];
+        seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
+#pragma unroll
+        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        const T pr = T(1) - p2;
+#pragma unroll
+        for (int o = 0; o < 3; o++) s[o] = d[o] * pr;
+        w[second] = c2[second];
+        seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
+#pragma unroll
+        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+    } else {
+        T path[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) path[a] = (T(max(c1[a], c2[a])) - p[a]) / d[a];
+        T vx, vy, vz;
+        sort3_desc(path[0], path[1], path[2], vx, vy, vz);
+        const T fr[4] = {vz, vy - vz, vx - vy, T(1) - vx};
+#pragma unroll
+        for (int sg = 0; sg < 4; sg++) {
+#pragma unroll
+            for (int o = 0; o < 3; o++) s[o] = d[o] * fr[sg];
+            if (sg > 0) {
+#pragma unroll
+                for (int o = 0; o < 3; o++) w[o] = ifloor(p[o] + T(0.5) * s[o]);
+            }
+            seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
+#pragma unroll
+            for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        }
+    }
+}
+
+}  // namespace qp

@@ -1,0 +1,166 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU checker.
+
+FP64: bit-identical where the operation order is the reference's (fields
+without particles, one particle, the first step of the particles, cell
+indices and the traversal permutation); elsewhere within 1e-12 relative
+(the current J is summed with atomics, so only its rounding order differs).
+Mixed precision: within the tolerances stated per test.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._cases import PUSHER_ID, SOLVER_ID, all_particles, small_case
+from tests.conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+KIND = "ref" if O.available("ref", "parity") else "port"
+FKEYS = ("ex", "ey", "ez", "bx", "by", "bz")
+RTOL64 = 1e-12
+
+
+def _gpu(case, species, precision="fp64"):
+    from quill_b200.api import Region
+    return Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt, species_cmr=species,
+                  solver=case.solver, pusher=case.pusher, precision=precision)
+
+
+def _cpu(case, icmr=()):
+    return O.Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt,
+                    solver=SOLVER_ID[case.solver], pusher=PUSHER_ID[case.pusher], icmr=icmr, kind=KIND)
+
+
+def _load_both(case, fields, parts, species, precision="fp64"):
+    icmr = tuple(c for c in species if c not in (-1.0, 1.0, 0.0))
+    g, c = _gpu(case, species, precision), _cpu(case, icmr)
+    for r in (g, c):
+        r.set_fields(*[fields[k] for k in FKEYS])
+        r.init_boundaries()
+    for i, p in enumerate(parts):
+        g.add_particles(i, p)
+    if parts:
+        c.add_particles(all_particles(parts))
+    return g, c
+
+
+def _rel(a, b):
+    scale = np.max(np.abs(b))
+    return 0.0 if scale == 0 else float(np.max(np.abs(a - b)) / scale)
+
+
+def _split_by_species(cp, species):
+    return [{k: v[cp["cmr"] == s] for k, v in cp.items()} for s in species]
+
+
+@pytest.fixture(autouse=True)
+def _need_gpu():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.mark.parametrize("solver", ["fdtd", "ndfx", "five_point"])
+def test_fields_only_bitwise(solver):
+    dtdx = 0.3 if solver == "five_point" else 0.5
+    case, fields, _ = small_case(solver, dt_over_dx=dtdx, n=(23, 19, 17))
+    g, c = _load_both(case, fields, [], (-1.0,))
+    np.testing.assert_array_equal(g.get_fields(), c.get_fields())
+    for _ in range(5):
+        g.step(1)
+        c.step(1)
+    np.testing.assert_array_equal(g.get_fields(), c.get_fields())
+
+
+@pytest.mark.parametrize("solver", ["fdtd", "ndfx", "five_point"])
+@pytest.mark.parametrize("pusher", ["boris", "vay"])
+def test_steps_fp64(solver, pusher):
+    dtdx = 0.3 if solver == "five_point" else 0.5
+    species = (-1.0, 1.0, 1 / 1836.15, 0.0)
+    case, fields, parts = small_case(solver, pusher, dt_over_dx=dtdx, species=species, loaded_in_boundary=True)
+    g, c = _load_both(case, fields, parts, species)
+    for step in range(8):
+        dg = g.step(1, external_bz=0.3)[0]
+        dc = c.step(1, external_bz=0.3)[0]
+        cp = _split_by_species(c.get_particles(), species)
+        for si in range(len(species)):
+            gp = g.get_particles(si)
+            # cell indices and the traversal permutation are exact
+            np.testing.assert_array_equal(gp["cell"], cp[si]["cell"], err_msg=f"step {step} species {si}")
+            for k in ("x", "y", "z", "ux", "uy", "uz", "g", "q"):
+                if step == 0:
+                    np.testing.assert_array_equal(gp[k], cp[si][k], err_msg=f"step {step} {k}")
+                else:
+                    assert _rel(gp[k], cp[si][k]) <= RTOL64, (step, si, k, _rel(gp[k], cp[si][k]))
+        fg, fc = g.get_fields(), c.get_fields()
+        for a in range(12):
+            assert _rel(fg[a], fc[a]) <= RTOL64, (step, a, _rel(fg[a], fc[a]))
+        np.testing.assert_allclose(dg.as_array(), dc, rtol=1e-12, atol=0)
+
+
+def test_single_particle_bitwise():
+    case, fields, parts = small_case("fdtd", "boris")
+    p = {k: v[1000:1001] for k, v in parts[0].items()}
+    p["ux"][:] = 2.0; p["uy"][:] = -1.5; p["uz"][:] = 1.2
+    p["g"][:] = np.sqrt(1 + 4 + 2.25 + 1.44)
+    g, c = _load_both(case, fields, [p], (-1.0,))
+    for _ in range(10):
+        g.step(1)
+        c.step(1)
+        np.testing.assert_array_equal(g.get_fields(), c.get_fields())
+        gp, cp = g.get_particles(0), c.get_particles()
+        for k in ("x", "y", "z", "ux", "uy", "uz", "g"):
+            np.testing.assert_array_equal(gp[k], cp[k])
+
+
+def test_empty_and_all_erased():
+    case, fields, parts = small_case("fdtd", "boris")
+    g, c = _load_both(case, fields, [], (-1.0, 1.0))
+    d = g.step(3)
+    assert g.count(0) == 0 and d[-1].N_qp_e == 0
+    # particles only in the boundary layers: all erased on the first step
+    p = {k: v[:4].copy() for k, v in parts[0].items()}
+    p["x"][:] = [0.5, 0.7, case.nx - 1.5, case.nx - 0.2]
+    g.add_particles(0, p)
+    g.step(1)
+    assert g.count(0) == 0
+
+
+def test_checkpoint_restore_roundtrip():
+    case, fields, parts = small_case("ndfx", "vay", species=(-1.0, 1 / 1836.15))
+    g, _ = _load_both(case, fields, parts, (-1.0, 1 / 1836.15))
+    g.step(2)
+    g.checkpoint(1)
+    g.step(3)
+    f1, p1 = g.get_fields(), g.get_particles(0)
+    g.restore(1)
+    g.step(3)
+    f2, p2 = g.get_fields(), g.get_particles(0)
+    np.testing.assert_array_equal(p1["cell"], p2["cell"])
+    for a in range(12):
+        assert _rel(f2[a], f1[a]) <= RTOL64
+    for k in ("x", "ux", "g"):
+        assert _rel(p2[k], p1[k]) <= RTOL64
+
+
+@pytest.mark.parametrize("solver", ["fdtd", "ndfx", "five_point"])
+def test_mixed_precision_close(solver):
+    """FP32 path against the FP64 checker: fields within 1e-4 of their peak
+    after 5 steps, particle positions within 1e-4 cells."""
+    dtdx = 0.3 if solver == "five_point" else 0.5
+    species = (-1.0, 1 / 1836.15)
+    case, fields, parts = small_case(solver, "boris", dt_over_dx=dtdx, species=species)
+    g, c = _load_both(case, fields, parts, species, precision="mixed")
+    for _ in range(5):
+        g.step(1)
+        c.step(1)
+    fg, fc = g.get_fields(), c.get_fields()
+    for a in range(6):
+        assert _rel(fg[a], fc[a]) <= 1e-4, (a, _rel(fg[a], fc[a]))
+    cp = _split_by_species(c.get_particles(), species)
+    gp = g.get_particles(0)
+    if gp["x"].size == cp[0]["x"].size and np.array_equal(gp["cell"], cp[0]["cell"]):
+        assert np.max(np.abs(gp["x"] - cp[0]["x"])) < 1e-4
+    else:
+        # a particle within FP32 round-off of a face may land in the
+        # neighbouring cell; counts must still agree closely
+        assert abs(gp["x"].size - cp[0]["x"].size) <= max(2, gp["x"].size // 2000)
