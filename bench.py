@@ -1,0 +1,448 @@
+"""Throughput of QUILL's per-timestep PIC loop on B200 (one JSON line).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config cfg5_512_fdtd_boris] [--grid NX NY NZ]
+
+Workload: the 512^3-cell, 4-ppc configuration (dx = lambda/20, dt = dx/2,
+FDTD solver, Boris pusher, QED off, uniform 0.05 n_cr electron plasma with
+10 keV Maxwellian momenta, linearly polarised a0 = 20 laser pulse): 5.4e8
+electrons, 1.34e8 cells.  Synthetic, seeded, generated on the GPU.
+
+A step is one full timestep of main.cpp:2321-2331 (push + deposition +
+rebin, diagnostics, Maxwell solver + Bbar).  `value` = particle-steps/s with
+the state resident in HBM; FP64 (the reference arithmetic) is the headline,
+the mixed-precision run is reported in `mixed`.  `e2e` = the same metric for
+the whole job through the C ABI from pinned host buffers (create, load
+fields and particles, K steps with the per-step diagnostics copied to the
+host, dump of the fields to the host).  Inputs (tens of GB) are far larger
+than L2, so no flush is needed between steps.
+
+`--impl reference` times the reference's own CPU build (oracle/_ref) on the
+host cores: one process per core, each stepping a 64^3 sub-box of the same
+plasma (the reference's own parallelism is one x-slab per MPI rank).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+# algorithmic bytes per particle-step and per cell-update (push kernel reads
+# x y z ux uy uz g q and writes all but q; the fused field step reads E B J,
+# writes E B Bbar, the deposit flush writes J once)
+BYTES = {"fp64": (120, 168), "mixed": (68, 84)}
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU side: the reference build on a bounded sample
+# ----------------------------------------------------------------------------
+
+def _cpu_sample(args_tuple):
+    """One process: the reference (or the restatement) stepping a sub-box of
+    the configuration's plasma; returns (particle-steps, cell-updates, s)."""
+    kind, cfg_name, box, steps, warm, seed = args_tuple
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from oracle import oracle as O
+    from quill_b200 import workloads as W
+    case = W.scaled(W.config(cfg_name), box, box, box)
+    case.seed = seed
+    fields, parts = W.build(case)
+    solver = {"fdtd": 0, "ndfx": 1, "five_point": 2}[case.solver]
+    pusher = {"vay": 0, "boris": 1}[case.pusher]
+    icmr = tuple(sp.cmr for sp in case.species if sp.cmr not in (-1.0, 1.0, 0.0))
+    r = O.Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt, solver=solver, pusher=pusher,
+                 icmr=icmr, kind=kind, flavour="fast")
+    r.set_fields(*[fields[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
+    r.init_boundaries()
+    r.add_particles({k: np.concatenate([p[k] for p in parts]) for k in parts[0]})
+    r.step(warm)
+    n0 = r.count()
+    t0 = time.perf_counter()
+    d = r.step(steps)
+    dt = time.perf_counter() - t0
+    n1 = r.count()
+    nc = case.nx * case.ny * case.nz
+    return (0.5 * (n0 + n1) * steps, nc * steps, dt, n0)
+
+
+def cpu_kind():
+    from oracle import oracle as O
+    return "reference" if O.available("ref", "fast") else "port"
+
+
+def run_cpu(cfg_name, procs, box=64, steps=30, warm=2):
+    kind = "ref" if cpu_kind() == "reference" else "port"
+    work = [(kind, cfg_name, box, steps, warm, 1000 + r) for r in range(procs)]
+    if procs == 1:
+        res = [_cpu_sample(work[0])]
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_cpu_sample, work)
+    ps = sum(r[0] for r in res)
+    cu = sum(r[1] for r in res)
+    tmax = max(r[2] for r in res)
+    return {"particle_steps_per_s": ps / tmax, "cell_updates_per_s": cu / tmax, "seconds": tmax,
+            "particles_per_box": res[0][3], "kind": cpu_kind(), "procs": procs, "box": box, "steps": steps}
+
+
+# ----------------------------------------------------------------------------
+# GPU side
+# ----------------------------------------------------------------------------
+
+def build_region(case, precision, device_index, planes_per_chunk=48):
+    import torch
+    from quill_b200 import workloads as W
+    from quill_b200.api import Region
+    f = W.make_fields_torch(case, device=f"cuda:{device_index}")
+    reg = Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt,
+                 species_cmr=tuple(sp.cmr for sp in case.species), solver=case.solver, pusher=case.pusher,
+                 precision=precision, device=device_index)
+    reg.set_stream(torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    reg.lib.qp_load_fields(reg.h, *[_tp(f[k]) for k in ("ex", "ey", "ez", "bx", "by", "bz")])
+    del f
+    reg.init_boundaries()
+    for si, sp in enumerate(case.species):
+        for ch in W.particle_chunks_torch(case, sp, planes_per_chunk, device=f"cuda:{device_index}",
+                                          seed=case.seed + 17 * si):
+            _load_torch(reg, si, ch)
+            del ch
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return reg
+
+
+def _tp(t):
+    import ctypes as C
+    return C.cast(t.data_ptr(), C.POINTER(C.c_double))
+
+
+def _load_torch(reg, si, ch):
+    keys = ("x", "y", "z", "ux", "uy", "uz", "g", "q")
+    r = reg.lib.qp_load_particles(reg.h, si, ch["x"].numel(), *[_tp(ch[k]) for k in keys], None)
+    reg._check(r)
+
+
+def total_energy(d):
+    return d.energy_f + d.energy_e + d.energy_p + d.energy_ph + sum(d.ienergy[m] for m in range(d.n_ion))
+
+
+def time_region(reg, steps, warmup, device_index):
+    """Device-resident timing of `steps` steps after `warmup` steps."""
+    import torch
+    diags = reg.step(warmup) if warmup else []
+    reg.set_timing(True)
+    l0 = reg.launch_count()
+    n_before = sum(reg.count(i) for i in range(reg.n_species))
+    clk = Clocks(device_index)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk.start()
+    time.sleep(0.3)
+    e0.record()
+    d = reg.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    launches = reg.launch_count() - l0
+    phase_ms, nst = reg.get_timing()
+    reg.set_timing(False)
+    n_after = sum(reg.count(i) for i in range(reg.n_species))
+    psteps = sum(sum(x.n_macro[i] for i in range(reg.n_species)) for x in d)
+    # particles pushed per step are those alive at its start: n_before, then
+    # the counts after each step
+    pushed = n_before + sum(sum(x.n_macro[i] for i in range(reg.n_species)) for x in d[:-1])
+    return {"ms": ms, "steps": steps, "pushed": pushed, "launches": launches, "phase_ms": list(phase_ms),
+            "clocks": clocks, "diags": diags + d, "n_after": n_after}
+
+
+def e2e_run(case, precision, steps, device_index, host):
+    """Whole job through the C ABI from pinned host buffers."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from quill_b200.api import Diag, Region
+    t0 = time.perf_counter()
+    reg = Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt,
+                 species_cmr=tuple(sp.cmr for sp in case.species), solver=case.solver, pusher=case.pusher,
+                 precision=precision, device=device_index)
+    lib = reg.lib
+    reg._check(lib.qp_load_fields(reg.h, *[C.cast(host["f"][k].data_ptr(), C.POINTER(C.c_double))
+                                           for k in ("ex", "ey", "ez", "bx", "by", "bz")]))
+    reg.init_boundaries()
+    keys = ("x", "y", "z", "ux", "uy", "uz", "g", "q")
+    h2d = sum(host["f"][k].numel() * 8 for k in host["f"])
+    for si, chunks in enumerate(host["p"]):
+        for ch in chunks:
+            reg._check(lib.qp_load_particles(reg.h, si, ch["x"].numel(),
+                                             *[C.cast(ch[k].data_ptr(), C.POINTER(C.c_double)) for k in keys], None))
+            h2d += sum(ch[k].numel() * 8 for k in keys)
+    diag = (Diag * steps)()
+    pushed = sum(reg.count(i) for i in range(reg.n_species))
+    reg._check(lib.qp_step(reg.h, steps, 0.0, diag))
+    pushed += sum(sum(diag[s].n_macro[i] for i in range(reg.n_species)) for s in range(steps - 1))
+    out = host["out"]
+    reg._check(lib.qp_dump_fields(reg.h, C.cast(out.data_ptr(), C.POINTER(C.c_double))))
+    reg.close()
+    t = time.perf_counter() - t0
+    d2h = steps * C.sizeof(Diag) + out.numel() * 8
+    return {"value": pushed / t, "seconds": t, "steps": steps, "h2d_bytes_per_step": h2d // steps,
+            "d2h_bytes_per_step": d2h // steps}
+
+
+def pinned_host_state(case, device_index):
+    """Generate the state on the GPU and copy it to pinned host memory (not
+    timed)."""
+    import torch
+    from quill_b200 import workloads as W
+    f = W.make_fields_torch(case, device=f"cuda:{device_index}")
+    hf = {k: v.cpu().pin_memory() for k, v in f.items()}
+    del f
+    hp = []
+    for si, sp in enumerate(case.species):
+        chunks = []
+        for ch in W.particle_chunks_torch(case, sp, 48, device=f"cuda:{device_index}", seed=case.seed + 17 * si):
+            chunks.append({k: v.cpu().pin_memory() for k, v in ch.items()})
+        hp.append(chunks)
+    out = torch.empty(12 * case.nx * case.ny * case.nz, dtype=torch.float64).pin_memory()
+    torch.cuda.empty_cache()
+    return {"f": hf, "p": hp, "out": out}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg5_512_fdtd_boris")
+    ap.add_argument("--grid", type=int, nargs=3, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=30)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from quill_b200 import workloads as W
+    case = W.config(args.config)
+    if args.grid:
+        case = W.scaled(case, *args.grid)
+    nc = case.nx * case.ny * case.nz
+    metric = "particle-steps/s & field cell-updates/s, FP64 vs mixed, 1 B200, at stated drift"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        procs = os.cpu_count() or 1
+        r = run_cpu(args.config, procs, steps=max(args.steps, 5), warm=min(args.warmup, 2))
+        line = {
+            "impl": "reference", "metric": metric, "value": r["particle_steps_per_s"], "unit": "particle-steps/s",
+            "n_gpus": 0, "steps": r["steps"], "warmup": min(args.warmup, 2),
+            "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "cell_updates_per_s": r["cell_updates_per_s"],
+            "config": {"workload": f"{args.config} physics on {r['procs']} independent {r['box']}^3 sub-boxes "
+                                   f"(one per host core, {r['particles_per_box']} particles each)",
+                       "parallelism": f"{r['procs']} processes"},
+            "cpu_baseline": {"value": r["particle_steps_per_s"], "unit": "particle-steps/s", "cores": r["procs"],
+                             "kind": r["kind"], "sample": f"{r['procs']} x {r['box']}^3 boxes x {r['steps']} steps"},
+            "e2e": {"value": r["particle_steps_per_s"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = local
+    # one stream for torch (generation) and the library (qp_set_stream), so
+    # that the library's copies are ordered after the generating kernels
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    case.seed = 1234 + rank
+
+    peak, peak_kind = hbm_peak()
+    results = {}
+    for prec in (["fp64"] if args.no_mixed else ["fp64", "mixed"]):
+        reg = build_region(case, prec, dev)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t = time_region(reg, args.steps, args.warmup, dev)
+        f_end = torch.empty((12, case.nx, case.ny, case.nz), dtype=torch.float64, device=f"cuda:{dev}")
+        reg._check(reg.lib.qp_dump_fields(reg.h, _tp(f_end)))
+        t["fields_end"] = f_end[:6].clone()
+        del f_end
+        reg.close()
+        del reg
+        torch.cuda.empty_cache()
+        ms = t["ms"]
+        if dist:
+            x = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            ms = float(x.item())
+            y = torch.tensor([float(t["pushed"])], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(y)
+            pushed_all = float(y.item())
+        else:
+            pushed_all = float(t["pushed"])
+        bp, bc = BYTES[prec]
+        np_avg = t["pushed"] / t["steps"]
+        push_ms = t["phase_ms"][0] / t["steps"]
+        achieved = np_avg * bp / (push_ms * 1e-3) / 1e9
+        d = t["diags"]
+        w0, w1 = total_energy(d[0]), total_energy(d[-1])
+        results[prec] = {
+            "value": pushed_all / (ms * 1e-3),
+            "cell_updates_per_s": world * nc * t["steps"] / (ms * 1e-3),
+            "ms_per_step": ms / t["steps"],
+            "gpu_launches": t["launches"],
+            "phase_ms_per_step": {k: v / t["steps"] for k, v in zip(("push_deposit", "rebin", "fields", "diag"),
+                                                                     t["phase_ms"])},
+            "roofline": {"kernel": "push_deposit (k_push64)" if prec == "fp64" else "push_deposit (k_push32)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": np_avg * bp},
+            "step_roofline_frac": (np_avg * bp + nc * bc) / (ms * 1e-3 / t["steps"]) / 1e9 / peak,
+            "energy_drift": (w1 - w0) / w0 if w0 else None,
+            "drift_steps": len(d),
+            "clocks": t["clocks"],
+            "fields_end": t["fields_end"],
+            "particles": t["n_after"],
+        }
+    # mixed vs FP64 field error after the same steps from the same state
+    if "mixed" in results:
+        a, b = results["mixed"]["fields_end"], results["fp64"]["fields_end"]
+        results["mixed"]["field_rel_l2_vs_fp64"] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    for r in results.values():
+        r.pop("fields_end", None)
+
+    e2e = None
+    if not args.no_e2e:
+        host = pinned_host_state(case, dev)
+        e2e = e2e_run(case, "fp64", args.steps, dev, host)
+        del host
+        if dist:
+            x = torch.tensor([e2e["seconds"]], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            e2e["value"] = e2e["value"] * e2e["seconds"] / float(x.item()) * world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        c = run_cpu(args.config, 1, steps=args.cpu_steps, warm=2)
+        cpu = {"value": c["particle_steps_per_s"], "unit": "particle-steps/s", "cores": 1, "kind": c["kind"],
+               "sample": f"{args.config} physics on one 64^3 box ({c['particles_per_box']} particles), "
+                         f"{c['steps']} steps after 2 warm-up steps, {c['seconds']:.1f} s",
+               "cell_updates_per_s": c["cell_updates_per_s"], "host_cores_total": os.cpu_count()}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    f64 = results["fp64"]
+    line = {
+        "metric": metric, "value": f64["value"], "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": f64["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, generated on the GPU)",
+        "cell_updates_per_s": f64["cell_updates_per_s"],
+        "config": {"workload": f"{case.name}: {case.nx}x{case.ny}x{case.nz} cells, dx=lambda/{round(1 / case.dx_lambda)}, "
+                               f"dt=dx/2, {case.solver.upper()} + {case.pusher}, QED off, "
+                               f"{f64['particles']} electrons (4 ppc, 0.05 n_cr, 10 keV)",
+                   "l2_flush": "not needed: particle and field arrays (>70 GB) exceed L2",
+                   "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas (one region per GPU)"},
+        "roofline": f64["roofline"], "step_roofline_frac": f64["step_roofline_frac"],
+        "energy_drift": f64["energy_drift"], "drift_steps": f64["drift_steps"],
+        "phase_ms_per_step": f64["phase_ms_per_step"],
+        "clocks": f64["clocks"], "gpu_launches": f64["gpu_launches"],
+        "mixed": {k: v for k, v in results.get("mixed", {}).items() if k != "clocks"} or None,
+        "e2e": ({"value": e2e["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": e2e["h2d_bytes_per_step"],
+                 "d2h_bytes_per_step": e2e["d2h_bytes_per_step"], "seconds": e2e["seconds"],
+                 "includes": "qp_create, field + particle load from pinned host memory, K steps with per-step "
+                             "diagnostics to host, field dump to host"} if e2e else None),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -94,8 +94,8 @@ int qp_create(const qp_params* params, qp_handle** out);
 /* ~spatial_region (low-level.cpp:152-184). */
 int qp_destroy(qp_handle* h);
 
-/* Copy E and B from host planes (nx*ny*nz doubles each, k fastest); the
- * device copy is converted to the handle's precision.  Replaces the field
+/* Copy E and B from planes of nx*ny*nz doubles each (k fastest), in host
+ * or device memory; the device copy is converted to the handle's precision.  Replaces the field
  * initialisers writing spatial_region::ce/cb (init.cpp:6-400). */
 int qp_load_fields(qp_handle* h, const double* ex, const double* ey, const double* ez,
                    const double* bx, const double* by, const double* bz);
@@ -104,8 +104,8 @@ int qp_load_fields(qp_handle* h, const double* ex, const double* ey, const doubl
  * (main.cpp:2288-2289, advance.cpp:85-88, maxwell.cpp:135/338/532). */
 int qp_init_boundaries(qp_handle* h);
 
-/* Append n particles of one species from host arrays (cell units; chi may
- * be NULL).  Within a cell the given order becomes the traversal order;
+/* Append n particles of one species from host or device arrays (cell
+ * units; chi may be NULL).  Within a cell the given order becomes the traversal order;
  * particles of a later call precede those already in the cell, as head
  * insertion by spatial_region::place (plist.cpp:22-39) would put them.
  * Positions must lie in [0, n) per axis.  Replaces new_particle + place
@@ -123,7 +123,8 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag);
 /* Diagnostics of the last completed step. */
 int qp_get_diag(qp_handle* h, qp_diag* out);
 
-/* Copy fields to host: 12 planes E(3) B(3) J(3) Bbar(3), FP64. */
+/* Copy fields out (host or device memory): 12 planes E(3) B(3) J(3)
+ * Bbar(3), FP64. */
 int qp_dump_fields(qp_handle* h, double* out12);
 
 /* Live particle count of one species. */
@@ -151,6 +152,23 @@ int qp_set_stream(qp_handle* h, void* cuda_stream);
 /* Number of this library's kernel launches issued since the handle was
  * created (for launch accounting). */
 int qp_launch_count(qp_handle* h, int64_t* out);
+
+/* Device evaluation of the QED rate functions of mc.cpp:26-116 for n
+ * samples (host or device arrays).  in: 12 doubles per sample
+ * (e[3] b[3] u[3] g r chi); out: 5 per sample (chi(e,b,u,g), w(g,r,chi),
+ * r after w (w rescales r for chi <= 0.133), tilde_w(g,r,chi),
+ * mathcal_W(e,b)).  e_s = lambda_cm / 2.4263086e-10 (main.cpp:2276). */
+int qp_eval_qed_rates(int device, double lambda_cm, int64_t n, const double* in, double* out);
+
+/* Per-phase CUDA-event timing of qp_step on the handle's stream: enable
+ * (resets the totals) or disable.  No reference counterpart (the reference
+ * logs coarse times() wall clocks only, main.cpp:2228-2230). */
+int qp_set_timing(qp_handle* h, int enable);
+
+/* Accumulated milliseconds since qp_set_timing(h, 1): [0] particle push and
+ * current deposition, [1] rebin, [2] Maxwell solver + Bbar, [3] J reset and
+ * diagnostics; *steps = timed steps (nullable). */
+int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
 
 #ifdef __cplusplus
 }

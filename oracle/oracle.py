@@ -29,7 +29,20 @@ _DP = C.POINTER(C.c_double)
 _LP = C.POINTER(C.c_long)
 
 
+def _has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+        return " avx512f " in flags and " avx512vl " in flags and " avx512_fp16 " in flags
+    except OSError:
+        return False
+
+
 def lib_path(kind: str = "port", flavour: str = "parity") -> str:
+    if flavour == "fast" and _has_avx512():
+        v4 = lib_path(kind, "fast_v4")
+        if os.path.exists(v4):
+            return v4
     if kind == "ref":
         return os.path.join(HERE, "_ref", f"libquill_ref_{flavour}.so")
     return os.path.join(HERE, f"liboracle_{flavour}.so")

@@ -101,6 +101,9 @@ def load_library(path: str | None = None):
         "qp_synchronize": (C.c_int, [VP]),
         "qp_set_stream": (C.c_int, [VP, VP]),
         "qp_launch_count": (C.c_int, [VP, I64P]),
+        "qp_set_timing": (C.c_int, [VP, C.c_int]),
+        "qp_eval_qed_rates": (C.c_int, [C.c_int, D, I64, DP, DP]),
+        "qp_get_timing": (C.c_int, [VP, DP, I64P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -115,6 +118,18 @@ def _dp(a):
 
 
 PARTICLE_KEYS = ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")
+
+
+def eval_qed_rates(samples: np.ndarray, lambda_cm: float = 1e-4, device: int = 0) -> np.ndarray:
+    """Device evaluation of chi, w, r-after-w, tilde_w, vacuum W for rows of
+    (e[3] b[3] u[3] g r chi)."""
+    lib = load_library()
+    a = np.ascontiguousarray(samples, dtype=np.float64).reshape(-1, 12)
+    out = np.zeros((a.shape[0], 5))
+    r = lib.qp_eval_qed_rates(device, lambda_cm, a.shape[0], _dp(a), _dp(out))
+    if r != 0:
+        raise QPError(r, lib.qp_last_error(None).decode())
+    return out
 
 
 class Region:
@@ -228,6 +243,16 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_timing(self, enable: bool = True):
+        self._check(self.lib.qp_set_timing(self.h, int(bool(enable))))
+
+    def get_timing(self):
+        """(ms per phase [push, rebin, fields, diag], steps timed)."""
+        ms = np.zeros(4)
+        n = C.c_int64()
+        self._check(self.lib.qp_get_timing(self.h, _dp(ms), C.byref(n)))
+        return ms, n.value
 
     def launch_count(self) -> int:
         n = C.c_int64()

@@ -43,9 +43,32 @@ SolverCoef solver_coef(const qp_params& p) {
 
 void zero_planes_fp64(State& s, const ZeroPlane* zp, int n);
 void zero_planes_mixed(State& s, const ZeroPlane* zp, int n);
-int load_merge(State& s, int si, int64_t n_old, const int32_t* d_new_start, int32_t* d_perm_out);
+int load_merge(State& s, int si, int64_t slot0, const int32_t* d_new_start, int32_t* d_perm_out);
 
 static int n_arrays(const State& s) { return s.fp64 ? 9 : 10; }
+
+// New particles at slots [slot0, slot0 + n_new) of the current buffer, sorted
+// by cell (cells in d_cells, device): per-cell counts -> starts -> merged in
+// front of the particles already in each cell (head insertion order).
+static int merge_sorted_slots(State& s, int si, int64_t slot0, int64_t n_new, const int32_t* d_cells) {
+    Species& sp = s.sp[si];
+    const Grid gr = s.grid;
+    int32_t* nstart = nullptr;
+    int32_t* d_perm = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&nstart, (size_t)(gr.nc + 1) * sizeof(int32_t)));
+    QP_CUDA_CHECK(s, cudaMalloc(&d_perm, sp.cap * sizeof(int32_t)));
+    launch_histogram(s, d_cells, (int)n_new, sp.count);
+    exclusive_scan_i32(s, sp.count, nstart, gr.nc);
+    load_merge(s, si, slot0, nstart, d_perm);
+    QP_CUDA_CHECK(s, cudaGetLastError());
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    cudaFree(sp.perm);
+    sp.perm = d_perm;
+    cudaFree(nstart);
+    sp.n += n_new;
+    sp.slots = slot0 + n_new;
+    return QP_OK;
+}
 static size_t arr_elem(const State& s, int a) { return s.fp64 ? 8 : 4; }
 
 // Allocate (or grow, keeping contents) the particle arrays of a species.
@@ -99,6 +122,9 @@ static void free_state(State* s) {
         cudaFree(sp.cell_start);
         cudaFree(sp.cell_next);
         cudaFree(sp.count);
+        cudaFree(sp.born);
+        cudaFree(sp.born_fill);
+        cudaFree(sp.d_counter);
     }
     for (auto& sn : s->snap) {
         cudaFree(sn.fields);
@@ -110,6 +136,8 @@ static void free_state(State* s) {
     cudaFreeHost(s->h_diag);
     cudaFree(s->d_status);
     cudaFree(s->scan_tmp);
+    for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     s->stream = nullptr;
 }
@@ -123,6 +151,10 @@ struct qp_handle {
 using namespace qp;
 
 static thread_local std::string g_create_error;
+
+namespace qp {
+cudaError_t launch_qed_rates(int n, const double* d_in, double* d_out, double e_s, cudaStream_t st);
+}
 
 #define QP_H_CHECK(h)                              \
     do {                                           \
@@ -158,7 +190,16 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     if (p.precision < 0 || p.precision > 1) return bad("unknown precision");
     if (p.n_species < 0 || p.n_species > QP_MAX_SPECIES) return bad("n_species out of range");
     if (!(p.lambda_cm > 0)) return bad("lambda_cm must be positive");
-    if (p.qed) return bad("QED is not available in this build of the library");
+    if (p.qed) {
+        bool has_e = false, has_p = false, has_ph = false;
+        for (int i = 0; i < p.n_species; i++) {
+            has_e |= p.cmr[i] == -1;
+            has_p |= p.cmr[i] == 1;
+            has_ph |= p.cmr[i] == 0;
+        }
+        if (!(has_e && has_p && has_ph)) return bad("QED needs species with cmr -1, +1 and 0");
+        if (p.precision != QP_PREC_FP64) return bad("QED runs in FP64 precision");
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         g_create_error = "no CUDA device";
@@ -192,6 +233,15 @@ int qp_create(const qp_params* prm, qp_handle** out) {
         sp.cmr = p.cmr[i];
         sp.kind = p.cmr[i] == 0 ? KIND_PHOTON : (std::fabs(p.cmr[i]) == 1 ? KIND_LEPTON : KIND_ION);
         sp.ion_index = sp.kind == KIND_ION ? ion++ : -1;
+        if (sp.cmr == -1 && s.sp_e < 0) s.sp_e = i;
+        if (sp.cmr == 1 && s.sp_p < 0) s.sp_p = i;
+        if (sp.cmr == 0 && s.sp_ph < 0) s.sp_ph = i;
+        if (p.qed) {
+            if (e == cudaSuccess) e = cudaMalloc(&sp.born, nc * sizeof(int32_t));
+            if (e == cudaSuccess) e = cudaMalloc(&sp.born_fill, nc * sizeof(int32_t));
+            if (e == cudaSuccess) e = cudaMalloc(&sp.d_counter, sizeof(int));
+            if (e == cudaSuccess) e = cudaMemsetAsync(sp.d_counter, 0, sizeof(int), s.stream);
+        }
         e = cudaMalloc(&sp.cell_start, (nc + 1) * sizeof(int32_t));
         if (e == cudaSuccess) e = cudaMemsetAsync(sp.cell_start, 0, (nc + 1) * sizeof(int32_t), s.stream);
         if (e == cudaSuccess) e = cudaMalloc(&sp.cell_next, (nc + 1) * sizeof(int32_t));
@@ -246,6 +296,43 @@ int qp_synchronize(qp_handle* h) {
     return QP_OK;
 }
 
+int qp_eval_qed_rates(int device, double lambda_cm, int64_t n, const double* in, double* out) {
+    if (n < 0 || (n > 0 && (!in || !out)) || n > (int64_t)INT32_MAX / 12) return QP_ERR_ARG;
+    if (n == 0) return QP_OK;
+    if (cudaSetDevice(device) != cudaSuccess) return QP_ERR_CUDA;
+    double *din = nullptr, *dout = nullptr;
+    cudaError_t e = cudaMalloc(&din, n * 12 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&dout, n * 5 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(din, in, n * 12 * sizeof(double), cudaMemcpyDefault);
+    if (e == cudaSuccess) e = launch_qed_rates((int)n, din, dout, lambda_cm / 2.4263086e-10, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, n * 5 * sizeof(double), cudaMemcpyDefault);
+    cudaFree(din);
+    cudaFree(dout);
+    if (e != cudaSuccess) {
+        g_create_error = cudaGetErrorString(e);
+        return QP_ERR_CUDA;
+    }
+    return QP_OK;
+}
+
+int qp_set_timing(qp_handle* h, int enable) {
+    QP_H_CHECK(h);
+    State& s = h->st;
+    if (enable && !s.ev[0])
+        for (auto& e : s.ev) QP_CUDA_CHECK(s, cudaEventCreate(&e));
+    s.timing = enable != 0;
+    for (double& v : s.phase_ms) v = 0;
+    s.phase_steps = 0;
+    return QP_OK;
+}
+
+int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps) {
+    if (!h || !ms4) return QP_ERR_ARG;
+    for (int i = 0; i < 4; i++) ms4[i] = h->st.phase_ms[i];
+    if (steps) *steps = h->st.phase_steps;
+    return QP_OK;
+}
+
 int qp_launch_count(qp_handle* h, int64_t* out) {
     if (!h || !out) return QP_ERR_ARG;
     *out = h->st.launches;
@@ -259,17 +346,21 @@ int qp_load_fields(qp_handle* h, const double* ex, const double* ey, const doubl
     if (!ex || !ey || !ez || !bx || !by || !bz) { s.err = "null field plane"; return QP_ERR_ARG; }
     const size_t nc = (size_t)s.grid.nc;
     const double* src[6] = {ex, ey, ez, bx, by, bz};
+    // host or device planes (unified addressing decides the copy direction)
     if (s.fp64) {
         for (int a = 0; a < 6; a++)
-            QP_CUDA_CHECK(s, cudaMemcpyAsync((double*)s.fields + a * nc, src[a], nc * 8, cudaMemcpyHostToDevice, s.stream));
+            QP_CUDA_CHECK(s, cudaMemcpyAsync((double*)s.fields + a * nc, src[a], nc * 8, cudaMemcpyDefault, s.stream));
     } else {
-        std::vector<float> tmp(nc);
+        double* stage = nullptr;
+        QP_CUDA_CHECK(s, cudaMalloc(&stage, nc * 8));
         for (int a = 0; a < 6; a++) {
-            for (size_t c = 0; c < nc; c++) tmp[c] = (float)src[a][c];
-            QP_CUDA_CHECK(s, cudaMemcpyAsync((float*)s.fields + a * nc, tmp.data(), nc * 4, cudaMemcpyHostToDevice, s.stream));
-            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(stage, src[a], nc * 8, cudaMemcpyDefault, s.stream));
+            launch_f64_to_f32(s, stage, (float*)s.fields + a * nc, nc);
         }
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        cudaFree(stage);
     }
+    QP_CUDA_CHECK(s, cudaGetLastError());
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
     s.boundaries_done = false;
     return QP_OK;
@@ -305,6 +396,11 @@ int qp_init_boundaries(qp_handle* h) {
     return QP_OK;
 }
 
+// Host fallback for input that is not in cell order: gather to the host,
+// stable counting sort by cell (the given order is kept inside a cell) and
+// load again in sorted order.
+static int load_unsorted(qp_handle* h, int si, int64_t n, const double* const* src);
+
 int qp_load_particles(qp_handle* h, int si, int64_t n, const double* x, const double* y, const double* z,
                       const double* ux, const double* uy, const double* uz, const double* g, const double* q,
                       const double* chi) {
@@ -316,80 +412,154 @@ int qp_load_particles(qp_handle* h, int si, int64_t n, const double* x, const do
     if (!x || !y || !z || !ux || !uy || !uz || !g || !q) { s.err = "null particle array"; return QP_ERR_ARG; }
     Species& sp = s.sp[si];
     const Grid gr = s.grid;
-    const int64_t n_old = sp.n;
-    if (n_old + n >= (int64_t)INT32_MAX) { s.err = "particle count exceeds 2^31-1"; return QP_ERR_CAPACITY; }
-    // cells and a stable counting sort on the host
-    std::vector<int32_t> cell(n);
-    for (int64_t p = 0; p < n; p++) {
-        const double px = x[p], py = y[p], pz = z[p];
-        if (!(px >= 0 && px < gr.nx && py >= 0 && py < gr.ny && pz >= 0 && pz < gr.nz) ||
-            !std::isfinite(ux[p]) || !std::isfinite(uy[p]) || !std::isfinite(uz[p]) || !std::isfinite(g[p]) ||
-            !std::isfinite(q[p])) {
-            char b[160];
-            snprintf(b, sizeof b, "particle %lld outside the grid or not finite", (long long)p);
-            s.err = b;
-            return QP_ERR_CONFIG;
-        }
-        cell[p] = ((int)px * gr.ny + (int)py) * gr.nz + (int)pz;
-    }
-    std::vector<int32_t> start(gr.nc + 1, 0);
-    for (int64_t p = 0; p < n; p++) start[cell[p] + 1]++;
-    for (int c = 0; c < gr.nc; c++) start[c + 1] += start[c];
-    std::vector<int32_t> order(n);
-    {
-        std::vector<int32_t> fill(start.begin(), start.end() - 1);
-        for (int64_t p = 0; p < n; p++) order[fill[cell[p]]++] = (int32_t)p;
-    }
-    int r = ensure_capacity(s, si, n_old + n);
+    const int64_t slot0 = sp.slots;
+    if (slot0 + n >= (int64_t)INT32_MAX) { s.err = "particle count exceeds 2^31-1"; return QP_ERR_CAPACITY; }
+    int r = ensure_capacity(s, si, slot0 + n);
     if (r != QP_OK) return r;
+    const double* src[9] = {x, y, z, ux, uy, uz, g, q, chi};
     const int cur = sp.cur;
+    // scratch: cells (n), flags, first bad index, per-cell counts and starts
+    int32_t* cells = nullptr;
+    unsigned int* flags = nullptr;
+    int* first_bad = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&cells, n * sizeof(int32_t)));
+    QP_CUDA_CHECK(s, cudaMalloc(&flags, sizeof(unsigned int) + sizeof(int)));
+    first_bad = (int*)(flags + 1);
+    QP_CUDA_CHECK(s, cudaMemsetAsync(flags, 0, sizeof(unsigned int), s.stream));
+    QP_CUDA_CHECK(s, cudaMemsetAsync(first_bad, 0x7f, sizeof(int), s.stream));
+    double* stage = nullptr;
     if (s.fp64) {
-        const double* src[9] = {x, y, z, ux, uy, uz, g, q, chi};
-        std::vector<double> tmp(n);
+        // copy straight into the free slots, then validate in place
         for (int a = 0; a < 9; a++) {
             if (!sp.buf[cur][a]) continue;
-            for (int64_t t = 0; t < n; t++) tmp[t] = src[a] ? src[a][order[t]] : 0.0;
-            QP_CUDA_CHECK(s, cudaMemcpyAsync((double*)sp.buf[cur][a] + n_old, tmp.data(), n * 8, cudaMemcpyHostToDevice, s.stream));
-            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            double* dst = (double*)sp.buf[cur][a] + slot0;
+            if (src[a]) QP_CUDA_CHECK(s, cudaMemcpyAsync(dst, src[a], n * 8, cudaMemcpyDefault, s.stream));
+            else QP_CUDA_CHECK(s, cudaMemsetAsync(dst, 0, n * 8, s.stream));
         }
+        const double* st[8];
+        for (int a = 0; a < 8; a++) st[a] = (const double*)sp.buf[cur][a] + slot0;
+        launch_load_cells(s, st, (int)n, cells, flags, first_bad, 0);
     } else {
-        std::vector<int32_t> tc(n);
-        std::vector<float> tmp(n);
-        for (int64_t t = 0; t < n; t++) tc[t] = cell[order[t]];
-        QP_CUDA_CHECK(s, cudaMemcpyAsync((int32_t*)sp.buf[cur][0] + n_old, tc.data(), n * 4, cudaMemcpyHostToDevice, s.stream));
-        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-        const double* pos[3] = {x, y, z};
-        for (int a = 0; a < 3; a++) {
-            for (int64_t t = 0; t < n; t++) {
-                const double v = pos[a][order[t]];
-                float o = (float)(v - std::floor(v));
-                if (o >= 1.0f) o = 0.99999994f;
-                tmp[t] = o;
+        const int64_t CH = std::min<int64_t>(n, 1 << 24);
+        QP_CUDA_CHECK(s, cudaMalloc(&stage, CH * 9 * sizeof(double)));
+        PStore32 dst;
+        dst.cell = (int32_t*)sp.buf[cur][0];
+        float** pd[9] = {&dst.ox, &dst.oy, &dst.oz, &dst.ux, &dst.uy, &dst.uz, &dst.g, &dst.q, &dst.chi};
+        for (int a = 0; a < 9; a++) *pd[a] = (float*)sp.buf[cur][1 + a];
+        for (int64_t c0 = 0; c0 < n; c0 += CH) {
+            const int64_t m = std::min<int64_t>(CH, n - c0);
+            const double* st[9];
+            for (int a = 0; a < 9; a++) {
+                double* d = stage + a * CH;
+                if (src[a]) QP_CUDA_CHECK(s, cudaMemcpyAsync(d, src[a] + c0, m * 8, cudaMemcpyDefault, s.stream));
+                else QP_CUDA_CHECK(s, cudaMemsetAsync(d, 0, m * 8, s.stream));
+                st[a] = d;
             }
-            QP_CUDA_CHECK(s, cudaMemcpyAsync((float*)sp.buf[cur][1 + a] + n_old, tmp.data(), n * 4, cudaMemcpyHostToDevice, s.stream));
-            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-        }
-        const double* src[6] = {ux, uy, uz, g, q, chi};
-        for (int a = 0; a < 6; a++) {
-            if (!sp.buf[cur][4 + a]) continue;
-            for (int64_t t = 0; t < n; t++) tmp[t] = src[a] ? (float)src[a][order[t]] : 0.0f;
-            QP_CUDA_CHECK(s, cudaMemcpyAsync((float*)sp.buf[cur][4 + a] + n_old, tmp.data(), n * 4, cudaMemcpyHostToDevice, s.stream));
-            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            launch_load_cells(s, st, (int)m, cells, flags, first_bad, (int)c0);
+            launch_to_mixed(s, st, (int)m, dst, (int)(slot0 + c0));
         }
     }
-    // merge in front of the old particles of each cell
-    int32_t* d_new_start = nullptr;
-    int32_t* d_perm = nullptr;
-    QP_CUDA_CHECK(s, cudaMalloc(&d_new_start, (gr.nc + 1) * sizeof(int32_t)));
-    QP_CUDA_CHECK(s, cudaMalloc(&d_perm, sp.cap * sizeof(int32_t)));
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(d_new_start, start.data(), (gr.nc + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s.stream));
-    load_merge(s, si, n_old, d_new_start, d_perm);
+    launch_check_sorted(s, cells, (int)n, flags);
+    unsigned int hf[2] = {0, 0};
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(hf, flags, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s.stream));
     QP_CUDA_CHECK(s, cudaGetLastError());
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    cudaFree(sp.perm);
-    sp.perm = d_perm;
-    cudaFree(d_new_start);
-    sp.n = n_old + n;
+    if (stage) cudaFree(stage);
+    auto release = [&]() { cudaFree(cells); cudaFree(flags); };
+    if (hf[0] & 1) {
+        release();
+        char b[160];
+        snprintf(b, sizeof b, "particle %d outside the grid [0, n) or not finite", (int)hf[1]);
+        s.err = b;
+        return QP_ERR_CONFIG;
+    }
+    if (hf[0] & 2) {
+        release();
+        return load_unsorted(h, si, n, src);
+    }
+    int rm = merge_sorted_slots(s, si, slot0, n, cells);
+    release();
+    return rm;
+}
+
+static int load_unsorted(qp_handle* h, int si, int64_t n, const double* const* src) {
+    State& s = h->st;
+    const Grid gr = s.grid;
+    std::vector<std::vector<double>> a(9);
+    for (int k = 0; k < 9; k++) {
+        if (!src[k]) continue;
+        a[k].resize(n);
+        QP_CUDA_CHECK(s, cudaMemcpy(a[k].data(), src[k], n * 8, cudaMemcpyDefault));
+    }
+    std::vector<int32_t> cell(n);
+    for (int64_t p = 0; p < n; p++) cell[p] = ((int)a[0][p] * gr.ny + (int)a[1][p]) * gr.nz + (int)a[2][p];
+    std::vector<int64_t> start(gr.nc + 1, 0);
+    for (int64_t p = 0; p < n; p++) start[cell[p] + 1]++;
+    for (int c = 0; c < gr.nc; c++) start[c + 1] += start[c];
+    std::vector<int64_t> order(n);
+    for (int64_t p = 0; p < n; p++) order[start[cell[p]]++] = p;
+    std::vector<std::vector<double>> b(9);
+    const double* ptr[9] = {nullptr};
+    for (int k = 0; k < 9; k++) {
+        if (a[k].empty()) continue;
+        b[k].resize(n);
+        for (int64_t t = 0; t < n; t++) b[k][t] = a[k][order[t]];
+        ptr[k] = b[k].data();
+    }
+    return qp_load_particles(h, si, n, ptr[0], ptr[1], ptr[2], ptr[3], ptr[4], ptr[5], ptr[6], ptr[7], ptr[8]);
+}
+
+// Before a QED step: make room for every particle a push can create (a
+// photon per lepton, a pair per photon), then birth_from_vacuum: pairs
+// written to free slots of the current e-/e+ buffers, sorted by cell on the
+// host (they are rare) and merged at the head of their cells.
+static int qed_prepare(State& s) {
+    const int e = s.sp_e, p = s.sp_p, ph = s.sp_ph;
+    int64_t nlep = 0;
+    for (auto& sp : s.sp)
+        if (sp.kind == KIND_LEPTON) nlep += sp.n;
+    const int64_t nph = s.sp[ph].n;
+    int r;
+    if ((r = ensure_capacity(s, ph, std::max(s.sp[ph].slots, nph + nlep) + 1)) != QP_OK) return r;
+    if ((r = ensure_capacity(s, e, std::max(s.sp[e].slots, s.sp[e].n + nph) + 1024)) != QP_OK) return r;
+    if ((r = ensure_capacity(s, p, std::max(s.sp[p].slots, s.sp[p].n + nph) + 1024)) != QP_OK) return r;
+    for (auto& sp : s.sp)
+        if (sp.d_counter) QP_CUDA_CHECK(s, cudaMemsetAsync(sp.d_counter, 0, sizeof(int), s.stream));
+    launch_vacuum_fp64(s);
+    int kv[2] = {0, 0};
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(&kv[0], s.sp[e].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(&kv[1], s.sp[p].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    const int who[2] = {e, p};
+    for (int w = 0; w < 2; w++) {
+        Species& sp = s.sp[who[w]];
+        const int64_t k = std::min<int64_t>(kv[w], sp.cap - sp.slots);
+        if (k <= 0) continue;
+        const int64_t slot0 = sp.slots;
+        std::vector<int32_t> cells(k);
+        QP_CUDA_CHECK(s, cudaMemcpy(cells.data(), sp.newcell + slot0, k * 4, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> order(k);
+        for (int64_t t = 0; t < k; t++) order[t] = t;
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cells[a] < cells[b]; });
+        std::vector<double> tmp(k), srt(k);
+        for (int a = 0; a < 9; a++) {
+            if (!sp.buf[sp.cur][a]) continue;
+            double* d = (double*)sp.buf[sp.cur][a] + slot0;
+            QP_CUDA_CHECK(s, cudaMemcpy(tmp.data(), d, k * 8, cudaMemcpyDeviceToHost));
+            for (int64_t t = 0; t < k; t++) srt[t] = tmp[order[t]];
+            QP_CUDA_CHECK(s, cudaMemcpy(d, srt.data(), k * 8, cudaMemcpyHostToDevice));
+        }
+        std::vector<int32_t> sc(k);
+        for (int64_t t = 0; t < k; t++) sc[t] = cells[order[t]];
+        int32_t* dc = nullptr;
+        QP_CUDA_CHECK(s, cudaMalloc(&dc, k * 4));
+        QP_CUDA_CHECK(s, cudaMemcpy(dc, sc.data(), k * 4, cudaMemcpyHostToDevice));
+        r = merge_sorted_slots(s, who[w], slot0, k, dc);
+        cudaFree(dc);
+        if (r != QP_OK) return r;
+    }
+    for (auto& sp : s.sp)
+        if (sp.d_counter) QP_CUDA_CHECK(s, cudaMemsetAsync(sp.d_counter, 0, sizeof(int), s.stream));
     return QP_OK;
 }
 
@@ -430,20 +600,38 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
     if (nsteps < 0) { s.err = "negative step count"; return QP_ERR_ARG; }
     const size_t nc = (size_t)s.grid.nc;
     for (int l = 0; l < nsteps; l++) {
+        if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[0], s.stream));
         // padvance (advance.cpp:90-387): J = 0, push and deposit every species
         QP_CUDA_CHECK(s, cudaMemsetAsync((char*)s.fields + 6 * nc * s.field_elem, 0, 3 * nc * s.field_elem, s.stream));
         QP_CUDA_CHECK(s, cudaMemsetAsync(s.d_diag, 0, sizeof(DiagAccum), s.stream));
-        for (size_t i = 0; i < s.sp.size(); i++) {
-            if (s.fp64) launch_push_fp64(s, (int)i, external_bz);
-            else launch_push_mixed(s, (int)i, external_bz);
+        if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[1], s.stream));
+        std::vector<int> born(s.sp.size(), 0);
+        if (s.prm.qed) {
+            int r = qed_prepare(s);
+            if (r != QP_OK) return r;
+            for (size_t i = 0; i < s.sp.size(); i++) launch_push_fp64_qed(s, (int)i, external_bz);
+            QP_CUDA_CHECK(s, cudaGetLastError());
+            for (size_t i = 0; i < s.sp.size(); i++)
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(&born[i], s.sp[i].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            for (size_t i = 0; i < s.sp.size(); i++)
+                born[i] = (int)std::min<int64_t>(born[i], s.sp[i].cap - s.sp[i].n);
+        } else {
+            for (size_t i = 0; i < s.sp.size(); i++) {
+                if (s.fp64) launch_push_fp64(s, (int)i, external_bz);
+                else launch_push_mixed(s, (int)i, external_bz);
+            }
         }
         QP_CUDA_CHECK(s, cudaGetLastError());
+        if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[2], s.stream));
         for (size_t i = 0; i < s.sp.size(); i++)
-            if (s.sp[i].n > 0) rebin(s, (int)i);
+            if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i]);
         QP_CUDA_CHECK(s, cudaGetLastError());
+        if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[3], s.stream));
         // compute_energy field term on E, B before fadvance (main.cpp:2327)
         if (s.fp64) launch_field_energy_fp64(s);
         else launch_field_energy_mixed(s);
+        if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[4], s.stream));
         // fadvance: half B, E, half B, Bbar (maxwell.cpp:10-22, advance.cpp:13-18)
         for (int ph = 0; ph < 4; ph++) {
             if (s.fp64) launch_fields_fp64(s, ph == 2 ? 0 : ph);
@@ -454,6 +642,24 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
         unsigned int st = 0;
         QP_CUDA_CHECK(s, cudaMemcpyAsync(&st, s.d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s.stream));
         QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        if (s.timing) {
+            cudaEvent_t end = nullptr;
+            QP_CUDA_CHECK(s, cudaEventCreate(&end));
+            QP_CUDA_CHECK(s, cudaEventRecord(end, s.stream));
+            QP_CUDA_CHECK(s, cudaEventSynchronize(end));
+            float t01, t12, t23, t34, t4e;
+            cudaEventElapsedTime(&t01, s.ev[0], s.ev[1]);
+            cudaEventElapsedTime(&t12, s.ev[1], s.ev[2]);
+            cudaEventElapsedTime(&t23, s.ev[2], s.ev[3]);
+            cudaEventElapsedTime(&t34, s.ev[3], s.ev[4]);
+            cudaEventElapsedTime(&t4e, s.ev[4], end);
+            cudaEventDestroy(end);
+            s.phase_ms[0] += t12;
+            s.phase_ms[1] += t23;
+            s.phase_ms[2] += t4e;
+            s.phase_ms[3] += t01 + t34;
+            s.phase_steps++;
+        }
         fill_diag(s, &s.last_diag);
         s.last_diag.status = st ? (st & ST_NAN ? QP_ERR_NAN : (st & ST_CAPACITY ? QP_ERR_CAPACITY : QP_ERR_CONFIG)) : QP_OK;
         s.have_diag = true;
@@ -481,15 +687,21 @@ int qp_dump_fields(qp_handle* h, double* out) {
     State& s = h->st;
     if (!out) return QP_ERR_ARG;
     const size_t nc = (size_t)s.grid.nc;
+    cudaPointerAttributes at{};
+    const bool dev = cudaPointerGetAttributes(&at, out) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
     if (s.fp64) {
-        QP_CUDA_CHECK(s, cudaMemcpyAsync(out, s.fields, 12 * nc * 8, cudaMemcpyDeviceToHost, s.stream));
-        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(out, s.fields, 12 * nc * 8, cudaMemcpyDefault, s.stream));
+    } else if (dev) {
+        launch_f32_to_f64(s, (const float*)s.fields, out, 12 * nc);
     } else {
         std::vector<float> tmp(12 * nc);
         QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), s.fields, 12 * nc * 4, cudaMemcpyDeviceToHost, s.stream));
         QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
         for (size_t c = 0; c < 12 * nc; c++) out[c] = tmp[c];
     }
+    QP_CUDA_CHECK(s, cudaGetLastError());
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
     return QP_OK;
 }
 
@@ -575,12 +787,14 @@ int qp_checkpoint(qp_handle* h, int slot) {
     sn.arrays.assign(s.sp.size(), std::vector<void*>(11, nullptr));
     sn.n.assign(s.sp.size(), 0);
     sn.cap.assign(s.sp.size(), 0);
+    sn.slots.assign(s.sp.size(), 0);
     sn.cell_start.resize(s.sp.size(), nullptr);
     for (size_t i = 0; i < s.sp.size(); i++) {
         Species& sp = s.sp[i];
         const int64_t cap = sp.cap;
         sn.cap[i] = cap;
         sn.n[i] = sp.n;
+        sn.slots[i] = sp.slots;
         if (cap > 0) {
             for (int a = 0; a < 10; a++) {
                 if (!sp.buf[sp.cur][a]) continue;
@@ -621,6 +835,7 @@ int qp_restore(qp_handle* h, int slot) {
         }
         QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.cell_start, sn.cell_start[i], (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
         sp.n = sn.n[i];
+        sp.slots = sn.slots[i];
     }
     s.step_index = sn.step_index;
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));

@@ -53,7 +53,8 @@ struct Species {
     int kind = KIND_LEPTON;
     int ion_index = -1;
     int64_t n = 0;       // live particles
-    int64_t cap = 0;     // slots
+    int64_t slots = 0;   // slots of buf[cur] that perm may reference
+    int64_t cap = 0;     // allocated slots
     // two buffers of each array; `cur` holds the particles in the layout of
     // the previous push, read through `perm` in traversal order
     void* buf[2][10] = {{nullptr}};
@@ -63,6 +64,9 @@ struct Species {
     int32_t* cell_start = nullptr; // nc+1, traversal order at the start of a step
     int32_t* cell_next = nullptr;  // nc+1, traversal order after the rebin
     int32_t* count = nullptr;      // nc, rebin histogram
+    int32_t* born = nullptr;       // nc, particles born per cell in a push (QED)
+    int32_t* born_fill = nullptr;  // nc, placement counters for the born
+    int* d_counter = nullptr;      // device append counter (QED)
 };
 
 struct DiagAccum {
@@ -92,13 +96,20 @@ struct State {
     int64_t launches = 0;
     int64_t step_index = 0;
     bool boundaries_done = false;
+    int sp_e = -1, sp_p = -1, sp_ph = -1;  // QED species (cmr -1, +1, 0)
     std::string err;
+    // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
+    // diagnostics + J reset)
+    bool timing = false;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double phase_ms[4] = {0, 0, 0, 0};
+    int64_t phase_steps = 0;
     // checkpoints (device-resident copies)
     struct Snap {
         bool valid = false;
         void* fields = nullptr;
         std::vector<std::vector<void*>> arrays;  // per species, 10 arrays
-        std::vector<int64_t> n, cap;
+        std::vector<int64_t> n, cap, slots;
         std::vector<int32_t*> cell_start;
         int64_t step_index = 0;
     } snap[4];
@@ -108,6 +119,8 @@ struct State {
 void launch_fields_fp64(State& s, int phase);          // phase: 0 half B, 1 E, 2 half B, 3 Bbar
 void launch_init_boundaries_fp64(State& s);
 void launch_push_fp64(State& s, int species, double external_bz);
+int launch_push_fp64_qed(State& s, int species, double external_bz);
+int launch_vacuum_fp64(State& s);
 void launch_field_energy_fp64(State& s);
 
 // ---- mixed precision (qp_mixed.cu) ----
@@ -119,10 +132,15 @@ void launch_field_energy_mixed(State& s);
 // ---- rebin and scans (qp_rebin.cu) ----
 // Rebin after a push: count -> scan -> assign; leaves the new traversal
 // order in sp.perm / sp.cell_next and swaps buffers.  Returns the new count.
-int64_t rebin(State& s, int species);
-// Sort freshly loaded particles (n_new appended at the tail of buf[cur],
-// cell ids in newcell) into traversal order; returns QP_OK or an error.
-int load_sort(State& s, int species, int64_t n_old, int64_t n_new, const int32_t* d_cells_new);
+int64_t rebin(State& s, int species, int64_t born);
+// Loading (qp_load.cu)
+void launch_load_cells(State& s, const double* const* a, int n, int32_t* cells, unsigned int* flags,
+                       int* first_bad, int base);
+void launch_check_sorted(State& s, const int32_t* cells, int n, unsigned int* flags);
+void launch_histogram(State& s, const int32_t* cells, int n, int32_t* count);
+void launch_to_mixed(State& s, const double* const* a, int n, PStore32 dst, int at);
+void launch_f64_to_f32(State& s, const double* a, float* b, size_t n);
+void launch_f32_to_f64(State& s, const float* a, double* b, size_t n);
 void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n);
 
 }  // namespace qp

@@ -119,4 +119,22 @@ struct PushArgs {
     DiagAccum* diag;
 };
 
+// Destination of particles born during a push (QED): slots
+// [base, cap) of the target species' output buffer, claimed with *counter.
+template <typename Store>
+struct AppendTarget {
+    Store dst;
+    int32_t* newcell;
+    int* counter;
+    int base;
+    int cap;
+    int sp;  // species index (diagnostics)
+};
+
+struct QedArgs {
+    double e_s;
+    uint32_t key0, key1;  // random stream key (seed)
+    uint32_t step;        // step counter
+};
+
 }  // namespace qp

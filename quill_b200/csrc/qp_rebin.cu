@@ -42,12 +42,13 @@ __global__ void __launch_bounds__(256) k_rebin_count(Grid g, const int32_t* __re
 __global__ void __launch_bounds__(256) k_rebin_assign(Grid g, const int32_t* __restrict__ cs,
                                                       const int32_t* __restrict__ newcell,
                                                       const int32_t* __restrict__ start,
+                                                      const int32_t* __restrict__ born,
                                                       int32_t* __restrict__ perm) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nc) return;
     const int k = c % g.nz, j = (c / g.nz) % g.ny, i = c / g.nynz;
     if (!inside(g, i, j, k)) return;
-    int pos = start[c];
+    int pos = start[c] + (born ? born[c] : 0);
     const int end = start[c + 1];
     if (pos == end) return;
     for (int di = -1; di <= 1; di++)
@@ -62,6 +63,31 @@ __global__ void __launch_bounds__(256) k_rebin_assign(Grid g, const int32_t* __r
     const int e = __ldg(cs + c + 1);
     for (int p = __ldg(cs + c); p < e; p++)
         if (__ldg(newcell + p) == c) perm[pos++] = p;
+}
+
+// Particles born during this step's pushes (QED) sit at slots [n, n + A) of
+// the output buffer with their cell in newcell.  They go first in their cell
+// (they were head-inserted when born, plist.cpp:22-39); among themselves in
+// claim order.
+__global__ void k_born_hist(const int32_t* __restrict__ newcell, int n, int A, int32_t* __restrict__ born) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A) return;
+    const int c = newcell[n + t];
+    if (c >= 0) atomicAdd(born + c, 1);
+}
+
+__global__ void k_add_i32_inplace(int32_t* __restrict__ a, const int32_t* __restrict__ b, int n) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < n) a[x] += b[x];
+}
+
+__global__ void k_born_place(const int32_t* __restrict__ newcell, int n, int A, const int32_t* __restrict__ start,
+                             int32_t* __restrict__ fill, int32_t* __restrict__ perm) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A) return;
+    const int c = newcell[n + t];
+    if (c < 0) return;
+    perm[start[c] + atomicAdd(fill + c, 1)] = n + t;
 }
 
 // ---------------------------------------------------------------- scan ----
@@ -151,16 +177,31 @@ void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n) {
     s.launches += 3;
 }
 
-int64_t rebin(State& s, int si) {
+int64_t rebin(State& s, int si, int64_t born) {
     Species& sp = s.sp[si];
     const Grid g = s.grid;
     const int nb = (g.nc + 255) / 256;
+    const int n = (int)sp.n, A = (int)born;
     k_rebin_count<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.count);
+    s.launches++;
+    if (A > 0) {
+        cudaMemsetAsync(sp.born, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
+        cudaMemsetAsync(sp.born_fill, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
+        k_born_hist<<<(A + 255) / 256, 256, 0, s.stream>>>(sp.newcell, n, A, sp.born);
+        k_add_i32_inplace<<<nb, 256, 0, s.stream>>>(sp.count, sp.born, g.nc);
+        s.launches += 2;
+    }
     exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc);
-    k_rebin_assign<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.cell_next, sp.perm);
-    s.launches += 2;
+    k_rebin_assign<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.cell_next, A > 0 ? sp.born : nullptr,
+                                             sp.perm);
+    s.launches++;
+    if (A > 0) {
+        k_born_place<<<(A + 255) / 256, 256, 0, s.stream>>>(sp.newcell, n, A, sp.cell_next, sp.born_fill, sp.perm);
+        s.launches++;
+    }
     std::swap(sp.cell_start, sp.cell_next);
     sp.cur = 1 - sp.cur;
+    sp.slots = (int64_t)n + A;  // the push wrote traversal positions [0, n), births after them
     int32_t total = 0;
     cudaMemcpyAsync(&total, sp.cell_start + g.nc, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream);
     cudaStreamSynchronize(s.stream);
@@ -168,18 +209,18 @@ int64_t rebin(State& s, int si) {
     return total;
 }
 
-// Merge freshly uploaded particles (slots [n_old, n_old + n_new) of the
+// Merge freshly uploaded particles (slots [slot0, slot0 + n_new) of the
 // current buffer, already sorted by cell with given order inside a cell,
 // per-cell counts in new_count) in front of the old particles of each cell.
 __global__ void __launch_bounds__(256) k_load_merge(Grid g, const int32_t* __restrict__ old_start,
                                                     const int32_t* __restrict__ new_start,
                                                     const int32_t* __restrict__ merged_start,
                                                     const int32_t* __restrict__ old_perm,
-                                                    int32_t* __restrict__ perm, int n_old) {
+                                                    int32_t* __restrict__ perm, int slot0) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nc) return;
     int pos = merged_start[c];
-    for (int p = new_start[c]; p < new_start[c + 1]; p++) perm[pos++] = n_old + p;
+    for (int p = new_start[c]; p < new_start[c + 1]; p++) perm[pos++] = slot0 + p;
     for (int p = old_start[c]; p < old_start[c + 1]; p++) perm[pos++] = old_perm[p];
 }
 
@@ -190,14 +231,14 @@ __global__ void k_add_i32(const int32_t* a, const int32_t* b, int32_t* out, int 
 
 // new_start: exclusive scan of the new particles' per-cell counts (device,
 // nc+1); scratch: nc+1 ints.  perm_out receives the merged permutation.
-int load_merge(State& s, int si, int64_t n_old, const int32_t* d_new_start, int32_t* d_perm_out) {
+int load_merge(State& s, int si, int64_t slot0, const int32_t* d_new_start, int32_t* d_perm_out) {
     Species& sp = s.sp[si];
     const Grid g = s.grid;
     const int nb = (g.nc + 255) / 256;
     k_add_i32<<<nb, 256, 0, s.stream>>>(sp.cell_start, d_new_start, sp.count, g.nc);
     exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc);
     k_load_merge<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, d_new_start, sp.cell_next, sp.perm, d_perm_out,
-                                           (int)n_old);
+                                           (int)slot0);
     s.launches += 2;
     std::swap(sp.cell_start, sp.cell_next);
     return QP_OK;

@@ -213,3 +213,93 @@ def build(case: Case):
     fields = make_fields(case)
     parts = [make_particles(case, sp, rng) for sp in case.species]
     return fields, parts
+
+
+# ---------------------------------------------------------------------------
+# Device-side generation (torch on the GPU) of the same states, for sizes
+# where host generation would dominate (the 512^3 configuration holds 5.4e8
+# particles).  Same formulas as make_fields / make_particles; the random
+# streams differ from numpy's.
+# ---------------------------------------------------------------------------
+
+def make_fields_torch(case: Case, device="cuda"):
+    import torch
+    nx, ny, nz = case.nx, case.ny, case.nz
+    z0 = lambda: torch.zeros((nx, ny, nz), dtype=torch.float64, device=device)
+    f = {k: z0() for k in ("ex", "ey", "ez", "bx", "by", "bz")}
+    L = case.laser
+    if L is None:
+        return f
+    dx = case.dx
+    xs = 0.849 * L.fwhm_lambda * TWO_PI * 2 * math.sqrt(TWO_PI) / 3.0
+    xs = min(xs, 0.45 * nx * dx)
+    w = L.waist_lambda * TWO_PI
+    xc = xs
+    i = torch.arange(nx, dtype=torch.float64, device=device)
+    j = torch.arange(ny, dtype=torch.float64, device=device)
+    k = torch.arange(nz, dtype=torch.float64, device=device)
+
+    def wave(xp, phase):
+        xpos = xp * dx
+        a = (xpos - xc) / xs
+        env = torch.where(a.abs() < 1, torch.cos(0.5 * math.pi * a) ** 2, torch.zeros_like(a))
+        return L.a0 * env * torch.cos(xpos - xc + phase)
+
+    def trans(jp, kp):
+        ry = ((jp - ny / 2) * dx) ** 2
+        rz = ((kp - nz / 2) * dx) ** 2
+        return torch.exp(-(ry[:, None] + rz[None, :]) / (w * w))
+
+    pol = [1.0, 0.0] if L.polarization == "linear" else [1.0 / math.sqrt(2), 1.0 / math.sqrt(2)]
+    t_ey = trans(j + 0.5, k)
+    f["ey"] = pol[0] * wave(i, 0.0)[:, None, None] * t_ey[None]
+    f["bz"] = pol[0] * wave(i + 0.5, 0.0)[:, None, None] * t_ey[None]
+    if pol[1]:
+        t_ez = trans(j, k + 0.5)
+        f["ez"] = pol[1] * wave(i, -0.5 * math.pi)[:, None, None] * t_ez[None]
+        f["by"] = -pol[1] * wave(i + 0.5, -0.5 * math.pi)[:, None, None] * t_ez[None]
+    if L.counter:
+        for key, sgn in (("ey", 1), ("ez", 1), ("by", -1), ("bz", -1)):
+            f[key] = f[key] + sgn * torch.flip(f[key], dims=(0,))
+    return {kk: v.contiguous() for kk, v in f.items()}
+
+
+def particle_chunks_torch(case: Case, sp: SpeciesSpec, planes_per_chunk=32, device="cuda", seed=0):
+    """Yield particle dicts (torch float64 tensors on the device) for groups
+    of x-planes, in traversal order, ppc per occupied cell."""
+    import torch
+    nx, ny, nz = case.nx, case.ny, case.nz
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    jj, kk = torch.meshgrid(torch.arange(1, ny - 2, device=device), torch.arange(1, nz - 2, device=device),
+                            indexing="ij")
+    jj, kk = jj.reshape(-1), kk.reshape(-1)
+    for i0 in range(1, nx - 2, planes_per_chunk):
+        i1 = min(i0 + planes_per_chunk, nx - 2)
+        ii = torch.arange(i0, i1, device=device).repeat_interleave(jj.numel())
+        cj = jj.repeat(i1 - i0)
+        ck = kk.repeat(i1 - i0)
+        n = torch.as_tensor(_profile(sp, case, ii.cpu().numpy(), cj.cpu().numpy(), ck.cpu().numpy()),
+                            device=device) if sp.density != "uniform" else None
+        if n is not None:
+            occ = n > 0
+            ii, cj, ck, n = ii[occ], cj[occ], ck[occ], n[occ]
+        m = ii.numel() * sp.ppc
+        if m == 0:
+            continue
+        rep = lambda t: t.repeat_interleave(sp.ppc).to(torch.float64)
+        x = rep(ii) + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
+        y = rep(cj) + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
+        z = rep(ck) + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
+        if sp.theta > 0:
+            s = math.sqrt(sp.theta)
+            ux, uy, uz = (torch.randn(m, generator=gen, device=device, dtype=torch.float64) * s for _ in range(3))
+        else:
+            ux = torch.zeros(m, device=device, dtype=torch.float64)
+            uy = torch.zeros_like(ux)
+            uz = torch.zeros_like(ux)
+        g = torch.sqrt(1 + ux * ux + uy * uy + uz * uz) if sp.cmr != 0 else torch.sqrt(ux * ux + uy * uy + uz * uz)
+        qv = (rep(n) if n is not None else torch.full((m,), sp.n0, device=device, dtype=torch.float64)) / sp.ppc
+        if sp.cmr < 0:
+            qv = -qv
+        yield {"x": x, "y": y, "z": z, "ux": ux, "uy": uy, "uz": uz, "g": g, "q": qv}

@@ -1,0 +1,126 @@
+"""QED: device rate functions against the reference's (mc.cpp:26-116), the
+counter-based random numbers against the published Philox4x32-10 answers,
+and photon-emission / pair-creation statistics of whole steps against the
+reference run with 16 seeds (agreement within 3 sigma)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.conftest import gpu_available
+
+KIND = "ref" if O.available("ref", "parity") else "port"
+
+
+def _rate_samples(n, seed=5):
+    rng = np.random.default_rng(seed)
+    e = rng.standard_normal((n, 3)) * 10 ** rng.uniform(1, 5, (n, 1))
+    b = rng.standard_normal((n, 3)) * 10 ** rng.uniform(1, 5, (n, 1))
+    u = rng.standard_normal((n, 3)) * 10 ** rng.uniform(0, 3.5, (n, 1))
+    g = np.sqrt(1 + (u * u).sum(1))
+    r = rng.uniform(0, 1, n)
+    chi = 10 ** rng.uniform(-3, 1, n)
+    return np.column_stack([e, b, u, g, r, chi])
+
+
+@pytest.mark.gpu
+def test_device_rates_match_reference():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200.api import eval_qed_rates
+    smp = _rate_samples(4000)
+    out = eval_qed_rates(smp)
+    reg = O.Region(8, 8, 8, 0.4, 0.4, 0.4, 0.2, kind=KIND)
+    for row, o in zip(smp, out):
+        e, b, u, g, r, chi = row[0:3], row[3:6], row[6:9], row[9], row[10], row[11]
+        ref_chi = reg.chi(e, b, u, g)
+        ref_w, ref_r = reg.w(g, r, chi)
+        ref_tw = reg.tilde_w(g, r, chi)
+        ref_W = reg.mathcal_W(e, b)
+        # CUDA's pow/exp/tanh are within a few ulp of the host libm: allow
+        # 1e-12 relative (the rates contain a difference of two terms)
+        np.testing.assert_allclose(o[0], ref_chi, rtol=1e-13)
+        np.testing.assert_allclose(o[2], ref_r, rtol=1e-15)
+        np.testing.assert_allclose(o[1], ref_w, rtol=1e-11, atol=1e-300)
+        np.testing.assert_allclose(o[3], ref_tw, rtol=1e-11, atol=1e-300)
+        np.testing.assert_allclose(o[4], ref_W, rtol=1e-11, atol=1e-300)
+
+
+# ---------------------------------------------------------------------------
+# whole-step statistics
+# ---------------------------------------------------------------------------
+N = 16
+DX = 2 * np.pi / 16
+DT = 0.5 * DX
+B0 = 400.0       # uniform Bz, chi ~ 1 for gamma ~ 1e3
+GAMMA0 = 1000.0
+STEPS = 6
+
+
+def _emission_case(seed, n_e=4000, n_ph=4000):
+    rng = np.random.default_rng(seed)
+    fields = {k: np.zeros((N, N, N)) for k in ("ex", "ey", "ez", "bx", "by", "bz")}
+    fields["bz"][:] = B0
+    parts = []
+    # electrons moving along +y (perpendicular to B), starting in x in [2, 6)
+    x = rng.uniform(2, 6, n_e); y = rng.uniform(2, 5, n_e); z = rng.uniform(2, 13, n_e)
+    u = np.sqrt(GAMMA0 ** 2 - 1)
+    e = {"x": x, "y": y, "z": z, "ux": np.zeros(n_e), "uy": np.full(n_e, u), "uz": np.zeros(n_e),
+         "g": np.full(n_e, GAMMA0), "q": np.full(n_e, -1e-8), "cmr": np.full(n_e, -1.0)}
+    # photons for pair creation: gamma 4000 along +y
+    xp = rng.uniform(8, 12, n_ph); yp = rng.uniform(2, 5, n_ph); zp = rng.uniform(2, 13, n_ph)
+    ph = {"x": xp, "y": yp, "z": zp, "ux": np.zeros(n_ph), "uy": np.full(n_ph, 4000.0), "uz": np.zeros(n_ph),
+          "g": np.full(n_ph, 4000.0), "q": np.full(n_ph, 1e-8), "cmr": np.zeros(n_ph)}
+    return fields, e, ph
+
+
+def _sort(p):
+    cell = (p["x"].astype(int) * N + p["y"].astype(int)) * N + p["z"].astype(int)
+    o = np.argsort(cell, kind="stable")
+    return {k: v[o] for k, v in p.items()}
+
+
+def _stats_from(parts_e, parts_p, parts_ph):
+    return {"n_ph": parts_ph["x"].size, "e_ph": parts_ph["g"].sum(), "n_p": parts_p["x"].size,
+            "e_e": parts_e["g"].sum()}
+
+
+def _ref_stats(seed):
+    fields, e, ph = _emission_case(0)
+    reg = O.Region(N, N, N, DX, DX, DX, DT, solver=0, pusher=1, qed=True, seed=seed, kind=KIND)
+    reg.set_fields(*[fields[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
+    reg.init_boundaries()
+    allp = _sort({k: np.concatenate([e[k], ph[k]]) for k in e})
+    reg.add_particles(allp)
+    reg.step(STEPS)
+    p = reg.get_particles()
+    sel = lambda c: {k: v[p["cmr"] == c] for k, v in p.items()}
+    return _stats_from(sel(-1.0), sel(1.0), sel(0.0))
+
+
+@pytest.mark.gpu
+def test_qed_step_statistics_vs_reference():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    if KIND != "ref":
+        pytest.skip("whole-step QED statistics need the compiled reference")
+    from quill_b200.api import Region
+    ref = [_ref_stats(1 + s) for s in range(16)]
+    gpu = []
+    for seed in range(16):
+        fields, e, ph = _emission_case(0)
+        g = Region(N, N, N, DX, DX, DX, DT, species_cmr=(-1.0, 1.0, 0.0), solver="fdtd", pusher="boris",
+                   qed=True, seed=1000 + seed)
+        g.set_fields(*[fields[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
+        g.init_boundaries()
+        g.add_particles(0, _sort(e))
+        g.add_particles(2, _sort(ph))
+        g.step(STEPS)
+        gpu.append(_stats_from(g.get_particles(0), g.get_particles(1), g.get_particles(2)))
+        g.close()
+    for key in ("n_ph", "e_ph", "n_p", "e_e"):
+        r = np.array([x[key] for x in ref], dtype=float)
+        v = np.array([x[key] for x in gpu], dtype=float)
+        # difference of the two 16-seed means within 3 sigma of that difference
+        sig = np.sqrt(r.var(ddof=1) / r.size + v.var(ddof=1) / v.size)
+        assert abs(v.mean() - r.mean()) <= 3 * sig + 1e-12 * abs(r.mean()), (key, v.mean(), r.mean(), sig)
+        assert r.mean() > 0
