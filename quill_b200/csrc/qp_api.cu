@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -214,6 +215,7 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.grid.nynz = p.ny * p.nz;
     s.grid.nc = p.nx * p.ny * p.nz;
     s.field_elem = s.fp64 ? 8 : 4;
+    if (const char* mb = getenv("QP_TILE_MINBLOCKS")) s.tile_minblocks = atoi(mb) == 2 ? 2 : 3;
     cudaError_t e = cudaSetDevice(p.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;
@@ -618,14 +620,15 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
                 born[i] = (int)std::min<int64_t>(born[i], s.sp[i].cap - s.sp[i].n);
         } else {
             for (size_t i = 0; i < s.sp.size(); i++) {
-                if (s.fp64) launch_push_fp64(s, (int)i, external_bz);
-                else launch_push_mixed(s, (int)i, external_bz);
+                if (s.fp64) launch_push_fp64_tile(s, (int)i, external_bz);
+                else launch_push_mixed_tile(s, (int)i, external_bz);
             }
         }
+        const bool counted = !s.prm.qed;
         QP_CUDA_CHECK(s, cudaGetLastError());
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[2], s.stream));
         for (size_t i = 0; i < s.sp.size(); i++)
-            if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i]);
+            if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i], counted);
         QP_CUDA_CHECK(s, cudaGetLastError());
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[3], s.stream));
         // compute_energy field term on E, B before fadvance (main.cpp:2327)

@@ -70,6 +70,104 @@ __global__ void __launch_bounds__(256) k_push64(Fields<double> f, Grid g, PStore
     block_diag(a.diag, a.sp, dq, de, dc);
 }
 
+// One particle of k_push64 / k_push64_tile: gather, push, deposition into
+// `sink`, new cell (-1 = erased).  Photons fly straight without current.
+template <int PUSHER, int KIND, typename Sink>
+__device__ __forceinline__ int push_one64(const Fields<double>& f, const Sink& sink, const Grid& g,
+                                          const PushArgs& a, double pos[3], double& ux, double& uy, double& uz,
+                                          double& gm, double q) {
+    const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
+    if (kill_layer(g, i0, j0, k0)) return -1;
+    double E[3], B[3];
+    gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
+    B[2] += a.ext_bz;
+    if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
+    const double t = a.dt / gm;
+    double d[3] = {ux * t, uy * t, uz * t};
+    d[0] = d[0] / a.dx;
+    d[1] = d[1] / a.dy;
+    d[2] = d[2] / a.dz;
+    if (KIND == KIND_PHOTON) {
+        pos[0] = pos[0] + d[0];
+        pos[1] = pos[1] + d[1];
+        pos[2] = pos[2] + d[2];
+    } else {
+        jdeposition_to(sink, g, pos, d, q, 0, 0, 0, a.status);
+    }
+    if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+    const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
+    const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
+    if (!moved || inside(g, i1, j1, k1)) return cidx(g, i1, j1, k1);
+    return -1;
+}
+
+// k_push64 with the current J accumulated per k-line segment in shared
+// memory (TileSink) and flushed once, and the rebin histogram (particles per
+// new cell) accumulated the same way.  One CTA per segment of L cells of a
+// line (i, j); its particles are the traversal range
+// [cell_start[first cell], cell_start[last cell + 1]).
+template <int PUSHER, int KIND, int L, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_push64_tile(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
+                                                     const int32_t* __restrict__ perm,
+                                                     int32_t* __restrict__ newcell,
+                                                     const int32_t* __restrict__ cell_start,
+                                                     int32_t* __restrict__ count, PushArgs a) {
+    using TS = TileSink<double, L>;
+    constexpr int NC = 9 * (L + 2);
+    __shared__ double sj[TS::SIZE];
+    __shared__ int scnt[NC];
+    const int k0 = blockIdx.x * L, j0 = blockIdx.y, i0 = blockIdx.z;
+    const int kend = min(k0 + L, g.nz);
+    const int c0 = cidx(g, i0, j0, k0);
+    const int pb = cell_start[c0], pe = cell_start[c0 + (kend - k0)];
+    if (pb == pe) return;  // uniform across the CTA
+    for (int e = threadIdx.x; e < TS::SIZE; e += blockDim.x) sj[e] = 0.0;
+    for (int e = threadIdx.x; e < NC; e += blockDim.x) scnt[e] = 0;
+    __syncthreads();
+    TS sink;
+    sink.sm = sj; sink.f = f; sink.ti0 = i0 - 1; sink.tj0 = j0 - 1; sink.tk0 = k0 - 1;
+    double dq = 0.0, de = 0.0;
+    unsigned long long dc = 0;
+    for (int s = pb + threadIdx.x; s < pe; s += blockDim.x) {
+        const int p = perm[s];
+        double pos[3] = {src.x[p], src.y[p], src.z[p]};
+        double ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
+        const double q = src.q[p];
+        const int nc = push_one64<PUSHER, KIND>(f, sink, g, a, pos, ux, uy, uz, gm, q);
+        newcell[s] = nc;
+        if (nc >= 0) {
+            dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
+            dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
+            dst.g[s] = gm; dst.q[s] = q;
+            if (dst.chi) dst.chi[s] = src.chi[p];
+            dq += q;
+            de += KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
+            dc += 1;
+            const unsigned di = (unsigned)((int)pos[0] - (i0 - 1)), dj = (unsigned)((int)pos[1] - (j0 - 1)),
+                           dk = (unsigned)((int)pos[2] - (k0 - 1));
+            if (di < 3u && dj < 3u && dk < (unsigned)(L + 2)) atomicAdd(scnt + ((int)di * 3 + (int)dj) * (L + 2) + (int)dk, 1);
+            else atomicAdd(count + nc, 1);
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < TS::SIZE; e += blockDim.x) {
+        const double v = sj[e];
+        if (v == 0.0) continue;
+        const int comp = e / (16 * TS::NK), r = e - comp * (16 * TS::NK);
+        const int i = sink.ti0 + r / (4 * TS::NK), j = sink.tj0 + (r / TS::NK) % 4, k = sink.tk0 + r % TS::NK;
+        if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) continue;
+        double* base = comp == 0 ? f.jx : (comp == 1 ? f.jy : f.jz);
+        atomicAdd(base + cidx(g, i, j, k), v);
+    }
+    for (int e = threadIdx.x; e < NC; e += blockDim.x) {
+        const int v = scnt[e];
+        if (v == 0) continue;
+        const int i = i0 - 1 + e / (3 * (L + 2)), j = j0 - 1 + (e / (L + 2)) % 3, k = k0 - 1 + e % (L + 2);
+        atomicAdd(count + cidx(g, i, j, k), v);
+    }
+    block_diag(a.diag, a.sp, dq, de, dc);
+}
+
 // Particle born during a push: appended to the target species' output
 // buffer with its final cell, erased (not stored) if the cell is not inside
 // (place(p), plist.cpp:22-39).  Counted in the target's diagnostics.
@@ -452,6 +550,36 @@ int launch_vacuum_fp64(State& s) {
         k_vacuum64<QP_PUSHER_BORIS><<<nb, 256, 0, s.stream>>>(f, s.grid, qa, p.dt, dV, qv, t0, t1, s.d_status);
     s.launches++;
     return QP_OK;
+}
+
+constexpr int TILE_L = 64;
+
+// Tiled push: also leaves the particles-per-new-cell histogram in sp.count
+// (zeroed here), so the rebin skips its counting pass.
+void launch_push_fp64_tile(State& s, int si, double external_bz) {
+    Species& sp = s.sp[si];
+    cudaMemsetAsync(sp.count, 0, (size_t)s.grid.nc * sizeof(int32_t), s.stream);
+    if (sp.n == 0) return;
+    PStore64 src = store64(sp, sp.cur), dst = store64(sp, 1 - sp.cur);
+    PushArgs a;
+    a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
+    a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
+    a.status = s.d_status; a.diag = s.d_diag;
+    dim3 grd((s.grid.nz + TILE_L - 1) / TILE_L, s.grid.ny, s.grid.nx);
+    Fields<double> f = fields64(s);
+    const bool vay = s.prm.pusher == QP_PUSHER_VAY;
+#define QP_LT(P, K)                                                                                          \
+    if (s.tile_minblocks == 2)                                                                                \
+        k_push64_tile<P, K, TILE_L, 2><<<grd, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell,  \
+                                                                  sp.cell_start, sp.count, a);               \
+    else                                                                                                      \
+        k_push64_tile<P, K, TILE_L, 3><<<grd, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell,  \
+                                                                  sp.cell_start, sp.count, a)
+    if (sp.kind == KIND_PHOTON) QP_LT(QP_PUSHER_BORIS, KIND_PHOTON);
+    else if (vay) QP_LT(QP_PUSHER_VAY, KIND_LEPTON);
+    else QP_LT(QP_PUSHER_BORIS, KIND_LEPTON);
+#undef QP_LT
+    s.launches++;
 }
 
 void launch_field_energy_fp64(State& s) {

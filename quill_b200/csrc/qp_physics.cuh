@@ -102,14 +102,23 @@ __device__ __forceinline__ void gather(const Fields<T>& f, const Grid& gr, int i
 // Current deposition (deposition.cpp:13-356)
 // ----------------------------------------------------------------------------
 
+// Destination of the current contributions: J in HBM through atomics.
+template <typename T>
+struct GlobalSink {
+    Fields<T> f;
+    __device__ __forceinline__ void add(int comp, int, int, int, int c, T v) const {
+        T* base = comp == 0 ? f.jx : (comp == 1 ? f.jy : f.jz);
+        atomicAdd(base + c, v);
+    }
+};
+
 // 12 contributions of one straight segment d starting at p, lying in the cell
 // with lower corner w (deposition.cpp:13-39).  p and w are in the particle's
 // frame; the global cell of the corner is base + w.  Out-of-grid targets are
 // skipped and flagged (cannot happen for dt < dx, dy, dz).
-template <typename T>
-__device__ __forceinline__ void seg_dep(const Fields<T>& f, const Grid& gr, const T p[3], const T d[3],
-                                        T q, const int w[3], int bi, int bj, int bk,
-                                        unsigned int* status) {
+template <typename T, typename Sink>
+__device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const T p[3], const T d[3], T q,
+                                        const int w[3], int bi, int bj, int bk, unsigned int* status) {
     const T xa = p[0] - T(w[0]), xb = T(1) - xa;
     const T ya = p[1] - T(w[1]), yb = T(1) - ya;
     const T za = p[2] - T(w[2]), zb = T(1) - za;
@@ -122,19 +131,42 @@ __device__ __forceinline__ void seg_dep(const Fields<T>& f, const Grid& gr, cons
     const int c = cidx(gr, wi, wj, wk);
     const int cj1 = c + gr.nz, ck1 = c + 1, ci1 = c + gr.nynz;
     const T third = T(3);
-    atomicAdd(f.jx + cj1 + 1, dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third));
-    atomicAdd(f.jx + ck1, dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - dy * dz / third));
-    atomicAdd(f.jx + cj1, dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - dy * dz / third));
-    atomicAdd(f.jx + c, dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + dy * dz / third));
-    atomicAdd(f.jy + ci1 + 1, dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + dx * dz / third));
-    atomicAdd(f.jy + ck1, dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - dx * dz / third));
-    atomicAdd(f.jy + ci1, dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - dx * dz / third));
-    atomicAdd(f.jy + c, dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + dx * dz / third));
-    atomicAdd(f.jz + ci1 + gr.nz, dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + dx * dy / third));
-    atomicAdd(f.jz + cj1, dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third));
-    atomicAdd(f.jz + ci1, dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third));
-    atomicAdd(f.jz + c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third));
+    sink.add(0, wi, wj + 1, wk + 1, cj1 + 1, dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third));
+    sink.add(0, wi, wj, wk + 1, ck1, dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - dy * dz / third));
+    sink.add(0, wi, wj + 1, wk, cj1, dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - dy * dz / third));
+    sink.add(0, wi, wj, wk, c, dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + dy * dz / third));
+    sink.add(1, wi + 1, wj, wk + 1, ci1 + 1, dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + dx * dz / third));
+    sink.add(1, wi, wj, wk + 1, ck1, dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - dx * dz / third));
+    sink.add(1, wi + 1, wj, wk, ci1, dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - dx * dz / third));
+    sink.add(1, wi, wj, wk, c, dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + dx * dz / third));
+    sink.add(2, wi + 1, wj + 1, wk, ci1 + gr.nz, dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + dx * dy / third));
+    sink.add(2, wi, wj + 1, wk, cj1, dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third));
+    sink.add(2, wi + 1, wj, wk, ci1, dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third));
+    sink.add(2, wi, wj, wk, c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third));
 }
+
+// Destination of the current contributions of the particles of one k-line
+// segment of L cells, (i0, j0, k0 .. k0+L-1): a shared-memory tile over
+// (i0-1 .. i0+2) x (j0-1 .. j0+2) x (k0-1 .. k0+L+1) per component, which
+// holds every contribution of a particle that moves less than a cell;
+// anything outside goes to HBM directly.
+template <typename T, int L>
+struct TileSink {
+    T* sm;
+    Fields<T> f;
+    int ti0, tj0, tk0;
+    static constexpr int NK = L + 3;
+    static constexpr int SIZE = 3 * 16 * NK;
+    __device__ __forceinline__ void add(int comp, int i, int j, int k, int c, T v) const {
+        const unsigned di = (unsigned)(i - ti0), dj = (unsigned)(j - tj0), dk = (unsigned)(k - tk0);
+        if (di < 4u && dj < 4u && dk < (unsigned)NK) {
+            atomicAdd(sm + ((comp * 4 + (int)di) * 4 + (int)dj) * NK + (int)dk, v);
+        } else {
+            T* base = comp == 0 ? f.jx : (comp == 1 ? f.jy : f.jz);
+            atomicAdd(base + c, v);
+        }
+    }
+};
 
 // Three ratios sorted descending with the reference's tie handling
 // (`regulate`, low-level.cpp:316-366).
@@ -156,85 +188,98 @@ __device__ __forceinline__ int ifloor(T v) { return (int)floor(v); }
 // segments), deposit each segment in its cell and advance p segment by
 // segment (deposition.cpp:41-356).  p is in a frame whose integer lattice is
 // the cell lattice shifted by base (base = 0 for absolute FP64 positions).
-template <typename T>
-__device__ __forceinline__ void jdeposition(const Fields<T>& f, const Grid& gr, T p[3], const T d[3], T q,
-                                            int bi, int bj, int bk, unsigned int* status) {
-    int c1[3], c2[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) { c1[a] = ifloor(p[a]); c2[a] = ifloor(p[a] + d[a]); }
-    const int cx = c1[0] != c2[0], cy = c1[1] != c2[1], cz = c1[2] != c2[2];
-    const int ncross = cx + cy + cz;
+// Written with per-axis selects instead of run-time array indices so that
+// everything stays in registers; the arithmetic is the reference's.
+template <typename T, typename Sink>
+__device__ __forceinline__ void jdeposition_to(const Sink& f, const Grid& gr, T p[3], const T d[3], T q,
+                                               int bi, int bj, int bk, unsigned int* status) {
+    const int c1x = ifloor(p[0]), c1y = ifloor(p[1]), c1z = ifloor(p[2]);
+    const int c2x = ifloor(p[0] + d[0]), c2y = ifloor(p[1] + d[1]), c2z = ifloor(p[2] + d[2]);
+    const bool cx = c1x != c2x, cy = c1y != c2y, cz = c1z != c2z;
+    const int ncross = (int)cx + (int)cy + (int)cz;
+    int w[3] = {c1x, c1y, c1z};
     T s[3];
-    int w[3] = {c1[0], c1[1], c1[2]};
     if (ncross == 0) {
         seg_dep(f, gr, p, d, q, w, bi, bj, bk, status);
-#pragma unroll
-        for (int o = 0; o < 3; o++) p[o] = p[o] + d[o];
+        p[0] = p[0] + d[0]; p[1] = p[1] + d[1]; p[2] = p[2] + d[2];
     } else if (ncross == 1) {
-        const int a = cx ? 0 : (cy ? 1 : 2);
-        s[a] = T(max(c1[a], c2[a])) - p[a];
-#pragma unroll
-        for (int o = 0; o < 3; o++) if (o != a) s[o] = d[o] * s[a] / d[a];
+        // the crossing axis a: up to its face, the other axes in proportion
+        const T pa = cx ? p[0] : (cy ? p[1] : p[2]);
+        const T da = cx ? d[0] : (cy ? d[1] : d[2]);
+        const int ma = cx ? max(c1x, c2x) : (cy ? max(c1y, c2y) : max(c1z, c2z));
+        const T sa = T(ma) - pa;
+        s[0] = cx ? sa : d[0] * sa / da;
+        s[1] = cy ? sa : d[1] * sa / da;
+        s[2] = cz ? sa : d[2] * sa / da;
         seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
-#pragma unroll
-        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
-#pragma unroll
-        for (int o = 0; o < 3; o++) s[o] = d[o] - s[o];
-        w[a] = c2[a];
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
+        s[0] = d[0] - s[0]; s[1] = d[1] - s[1]; s[2] = d[2] - s[2];
+        if (cx) w[0] = c2x;
+        if (cy) w[1] = c2y;
+        if (cz) w[2] = c2z;
         seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
-#pragma unroll
-        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
     } else if (ncross == 2) {
         // axis A carries the reference's path1 (y for (y,z) and (x,y), x for
-        // (x,z)), axis B its path2; B goes first only if path1 > path2
-        int A, B;
-        if (!cx) { A = 1; B = 2; }
-        else if (!cy) { A = 0; B = 2; }
-        else { A = 1; B = 0; }
-        const T pa = (T(max(c1[A], c2[A])) - p[A]) / d[A];
-        const T pb = (T(max(c1[B], c2[B])) - p[B]) / d[B];
-        int first = A, second = B;
-        T p1 = pa, p2 = pb;
-        if (pa > pb) { first = B; second = A; p1 = pb; p2 = pa; }
-#pragma unroll
-        for (int o = 0; o < 3; o++) s[o] = d[o] * p1;
+        // (x,z)), axis B its path2 (z, z, x); B goes first only if
+        // path1 > path2
+        const bool A0 = cx && !cy;   // A = x (x,z case); else A = y
+        const bool B0 = cx && cy;    // B = x (x,y case); else B = z
+        const T pA = A0 ? p[0] : p[1], dA = A0 ? d[0] : d[1];
+        const int mA = A0 ? max(c1x, c2x) : max(c1y, c2y);
+        const T pB = B0 ? p[0] : p[2], dB = B0 ? d[0] : d[2];
+        const int mB = B0 ? max(c1x, c2x) : max(c1z, c2z);
+        const T pa = (T(mA) - pA) / dA;
+        const T pb = (T(mB) - pB) / dB;
+        const bool bfirst = pa > pb;
+        const T p1 = bfirst ? pb : pa, p2 = bfirst ? pa : pb;
+        // axis indices of the first and second crossing
+        const int fa = bfirst ? (B0 ? 0 : 2) : (A0 ? 0 : 1);
+        const int sa2 = bfirst ? (A0 ? 0 : 1) : (B0 ? 0 : 2);
+        s[0] = d[0] * p1; s[1] = d[1] * p1; s[2] = d[2] * p1;
         seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
-#pragma unroll
-        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
         const T pm = p2 - p1;
-#pragma unroll
-        for (int o = 0; o < 3; o++) s[o] = d[o] * pm;
-        w[first] = c2[first];
+        s[0] = d[0] * pm; s[1] = d[1] * pm; s[2] = d[2] * pm;
+        if (fa == 0) w[0] = c2x;
+        if (fa == 1) w[1] = c2y;
+        if (fa == 2) w[2] = c2z;
         seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
-#pragma unroll
-        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
         const T pr = T(1) - p2;
-#pragma unroll
-        for (int o = 0; o < 3; o++) s[o] = d[o] * pr;
-        w[second] = c2[second];
+        s[0] = d[0] * pr; s[1] = d[1] * pr; s[2] = d[2] * pr;
+        if (sa2 == 0) w[0] = c2x;
+        if (sa2 == 1) w[1] = c2y;
+        if (sa2 == 2) w[2] = c2z;
         seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
-#pragma unroll
-        for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
     } else {
-        T path[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++) path[a] = (T(max(c1[a], c2[a])) - p[a]) / d[a];
+        const T path0 = (T(max(c1x, c2x)) - p[0]) / d[0];
+        const T path1 = (T(max(c1y, c2y)) - p[1]) / d[1];
+        const T path2 = (T(max(c1z, c2z)) - p[2]) / d[2];
         T vx, vy, vz;
-        sort3_desc(path[0], path[1], path[2], vx, vy, vz);
+        sort3_desc(path0, path1, path2, vx, vy, vz);
         const T fr[4] = {vz, vy - vz, vx - vy, T(1) - vx};
 #pragma unroll
         for (int sg = 0; sg < 4; sg++) {
-#pragma unroll
-            for (int o = 0; o < 3; o++) s[o] = d[o] * fr[sg];
+            s[0] = d[0] * fr[sg]; s[1] = d[1] * fr[sg]; s[2] = d[2] * fr[sg];
             if (sg > 0) {
-#pragma unroll
-                for (int o = 0; o < 3; o++) w[o] = ifloor(p[o] + T(0.5) * s[o]);
+                w[0] = ifloor(p[0] + T(0.5) * s[0]);
+                w[1] = ifloor(p[1] + T(0.5) * s[1]);
+                w[2] = ifloor(p[2] + T(0.5) * s[2]);
             }
             seg_dep(f, gr, p, s, q, w, bi, bj, bk, status);
-#pragma unroll
-            for (int o = 0; o < 3; o++) p[o] = p[o] + s[o];
+            p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
         }
     }
+}
+
+// jdeposition straight into J in HBM (atomics per contribution).
+template <typename T>
+__device__ __forceinline__ void jdeposition(const Fields<T>& f, const Grid& gr, T p[3], const T d[3], T q,
+                                            int bi, int bj, int bk, unsigned int* status) {
+    GlobalSink<T> sink{f};
+    jdeposition_to(sink, gr, p, d, q, bi, bj, bk, status);
 }
 
 }  // namespace qp

@@ -177,13 +177,15 @@ void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n) {
     s.launches += 3;
 }
 
-int64_t rebin(State& s, int si, int64_t born) {
+int64_t rebin(State& s, int si, int64_t born, bool counted) {
     Species& sp = s.sp[si];
     const Grid g = s.grid;
     const int nb = (g.nc + 255) / 256;
     const int n = (int)sp.n, A = (int)born;
-    k_rebin_count<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.count);
-    s.launches++;
+    if (!counted) {
+        k_rebin_count<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.count);
+        s.launches++;
+    }
     if (A > 0) {
         cudaMemsetAsync(sp.born, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
         cudaMemsetAsync(sp.born_fill, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
