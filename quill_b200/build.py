@@ -18,6 +18,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libquill_b200.so")
+DRIVER = os.path.join(PKG, "qp_driver")
+DRIVER_SRC = os.path.join(PKG, "driver", "qp_driver.cpp")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -57,6 +59,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
             subprocess.run(cmd, check=True)
     if force or _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if force or _newer(DRIVER, [DRIVER_SRC, LIB, os.path.join(ROOT, "include", "quill_b200.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", f"-I{os.path.join(ROOT, 'include')}", DRIVER_SRC, "-o", DRIVER,
+               f"-L{PKG}", "-lquill_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

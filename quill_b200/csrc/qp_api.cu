@@ -215,7 +215,6 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.grid.nynz = p.ny * p.nz;
     s.grid.nc = p.nx * p.ny * p.nz;
     s.field_elem = s.fp64 ? 8 : 4;
-    if (const char* mb = getenv("QP_TILE_MINBLOCKS")) s.tile_minblocks = atoi(mb) == 2 ? 2 : 3;
     cudaError_t e = cudaSetDevice(p.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;
@@ -620,8 +619,8 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
                 born[i] = (int)std::min<int64_t>(born[i], s.sp[i].cap - s.sp[i].n);
         } else {
             for (size_t i = 0; i < s.sp.size(); i++) {
-                if (s.fp64) launch_push_fp64_tile(s, (int)i, external_bz);
-                else launch_push_mixed_tile(s, (int)i, external_bz);
+                if (s.fp64) launch_push_fp64(s, (int)i, external_bz);
+                else launch_push_mixed(s, (int)i, external_bz);
             }
         }
         const bool counted = !s.prm.qed;

@@ -6,56 +6,74 @@
 
 namespace qp {
 
-// One thread per particle in traversal order: gather -> push -> current
-// deposition (moving the particle segment by segment) -> new cell.  The
-// particle is read through perm from the previous layout and written at its
-// traversal position into the other buffer.  Erased particles (outside
-// is_inside after a move, or in a p_boundary layer on entry) get newcell -1.
-// advance.cpp:90-387 with QED off: photons fly straight without current
-// (:155-252), leptons and ions are pushed and deposit (:253-371).
+// One particle: gather, push, displacement, current deposition, new cell
+// (-1 = erased; place(), plist.cpp:7-39).  A move that stays inside its cell
+// (one segment) returns its 12 contributions in v[] and its cell in *corner
+// for the warp-level run reduction; moves that cross faces deposit their
+// segments directly.  Photons fly straight without current.
+// advance.cpp:90-387 with QED off: photons :155-252, leptons and ions
+// :253-371.
 template <int PUSHER, int KIND>
-__global__ void __launch_bounds__(256) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
-                                                const int32_t* __restrict__ perm,
-                                                int32_t* __restrict__ newcell, PushArgs a) {
+__device__ __forceinline__ int push_one64(const Fields<double>& f, const Grid& g, const PushArgs& a, double pos[3],
+                                          double& ux, double& uy, double& uz, double& gm, double q, int* corner,
+                                          double v[12]) {
+    const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
+    if (kill_layer(g, i0, j0, k0)) return -1;
+    double E[3], B[3];
+    gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
+    B[2] += a.ext_bz;
+    if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
+    // particle::get_displacement (containers.cpp:58-67), then per-axis
+    // division by the cell size (advance.cpp:281-284)
+    const double t = a.dt / gm;
+    double d[3] = {ux * t, uy * t, uz * t};
+    d[0] = d[0] / a.dx;
+    d[1] = d[1] / a.dy;
+    d[2] = d[2] / a.dz;
+    if (KIND == KIND_PHOTON) {
+        pos[0] = pos[0] + d[0];
+        pos[1] = pos[1] + d[1];
+        pos[2] = pos[2] + d[2];
+    } else {
+        const int w[3] = {ifloor(pos[0]), ifloor(pos[1]), ifloor(pos[2])};
+        if (w[0] == ifloor(pos[0] + d[0]) && w[1] == ifloor(pos[1] + d[1]) && w[2] == ifloor(pos[2] + d[2])) {
+            seg_values(pos, d, q, w, v);
+            *corner = cidx(g, w[0], w[1], w[2]);
+            pos[0] = pos[0] + d[0];
+            pos[1] = pos[1] + d[1];
+            pos[2] = pos[2] + d[2];
+        } else {
+            jdeposition(f, g, pos, d, q, 0, 0, 0, a.status);
+        }
+    }
+    if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+    const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
+    const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
+    if (!moved || inside(g, i1, j1, k1)) return cidx(g, i1, j1, k1);
+    return -1;
+}
+
+// One thread per particle in traversal order.  The particle is read through
+// perm from the previous layout and written at its traversal position into
+// the other buffer; newcell and the particles-per-new-cell histogram
+// (count) feed the rebin.
+template <int PUSHER, int KIND>
+__global__ void __launch_bounds__(256, 3) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
+                                                   const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
+                                                   int32_t* __restrict__ count, PushArgs a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
+    int corner = -1, nc = -1;
+    double v[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) v[k] = 0.0;
     if (s < a.n) {
         const int p = perm[s];
         double pos[3] = {src.x[p], src.y[p], src.z[p]};
         double ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
         const double q = src.q[p];
-        const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
-        int nc = -1;
-        if (!kill_layer(g, i0, j0, k0)) {
-            double E[3], B[3];
-            {
-                const int i = (int)floor(pos[0]), j = (int)floor(pos[1]), k = (int)floor(pos[2]);
-                gather(f, g, i, j, k, pos[0] - i, pos[1] - j, pos[2] - k, E, B);
-            }
-            B[2] += a.ext_bz;
-            if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
-            // particle::get_displacement (containers.cpp:58-67), then per-axis
-            // division by the cell size (advance.cpp:281-284)
-            const double t = a.dt / gm;
-            double d[3] = {ux * t, uy * t, uz * t};
-            d[0] = d[0] / a.dx;
-            d[1] = d[1] / a.dy;
-            d[2] = d[2] / a.dz;
-            if (KIND == KIND_PHOTON) {
-                pos[0] = pos[0] + d[0];
-                pos[1] = pos[1] + d[1];
-                pos[2] = pos[2] + d[2];
-            } else {
-                jdeposition(f, g, pos, d, q, 0, 0, 0, a.status);
-            }
-            if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
-            // place(p, i, j, k) (plist.cpp:7-39): relink only if the cell
-            // changed, erase if the new cell is not inside
-            const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
-            const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
-            if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
-        }
+        nc = push_one64<PUSHER, KIND>(f, g, a, pos, ux, uy, uz, gm, q, &corner, v);
         newcell[s] = nc;
         if (nc >= 0) {
             dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
@@ -67,104 +85,8 @@ __global__ void __launch_bounds__(256) k_push64(Fields<double> f, Grid g, PStore
             dc = 1;
         }
     }
-    block_diag(a.diag, a.sp, dq, de, dc);
-}
-
-// One particle of k_push64 / k_push64_tile: gather, push, deposition into
-// `sink`, new cell (-1 = erased).  Photons fly straight without current.
-template <int PUSHER, int KIND, typename Sink>
-__device__ __forceinline__ int push_one64(const Fields<double>& f, const Sink& sink, const Grid& g,
-                                          const PushArgs& a, double pos[3], double& ux, double& uy, double& uz,
-                                          double& gm, double q) {
-    const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
-    if (kill_layer(g, i0, j0, k0)) return -1;
-    double E[3], B[3];
-    gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
-    B[2] += a.ext_bz;
-    if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
-    const double t = a.dt / gm;
-    double d[3] = {ux * t, uy * t, uz * t};
-    d[0] = d[0] / a.dx;
-    d[1] = d[1] / a.dy;
-    d[2] = d[2] / a.dz;
-    if (KIND == KIND_PHOTON) {
-        pos[0] = pos[0] + d[0];
-        pos[1] = pos[1] + d[1];
-        pos[2] = pos[2] + d[2];
-    } else {
-        jdeposition_to(sink, g, pos, d, q, 0, 0, 0, a.status);
-    }
-    if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
-    const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
-    const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
-    if (!moved || inside(g, i1, j1, k1)) return cidx(g, i1, j1, k1);
-    return -1;
-}
-
-// k_push64 with the current J accumulated per k-line segment in shared
-// memory (TileSink) and flushed once, and the rebin histogram (particles per
-// new cell) accumulated the same way.  One CTA per segment of L cells of a
-// line (i, j); its particles are the traversal range
-// [cell_start[first cell], cell_start[last cell + 1]).
-template <int PUSHER, int KIND, int L, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_push64_tile(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
-                                                     const int32_t* __restrict__ perm,
-                                                     int32_t* __restrict__ newcell,
-                                                     const int32_t* __restrict__ cell_start,
-                                                     int32_t* __restrict__ count, PushArgs a) {
-    using TS = TileSink<double, L>;
-    constexpr int NC = 9 * (L + 2);
-    __shared__ double sj[TS::SIZE];
-    __shared__ int scnt[NC];
-    const int k0 = blockIdx.x * L, j0 = blockIdx.y, i0 = blockIdx.z;
-    const int kend = min(k0 + L, g.nz);
-    const int c0 = cidx(g, i0, j0, k0);
-    const int pb = cell_start[c0], pe = cell_start[c0 + (kend - k0)];
-    if (pb == pe) return;  // uniform across the CTA
-    for (int e = threadIdx.x; e < TS::SIZE; e += blockDim.x) sj[e] = 0.0;
-    for (int e = threadIdx.x; e < NC; e += blockDim.x) scnt[e] = 0;
-    __syncthreads();
-    TS sink;
-    sink.sm = sj; sink.f = f; sink.ti0 = i0 - 1; sink.tj0 = j0 - 1; sink.tk0 = k0 - 1;
-    double dq = 0.0, de = 0.0;
-    unsigned long long dc = 0;
-    for (int s = pb + threadIdx.x; s < pe; s += blockDim.x) {
-        const int p = perm[s];
-        double pos[3] = {src.x[p], src.y[p], src.z[p]};
-        double ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
-        const double q = src.q[p];
-        const int nc = push_one64<PUSHER, KIND>(f, sink, g, a, pos, ux, uy, uz, gm, q);
-        newcell[s] = nc;
-        if (nc >= 0) {
-            dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
-            dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
-            dst.g[s] = gm; dst.q[s] = q;
-            if (dst.chi) dst.chi[s] = src.chi[p];
-            dq += q;
-            de += KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
-            dc += 1;
-            const unsigned di = (unsigned)((int)pos[0] - (i0 - 1)), dj = (unsigned)((int)pos[1] - (j0 - 1)),
-                           dk = (unsigned)((int)pos[2] - (k0 - 1));
-            if (di < 3u && dj < 3u && dk < (unsigned)(L + 2)) atomicAdd(scnt + ((int)di * 3 + (int)dj) * (L + 2) + (int)dk, 1);
-            else atomicAdd(count + nc, 1);
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < TS::SIZE; e += blockDim.x) {
-        const double v = sj[e];
-        if (v == 0.0) continue;
-        const int comp = e / (16 * TS::NK), r = e - comp * (16 * TS::NK);
-        const int i = sink.ti0 + r / (4 * TS::NK), j = sink.tj0 + (r / TS::NK) % 4, k = sink.tk0 + r % TS::NK;
-        if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) continue;
-        double* base = comp == 0 ? f.jx : (comp == 1 ? f.jy : f.jz);
-        atomicAdd(base + cidx(g, i, j, k), v);
-    }
-    for (int e = threadIdx.x; e < NC; e += blockDim.x) {
-        const int v = scnt[e];
-        if (v == 0) continue;
-        const int i = i0 - 1 + e / (3 * (L + 2)), j = j0 - 1 + (e / (L + 2)) % 3, k = k0 - 1 + e % (L + 2);
-        atomicAdd(count + cidx(g, i, j, k), v);
-    }
+    warp_deposit_runs(f, g, corner, v);
+    warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
 }
 
@@ -445,31 +367,6 @@ void zero_planes_fp64(State& s, const ZeroPlane* zp, int n) {
     }
 }
 
-void launch_push_fp64(State& s, int si, double external_bz) {
-    Species& sp = s.sp[si];
-    if (sp.n == 0) return;
-    PStore64 src, dst;
-    double** ps[9] = {&src.x, &src.y, &src.z, &src.ux, &src.uy, &src.uz, &src.g, &src.q, &src.chi};
-    double** pd[9] = {&dst.x, &dst.y, &dst.z, &dst.ux, &dst.uy, &dst.uz, &dst.g, &dst.q, &dst.chi};
-    for (int a = 0; a < 9; a++) {
-        *ps[a] = (double*)sp.buf[sp.cur][a];
-        *pd[a] = (double*)sp.buf[1 - sp.cur][a];
-    }
-    PushArgs a;
-    a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
-    a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
-    a.status = s.d_status; a.diag = s.d_diag;
-    const int nb = (int)((sp.n + 255) / 256);
-    Fields<double> f = fields64(s);
-    const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LP(P, K) k_push64<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a)
-    if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
-    else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
-    else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
-#undef QP_LP
-    s.launches++;
-}
-
 static PStore64 store64(Species& sp, int b) {
     PStore64 st;
     double** ps[9] = {&st.x, &st.y, &st.z, &st.ux, &st.uy, &st.uz, &st.g, &st.q, &st.chi};
@@ -552,11 +449,9 @@ int launch_vacuum_fp64(State& s) {
     return QP_OK;
 }
 
-constexpr int TILE_L = 64;
-
-// Tiled push: also leaves the particles-per-new-cell histogram in sp.count
-// (zeroed here), so the rebin skips its counting pass.
-void launch_push_fp64_tile(State& s, int si, double external_bz) {
+// Push of one species; also leaves the particles-per-new-cell histogram in
+// sp.count (zeroed here), so the rebin skips its counting pass.
+void launch_push_fp64(State& s, int si, double external_bz) {
     Species& sp = s.sp[si];
     cudaMemsetAsync(sp.count, 0, (size_t)s.grid.nc * sizeof(int32_t), s.stream);
     if (sp.n == 0) return;
@@ -565,20 +460,14 @@ void launch_push_fp64_tile(State& s, int si, double external_bz) {
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
-    dim3 grd((s.grid.nz + TILE_L - 1) / TILE_L, s.grid.ny, s.grid.nx);
+    const int nb = (int)((sp.n + 255) / 256);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LT(P, K)                                                                                          \
-    if (s.tile_minblocks == 2)                                                                                \
-        k_push64_tile<P, K, TILE_L, 2><<<grd, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell,  \
-                                                                  sp.cell_start, sp.count, a);               \
-    else                                                                                                      \
-        k_push64_tile<P, K, TILE_L, 3><<<grd, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell,  \
-                                                                  sp.cell_start, sp.count, a)
-    if (sp.kind == KIND_PHOTON) QP_LT(QP_PUSHER_BORIS, KIND_PHOTON);
-    else if (vay) QP_LT(QP_PUSHER_VAY, KIND_LEPTON);
-    else QP_LT(QP_PUSHER_BORIS, KIND_LEPTON);
-#undef QP_LT
+#define QP_LP(P, K) k_push64<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+    if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
+    else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
+    else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
+#undef QP_LP
     s.launches++;
 }
 

@@ -97,9 +97,6 @@ struct State {
     int64_t step_index = 0;
     bool boundaries_done = false;
     int sp_e = -1, sp_p = -1, sp_ph = -1;  // QED species (cmr -1, +1, 0)
-    // occupancy target of the tiled push (CTAs per SM the register budget is
-    // sized for); QP_TILE_MINBLOCKS=2 selects the spill-free variant
-    int tile_minblocks = 3;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
     // diagnostics + J reset)
@@ -122,7 +119,6 @@ struct State {
 void launch_fields_fp64(State& s, int phase);          // phase: 0 half B, 1 E, 2 half B, 3 Bbar
 void launch_init_boundaries_fp64(State& s);
 void launch_push_fp64(State& s, int species, double external_bz);
-void launch_push_fp64_tile(State& s, int species, double external_bz);
 int launch_push_fp64_qed(State& s, int species, double external_bz);
 int launch_vacuum_fp64(State& s);
 void launch_field_energy_fp64(State& s);
@@ -131,7 +127,6 @@ void launch_field_energy_fp64(State& s);
 void launch_fields_mixed(State& s, int phase);
 void launch_init_boundaries_mixed(State& s);
 void launch_push_mixed(State& s, int species, double external_bz);
-void launch_push_mixed_tile(State& s, int species, double external_bz);
 void launch_field_energy_mixed(State& s);
 
 // ---- rebin and scans (qp_rebin.cu) ----

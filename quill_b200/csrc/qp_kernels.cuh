@@ -112,6 +112,60 @@ __device__ __forceinline__ bool inside(const Grid& g, int i, int j, int k) {
     return i > 0 && i < g.nx - 2 && j > 0 && j < g.ny - 2 && k > 0 && k < g.nz - 2;
 }
 
+// Warp-level segmented reduction over runs of equal keys in consecutive lanes
+// (particles are sorted by cell, so a cell's particles sit in neighbouring
+// lanes).  Lanes with key < 0 take no part.  On return the first lane of
+// each run holds the run's sum in v[] and `head` is true for it.  Every lane
+// of the warp must call this.
+template <typename T, int NV>
+__device__ __forceinline__ bool warp_run_sum(int key, T v[NV]) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int ukey = key >= 0 ? key : -1 - lane;  // non-members form runs of one
+    const int prev = __shfl_up_sync(full, ukey, 1);
+    const bool head = lane == 0 || prev != ukey;
+    const unsigned heads = __ballot_sync(full, head);
+    // lanes (lane, lane + d] belong to this run iff no head among them
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long span = ((1ull << d) - 1ull) << (lane + 1);
+        const bool same = lane + d < 32 && ((unsigned long long)heads & span) == 0ull;
+#pragma unroll
+        for (int a = 0; a < NV; a++) {
+            const T o = __shfl_down_sync(full, v[a], d);
+            if (same) v[a] += o;
+        }
+    }
+    return head && key >= 0;
+}
+
+// The 12 J contributions of single-segment moves, summed per run of equal
+// corner cell in the warp and added to J by the run's first lane.
+template <typename T>
+__device__ __forceinline__ void warp_deposit_runs(const Fields<T>& f, const Grid& g, int corner, T v[12]) {
+    if (warp_run_sum<T, 12>(corner, v)) {
+        const int c = corner, I = g.nynz, J = g.nz;
+        atomicAdd(f.jx + c + J + 1, v[0]);
+        atomicAdd(f.jx + c + 1, v[1]);
+        atomicAdd(f.jx + c + J, v[2]);
+        atomicAdd(f.jx + c, v[3]);
+        atomicAdd(f.jy + c + I + 1, v[4]);
+        atomicAdd(f.jy + c + 1, v[5]);
+        atomicAdd(f.jy + c + I, v[6]);
+        atomicAdd(f.jy + c, v[7]);
+        atomicAdd(f.jz + c + I + J, v[8]);
+        atomicAdd(f.jz + c + J, v[9]);
+        atomicAdd(f.jz + c + I, v[10]);
+        atomicAdd(f.jz + c, v[11]);
+    }
+}
+
+// Particles per new cell for the rebin, one atomic per run of equal cells.
+__device__ __forceinline__ void warp_count_runs(int32_t* count, int cell) {
+    int n[1] = {cell >= 0 ? 1 : 0};
+    if (warp_run_sum<int, 1>(cell, n)) atomicAdd(count + cell, n[0]);
+}
+
 struct PushArgs {
     double cmr, dt, dx, dy, dz, ext_bz;
     int n, sp, kind;

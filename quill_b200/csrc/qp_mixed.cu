@@ -24,13 +24,20 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
     return r;
 }
 
+// One thread per particle in traversal order (see k_push64): the move runs in
+// the particle's cell frame (offsets in [0, 1)); single-segment moves go
+// through the warp-level run reduction, crossing moves deposit directly.
 template <int PUSHER, int KIND>
-__global__ void __launch_bounds__(256) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
-                                                const int32_t* __restrict__ perm,
-                                                int32_t* __restrict__ newcell, PushArgs32 a) {
+__global__ void __launch_bounds__(256, 3) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
+                                                   const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
+                                                   int32_t* __restrict__ count, PushArgs32 a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
+    int corner = -1, nc = -1;
+    float v[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) v[k] = 0.0f;
     if (s < a.n) {
         const int p = perm[s];
         const int c0 = src.cell[p];
@@ -38,8 +45,6 @@ __global__ void __launch_bounds__(256) k_push32(Fields<float> f, Grid g, PStore3
         float o[3] = {src.ox[p], src.oy[p], src.oz[p]};
         float ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
         const float q = src.q[p];
-        int nc = -1;
-        int i1 = i0, j1 = j0, k1 = k0;
         if (!kill_layer(g, i0, j0, k0)) {
             float E[3], B[3];
             gather(f, g, i0, j0, k0, o[0], o[1], o[2], E, B);
@@ -49,6 +54,11 @@ __global__ void __launch_bounds__(256) k_push32(Fields<float> f, Grid g, PStore3
             float d[3] = {ux * t * a.idx, uy * t * a.idy, uz * t * a.idz};
             if (KIND == KIND_PHOTON) {
                 o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
+            } else if (floorf(o[0] + d[0]) == 0.0f && floorf(o[1] + d[1]) == 0.0f && floorf(o[2] + d[2]) == 0.0f) {
+                const int w[3] = {0, 0, 0};
+                seg_values(o, d, q, w, v);
+                corner = c0;
+                o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
             } else {
                 jdeposition(f, g, o, d, q, i0, j0, k0, a.status);
             }
@@ -57,7 +67,7 @@ __global__ void __launch_bounds__(256) k_push32(Fields<float> f, Grid g, PStore3
             o[0] = wrap_offset(o[0], si);
             o[1] = wrap_offset(o[1], sj);
             o[2] = wrap_offset(o[2], sk);
-            i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
+            const int i1 = i0 + si, j1 = j0 + sj, k1 = k0 + sk;
             const bool moved = si | sj | sk;
             if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
@@ -73,94 +83,8 @@ __global__ void __launch_bounds__(256) k_push32(Fields<float> f, Grid g, PStore3
             dc = 1;
         }
     }
-    block_diag(a.diag, a.sp, dq, de, dc);
-}
-
-// k_push32 with the current J and the rebin histogram accumulated per
-// k-line segment in shared memory (see k_push64_tile).
-template <int PUSHER, int KIND, int L>
-__global__ void __launch_bounds__(256, 3) k_push32_tile(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
-                                                        const int32_t* __restrict__ perm,
-                                                        int32_t* __restrict__ newcell,
-                                                        const int32_t* __restrict__ cell_start,
-                                                        int32_t* __restrict__ count, PushArgs32 a) {
-    using TS = TileSink<float, L>;
-    constexpr int NC = 9 * (L + 2);
-    __shared__ float sj[TS::SIZE];
-    __shared__ int scnt[NC];
-    const int k0 = blockIdx.x * L, j0 = blockIdx.y, i0 = blockIdx.z;
-    const int kend = min(k0 + L, g.nz);
-    const int c0 = cidx(g, i0, j0, k0);
-    const int pb = cell_start[c0], pe = cell_start[c0 + (kend - k0)];
-    if (pb == pe) return;  // uniform across the CTA
-    for (int e = threadIdx.x; e < TS::SIZE; e += blockDim.x) sj[e] = 0.0f;
-    for (int e = threadIdx.x; e < NC; e += blockDim.x) scnt[e] = 0;
-    __syncthreads();
-    TS sink;
-    sink.sm = sj; sink.f = f; sink.ti0 = i0 - 1; sink.tj0 = j0 - 1; sink.tk0 = k0 - 1;
-    double dq = 0.0, de = 0.0;
-    unsigned long long dc = 0;
-    for (int s = pb + threadIdx.x; s < pe; s += blockDim.x) {
-        const int p = perm[s];
-        const int cc = src.cell[p];
-        const int ci = cc / g.nynz, cj = (cc / g.nz) % g.ny, ck = cc - (cc / g.nz) * g.nz;
-        float o[3] = {src.ox[p], src.oy[p], src.oz[p]};
-        float ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
-        const float q = src.q[p];
-        int nc = -1;
-        int i1 = ci, j1 = cj, k1 = ck;
-        if (!kill_layer(g, ci, cj, ck)) {
-            float E[3], B[3];
-            gather(f, g, ci, cj, ck, o[0], o[1], o[2], E, B);
-            B[2] += a.ext_bz;
-            if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
-            const float t = a.dt / gm;
-            float d[3] = {ux * t * a.idx, uy * t * a.idy, uz * t * a.idz};
-            if (KIND == KIND_PHOTON) {
-                o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
-            } else {
-                jdeposition_to(sink, g, o, d, q, ci, cj, ck, a.status);
-            }
-            if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
-            int si, sj2, sk;
-            o[0] = wrap_offset(o[0], si);
-            o[1] = wrap_offset(o[1], sj2);
-            o[2] = wrap_offset(o[2], sk);
-            i1 = ci + si; j1 = cj + sj2; k1 = ck + sk;
-            const bool moved = si | sj2 | sk;
-            if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
-        }
-        newcell[s] = nc;
-        if (nc >= 0) {
-            dst.cell[s] = nc;
-            dst.ox[s] = o[0]; dst.oy[s] = o[1]; dst.oz[s] = o[2];
-            dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
-            dst.g[s] = gm; dst.q[s] = q;
-            if (dst.chi) dst.chi[s] = src.chi[p];
-            dq += (double)q;
-            de += KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
-            dc += 1;
-            const unsigned di = (unsigned)(i1 - (i0 - 1)), dj = (unsigned)(j1 - (j0 - 1)), dk = (unsigned)(k1 - (k0 - 1));
-            if (di < 3u && dj < 3u && dk < (unsigned)(L + 2)) atomicAdd(scnt + ((int)di * 3 + (int)dj) * (L + 2) + (int)dk, 1);
-            else atomicAdd(count + nc, 1);
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < TS::SIZE; e += blockDim.x) {
-        const float v = sj[e];
-        if (v == 0.0f) continue;
-        const int comp = e / (16 * TS::NK), r = e - comp * (16 * TS::NK);
-        const int i = sink.ti0 + r / (4 * TS::NK), j = sink.tj0 + (r / TS::NK) % 4, k = sink.tk0 + r % TS::NK;
-        if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) continue;
-        float* base = comp == 0 ? f.jx : (comp == 1 ? f.jy : f.jz);
-        atomicAdd(base + cidx(g, i, j, k), v);
-    }
-    for (int e = threadIdx.x; e < NC; e += blockDim.x) {
-        const int v = scnt[e];
-        if (v == 0) continue;
-        const int i = i0 - 1 + e / (3 * (L + 2)), j = j0 - 1 + (e / (L + 2)) % 3, k = k0 - 1 + e % (L + 2);
-        atomicAdd(count + cidx(g, i, j, k), v);
-    }
+    warp_deposit_runs(f, g, corner, v);
+    warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
 }
 
@@ -208,8 +132,11 @@ void zero_planes_mixed(State& s, const ZeroPlane* zp, int n) {
     }
 }
 
+// Push of one species; also leaves the particles-per-new-cell histogram in
+// sp.count (zeroed here).
 void launch_push_mixed(State& s, int si, double external_bz) {
     Species& sp = s.sp[si];
+    cudaMemsetAsync(sp.count, 0, (size_t)s.grid.nc * sizeof(int32_t), s.stream);
     if (sp.n == 0) return;
     PStore32 src, dst;
     src.cell = (int32_t*)sp.buf[sp.cur][0];
@@ -228,41 +155,11 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     const int nb = (int)((sp.n + 255) / 256);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LP(P, K) k_push32<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a)
+#define QP_LP(P, K) k_push32<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
     if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
     else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
 #undef QP_LP
-    s.launches++;
-}
-
-void launch_push_mixed_tile(State& s, int si, double external_bz) {
-    constexpr int L = 64;
-    Species& sp = s.sp[si];
-    cudaMemsetAsync(sp.count, 0, (size_t)s.grid.nc * sizeof(int32_t), s.stream);
-    if (sp.n == 0) return;
-    PStore32 src, dst;
-    src.cell = (int32_t*)sp.buf[sp.cur][0];
-    dst.cell = (int32_t*)sp.buf[1 - sp.cur][0];
-    float** ps[9] = {&src.ox, &src.oy, &src.oz, &src.ux, &src.uy, &src.uz, &src.g, &src.q, &src.chi};
-    float** pd[9] = {&dst.ox, &dst.oy, &dst.oz, &dst.ux, &dst.uy, &dst.uz, &dst.g, &dst.q, &dst.chi};
-    for (int a = 0; a < 9; a++) {
-        *ps[a] = (float*)sp.buf[sp.cur][1 + a];
-        *pd[a] = (float*)sp.buf[1 - sp.cur][1 + a];
-    }
-    PushArgs32 a;
-    a.cmr = (float)sp.cmr; a.dt = (float)s.prm.dt;
-    a.idx = (float)(1.0 / s.prm.dx); a.idy = (float)(1.0 / s.prm.dy); a.idz = (float)(1.0 / s.prm.dz);
-    a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
-    a.status = s.d_status; a.diag = s.d_diag;
-    dim3 grd((s.grid.nz + L - 1) / L, s.grid.ny, s.grid.nx);
-    Fields<float> f = fields32(s);
-    const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LT(P, K) k_push32_tile<P, K, L><<<grd, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.cell_start, sp.count, a)
-    if (sp.kind == KIND_PHOTON) QP_LT(QP_PUSHER_BORIS, KIND_PHOTON);
-    else if (vay) QP_LT(QP_PUSHER_VAY, KIND_LEPTON);
-    else QP_LT(QP_PUSHER_BORIS, KIND_LEPTON);
-#undef QP_LT
     s.launches++;
 }
 

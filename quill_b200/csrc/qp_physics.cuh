@@ -145,28 +145,30 @@ __device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const 
     sink.add(2, wi, wj, wk, c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third));
 }
 
-// Destination of the current contributions of the particles of one k-line
-// segment of L cells, (i0, j0, k0 .. k0+L-1): a shared-memory tile over
-// (i0-1 .. i0+2) x (j0-1 .. j0+2) x (k0-1 .. k0+L+1) per component, which
-// holds every contribution of a particle that moves less than a cell;
-// anything outside goes to HBM directly.
-template <typename T, int L>
-struct TileSink {
-    T* sm;
-    Fields<T> f;
-    int ti0, tj0, tk0;
-    static constexpr int NK = L + 3;
-    static constexpr int SIZE = 3 * 16 * NK;
-    __device__ __forceinline__ void add(int comp, int i, int j, int k, int c, T v) const {
-        const unsigned di = (unsigned)(i - ti0), dj = (unsigned)(j - tj0), dk = (unsigned)(k - tk0);
-        if (di < 4u && dj < 4u && dk < (unsigned)NK) {
-            atomicAdd(sm + ((comp * 4 + (int)di) * 4 + (int)dj) * NK + (int)dk, v);
-        } else {
-            T* base = comp == 0 ? f.jx : (comp == 1 ? f.jy : f.jz);
-            atomicAdd(base + c, v);
-        }
-    }
-};
+// The 12 contributions of one segment (same arithmetic and order as
+// seg_dep), returned instead of deposited; targets relative to the corner
+// cell c: jx at c+nz+1, c+1, c+nz, c; jy at c+I+1, c+1, c+I, c; jz at
+// c+I+nz, c+nz, c+I, c (I = ny*nz).
+template <typename T>
+__device__ __forceinline__ void seg_values(const T p[3], const T d[3], T q, const int w[3], T v[12]) {
+    const T xa = p[0] - T(w[0]), xb = T(1) - xa;
+    const T ya = p[1] - T(w[1]), yb = T(1) - ya;
+    const T za = p[2] - T(w[2]), zb = T(1) - za;
+    const T dx = d[0], dy = d[1], dz = d[2];
+    const T third = T(3);
+    v[0] = dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third);
+    v[1] = dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - dy * dz / third);
+    v[2] = dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - dy * dz / third);
+    v[3] = dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + dy * dz / third);
+    v[4] = dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + dx * dz / third);
+    v[5] = dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - dx * dz / third);
+    v[6] = dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - dx * dz / third);
+    v[7] = dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + dx * dz / third);
+    v[8] = dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + dx * dy / third);
+    v[9] = dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third);
+    v[10] = dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third);
+    v[11] = dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third);
+}
 
 // Three ratios sorted descending with the reference's tie handling
 // (`regulate`, low-level.cpp:316-366).

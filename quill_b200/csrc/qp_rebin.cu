@@ -16,6 +16,11 @@
 
 namespace qp {
 
+// For a destination cell c = (i, j, k) inside the grid, the particles that
+// can arrive come from the 3x3 neighbouring lines (i-di, j-dj); on each line
+// the source cells k+1, k, k-1 form one contiguous traversal range
+// [cs[(i-di, j-dj, k-1)], cs[(i-di, j-dj, k+2)]).
+
 // Number of particles whose new cell is c (one thread per destination cell).
 __global__ void __launch_bounds__(256) k_rebin_count(Grid g, const int32_t* __restrict__ cs,
                                                      const int32_t* __restrict__ newcell,
@@ -26,19 +31,19 @@ __global__ void __launch_bounds__(256) k_rebin_count(Grid g, const int32_t* __re
     int n = 0;
     if (inside(g, i, j, k)) {
         for (int di = -1; di <= 1; di++)
-            for (int dj = -1; dj <= 1; dj++)
-                for (int dk = -1; dk <= 1; dk++) {
-                    const int s = c - (di * g.nynz + dj * g.nz + dk);
-                    const int e = __ldg(cs + s + 1);
-                    for (int p = __ldg(cs + s); p < e; p++) n += (__ldg(newcell + p) == c);
-                }
+            for (int dj = -1; dj <= 1; dj++) {
+                const int l = c - di * g.nynz - dj * g.nz;
+                const int e = __ldg(cs + l + 2);
+                for (int p = __ldg(cs + l - 1); p < e; p++) n += (__ldg(newcell + p) == c);
+            }
     }
     count[c] = n;
 }
 
-// Fill perm for destination cell c from start[c]: arrivals from the source
-// cells in descending linear index ((i+1, j+1, k+1) first), each source
-// scanned from its last particle down; then the stayers in ascending order.
+// Fill perm for destination cell c from start[c] (after the particles born
+// in c, if any): arrivals from the source cells in descending linear index
+// ((i+1, j+1, k+1) first), each scanned from its last particle down, then
+// the stayers in ascending order.
 __global__ void __launch_bounds__(256) k_rebin_assign(Grid g, const int32_t* __restrict__ cs,
                                                       const int32_t* __restrict__ newcell,
                                                       const int32_t* __restrict__ start,
@@ -51,17 +56,17 @@ __global__ void __launch_bounds__(256) k_rebin_assign(Grid g, const int32_t* __r
     int pos = start[c] + (born ? born[c] : 0);
     const int end = start[c + 1];
     if (pos == end) return;
+    const int own_b = __ldg(cs + c), own_e = __ldg(cs + c + 1);
     for (int di = -1; di <= 1; di++)
-        for (int dj = -1; dj <= 1; dj++)
-            for (int dk = -1; dk <= 1; dk++) {
-                if (di == 0 && dj == 0 && dk == 0) continue;
-                const int s = c - (di * g.nynz + dj * g.nz + dk);
-                const int b = __ldg(cs + s);
-                for (int p = __ldg(cs + s + 1) - 1; p >= b; p--)
-                    if (__ldg(newcell + p) == c) perm[pos++] = p;
+        for (int dj = -1; dj <= 1; dj++) {
+            const int l = c - di * g.nynz - dj * g.nz;
+            const int b = __ldg(cs + l - 1);
+            for (int p = __ldg(cs + l + 2) - 1; p >= b; p--) {
+                if (di == 0 && dj == 0 && p >= own_b && p < own_e) continue;  // the cell's own particles
+                if (__ldg(newcell + p) == c) perm[pos++] = p;
             }
-    const int e = __ldg(cs + c + 1);
-    for (int p = __ldg(cs + c); p < e; p++)
+        }
+    for (int p = own_b; p < own_e; p++)
         if (__ldg(newcell + p) == c) perm[pos++] = p;
 }
 

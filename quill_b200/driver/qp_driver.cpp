@@ -1,0 +1,593 @@
+// qp_driver: QUILL's driver (src/main.cpp) for one GPU region, on top of the
+// libquill_b200 C ABI.
+//
+//   python3 <quill>/parse.py <conf> | qp_driver
+//
+// Reads the record stream QUILL's parse.py writes (name, value, units, "$"
+// per record, a lone "$" at the end; var::read, low-level.cpp:376-451), with
+// QUILL's parameter names, units and defaults for the supported subset
+// (below), builds the initial laser field (f_init_cos with the default
+// cos envelope, init.cpp:6-210) and the plasma films (film /
+// fill_cell_by_particles, init.cpp:402-646), runs the time loop of
+// main.cpp:2319-2432 through qp_step and writes QUILL's output files in its
+// formats so that python/resread.py reads them: log, N, energy, field slices
+// ex..bz (text or binary, fout.cpp:180-235), rho (and rho_p / rho_ph), and
+// phasespace (9 values per particle).
+//
+// Supported parameters: dx dy dz dt lambda ne xlength ylength zlength t_end
+// output_period a0 a0y a0z polarization xsigma ysigma zsigma x0 y0 z0 phase
+// b_sign phi external_bz solver pusher qed film x0film filmwidth gradwidth
+// y0film y1film z0film z1film nfilm mcr Tfilm vxfilm xnpic_film ynpic_film
+// znpic_film xnpic ynpic znpic ions data_folder output_mode
+// e_components_for_output b_components_for_output particles_for_output enthp
+// mwindow (off only) and two additions: precision (fp64 | mixed) and seed.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "quill_b200.h"
+
+namespace {
+
+const double PI = 3.141592653589793;
+const double PROTON_MASS = 1836.1526721;  // include/physical_constants.h
+
+// ---------------------------------------------------------------- input ----
+struct Var {
+    std::string name;
+    double value = 0;
+    std::string units;
+};
+
+// One record: name, value (or '#'), units or text (or '#'), '$'.
+std::vector<Var> read_stream(std::istream& in) {
+    std::vector<Var> vars;
+    std::string name;
+    while (in >> name) {
+        if (name == "$") break;
+        std::string val, units, end;
+        in >> val >> units >> end;
+        if (end != "$") throw std::runtime_error("malformed record for " + name);
+        Var v;
+        v.name = name;
+        v.value = (val == "#" || val.empty() || val[0] == '[') ? 0.0 : std::stod(val);
+        v.units = units == "#" ? "" : units;
+        vars.push_back(v);
+    }
+    return vars;
+}
+
+// find (low-level.cpp:453-471): first record with this name at or after
+// position `from`, else an empty record.
+const Var& find(const std::vector<Var>& v, const std::string& n, size_t from = 0, size_t* at = nullptr) {
+    static const Var empty;
+    for (size_t i = from; i < v.size(); i++)
+        if (v[i].name == n) {
+            if (at) *at = i;
+            return v[i];
+        }
+    if (at) *at = v.size();
+    return empty;
+}
+
+// lengths: um / fs / lambda -> c/omega (main.cpp:2616-2650 pattern)
+double length(const Var& v, double lambda_cm) {
+    double x = v.value;
+    if (v.units == "um") x = x * 1e-4 / lambda_cm;
+    else if (v.units == "fs") x = x * 1e-15 * 2.99792458e10 / lambda_cm;
+    return x * 2 * PI;
+}
+
+// ------------------------------------------------------------ parameters ---
+struct Film {
+    double x0 = 0, width = 0, grad = 0, y0 = 0, y1 = 0, z0 = 0, z1 = 0, ne = 0, mcr = 1, T = 0, vx = 0;
+    int xn = 0, yn = 0, zn = 0;
+};
+
+struct Config {
+    double dx, dy, dz, dt, lambda, ne = 0, xlength, ylength, zlength;
+    std::vector<double> t_end, output_period;
+    double a0y = 0, a0z = 0, xsigma = 0, ysigma = 0, zsigma = 0, x0 = 0, y00 = 0, z00 = 0, phase = 0, phi = 0;
+    bool b_sign = true;
+    double external_bz = 0;
+    int solver = QP_SOLVER_NDFX, pusher = QP_PUSHER_VAY;
+    bool qed = true;
+    std::vector<Film> films;
+    std::string ions = "off";
+    int xnpic = 1, ynpic = 1, znpic = 1;
+    std::string data_folder = "results";
+    bool binary = false;
+    std::string e_out = "y", b_out = "z", particles_for_output = "e";
+    int enthp = 1;
+    int precision = QP_PREC_FP64;
+    uint64_t seed = 0;
+    std::string polarization = "linear";
+};
+
+Config parse(const std::vector<Var>& v) {
+    Config c;
+    c.dx = find(v, "dx").value * 2 * PI;
+    c.dy = find(v, "dy").value * 2 * PI;
+    c.dz = find(v, "dz").value * 2 * PI;
+    c.dt = find(v, "dt").value * 2 * PI;
+    Var lam = find(v, "lambda");
+    c.lambda = lam.units == "um" ? lam.value * 1e-4 : lam.value;  // cm
+    if (!(c.lambda > 0)) throw std::runtime_error("lambda must be given");
+    Var ne = find(v, "ne");
+    c.ne = ne.units == "ncr" ? ne.value * 1.11485e+13 / c.lambda / c.lambda : ne.value;
+    if (!(c.dx > 0 && c.dy > 0 && c.dz > 0 && c.dt > 0))
+        throw std::runtime_error("dx, dy, dz and dt must be given (automatic dt/dx of main.cpp:2603-2615 is not supported)");
+    auto len_lambda = [&](const char* n) {
+        Var x = find(v, n);
+        if (x.units == "um") return x.value * 1e-4 / c.lambda * 2 * PI;
+        if (x.units == "fs") return x.value * 1e-15 * 2.99792458e10 / c.lambda * 2 * PI;
+        return x.value * 2 * PI;
+    };
+    c.xlength = len_lambda("xlength");
+    c.ylength = len_lambda("ylength");
+    c.zlength = len_lambda("zlength");
+    // t_end / output_period pairs (main.cpp:2652-2662)
+    size_t pos = 0;
+    while (true) {
+        size_t at;
+        const Var& te = find(v, "t_end", pos, &at);
+        if (at >= v.size() || te.value == 0) break;
+        double t = te.value * 2 * PI;
+        if (te.units == "um") t = te.value * 1e-4 / c.lambda * 2 * PI;
+        if (te.units == "fs") t = te.value * 1e-15 * 2.99792458e10 / c.lambda * 2 * PI;
+        size_t at2;
+        const Var& op = find(v, "output_period", at + 1, &at2);
+        double per = op.units == "t_end" ? op.value * t : op.value * 2 * PI;
+        if (!(per > 0)) per = t;
+        c.t_end.push_back(t);
+        c.output_period.push_back(per);
+        pos = at + 1;
+    }
+    if (c.t_end.empty()) throw std::runtime_error("t_end must be given");
+    // laser amplitude and polarisation (main.cpp:2727-2805)
+    c.xsigma = length(find(v, "xsigma"), c.lambda);
+    c.ysigma = length(find(v, "ysigma"), c.lambda);
+    c.zsigma = length(find(v, "zsigma"), c.lambda);
+    c.x0 = length(find(v, "x0"), c.lambda);
+    c.y00 = length(find(v, "y0"), c.lambda);
+    c.z00 = length(find(v, "z0"), c.lambda);
+    if (find(v, "a0").value != 0) c.a0y = find(v, "a0").value;
+    const Var& pol = find(v, "polarization");
+    if (pol.units == "circular") { c.a0z = c.a0y; c.polarization = "circular"; }
+    if (pol.units == "elliptic") { c.a0z = pol.value * c.a0y; c.polarization = "elliptic"; }
+    if (find(v, "a0y").value != 0) {
+        c.a0y = find(v, "a0y").value;
+        c.a0z = find(v, "a0z").value;
+    } else if (find(v, "a0z").value != 0) {
+        c.a0z = find(v, "a0z").value;
+        c.a0y = 0;
+    }
+    const Var& ph = find(v, "phase");
+    c.phase = ph.units == "pi" ? ph.value * PI : ph.value;
+    c.b_sign = find(v, "b_sign").value != -1;
+    const Var& phi = find(v, "phi");
+    c.phi = phi.units == "deg" ? phi.value * PI / 180 : phi.value;
+    const Var& env = find(v, "f_envelope");
+    if (!env.units.empty() && env.units != "cos") throw std::runtime_error("only the cos laser envelope is supported");
+    c.external_bz = find(v, "external_bz").value;
+    // solver / pusher / qed (main.cpp:3542-3584); defaults NDFX, Vay, QED on
+    const std::string sv = find(v, "solver").units, pu = find(v, "pusher").units;
+    if (sv == "fdtd") c.solver = QP_SOLVER_FDTD;
+    else if (sv == "five_point") c.solver = QP_SOLVER_FIVE_POINT;
+    else if (sv.empty() || sv == "ndfx") c.solver = QP_SOLVER_NDFX;
+    else throw std::runtime_error("Solver unknown: " + sv);
+    if (pu == "boris") c.pusher = QP_PUSHER_BORIS;
+    else if (pu.empty() || pu == "vay") c.pusher = QP_PUSHER_VAY;
+    else throw std::runtime_error("Pusher unknown: " + pu);
+    const std::string q = find(v, "qed").units;
+    c.qed = !(q == "off");
+    if (find(v, "mwindow").units != "off")
+        throw std::runtime_error("set mwindow = off: the moving window is not part of this build");
+    // films (main.cpp:3055-3229)
+    c.xnpic = (int)find(v, "xnpic").value; if (c.xnpic <= 0) c.xnpic = 1;
+    c.ynpic = (int)find(v, "ynpic").value; if (c.ynpic <= 0) c.ynpic = 1;
+    c.znpic = (int)find(v, "znpic").value; if (c.znpic <= 0) c.znpic = 1;
+    c.ions = find(v, "ions").units;
+    for (size_t i = 0; i < v.size(); i++) {
+        if (v[i].name != "film" || v[i].units != "on") continue;
+        Film f;
+        size_t s = i + 1;
+        auto fl = [&](const char* n) { return length(find(v, n, s), c.lambda); };
+        f.x0 = fl("x0film");
+        f.width = fl("filmwidth");
+        f.grad = fl("gradwidth");
+        f.y0 = fl("y0film");
+        f.y1 = find(v, "y1film", s).value == 0 ? c.ylength : fl("y1film");
+        f.z0 = fl("z0film");
+        f.z1 = find(v, "z1film", s).value == 0 ? c.zlength : fl("z1film");
+        const Var& n = find(v, "nfilm", s);
+        f.ne = n.units == "ncr" ? n.value * 1.11485e+13 / c.lambda / c.lambda : (n.units == "ne" ? n.value * c.ne : n.value);
+        f.mcr = find(v, "mcr", s).value == 0 ? 1 : find(v, "mcr", s).value;
+        f.T = find(v, "Tfilm", s).value;
+        f.vx = find(v, "vxfilm", s).value;
+        f.xn = (int)find(v, "xnpic_film", s).value;
+        f.yn = (int)find(v, "ynpic_film", s).value;
+        f.zn = (int)find(v, "znpic_film", s).value;
+        if (f.xn == 0 || f.yn == 0 || f.zn == 0) { f.xn = c.xnpic; f.yn = c.ynpic; f.zn = c.znpic; }
+        c.films.push_back(f);
+    }
+    if (!find(v, "data_folder").units.empty()) c.data_folder = find(v, "data_folder").units;
+    c.binary = find(v, "output_mode").units == "binary";
+    if (!find(v, "e_components_for_output").units.empty()) c.e_out = find(v, "e_components_for_output").units;
+    if (!find(v, "b_components_for_output").units.empty()) c.b_out = find(v, "b_components_for_output").units;
+    if (!find(v, "particles_for_output").units.empty()) c.particles_for_output = find(v, "particles_for_output").units;
+    c.enthp = (int)find(v, "enthp").value; if (c.enthp <= 0) c.enthp = 1;
+    const std::string pr = find(v, "precision").units;
+    if (pr == "mixed") c.precision = QP_PREC_MIXED;
+    c.seed = (uint64_t)find(v, "seed").value;
+    return c;
+}
+
+// --------------------------------------------------------- initial state ---
+struct Grid3 {
+    int nx, ny, nz;
+    long nc() const { return (long)nx * ny * nz; }
+    long at(int i, int j, int k) const { return ((long)i * ny + j) * nz + k; }
+};
+
+// f_init_cos with the cos envelope (sscos = 0) and append = true
+// (init.cpp:6-210): the pulse frame r0 points from (x1, y0, z0) towards the
+// box centre; E and B of the envelope-modulated wave are rotated into the box.
+void laser_cos(const Config& c, const Grid3& g, std::vector<double>* F, double a0y, double a0z, double xc,
+               double x1, double y0, double z0, double phi) {
+    const double xs = c.xsigma * 2 * std::sqrt(2 * PI) / 3;
+    const double ys = c.ysigma * 2 * std::sqrt(2 * PI) / 3;
+    const double zs = c.zsigma * 2 * std::sqrt(2 * PI) / 3;
+    const double y12 = 0.5 * g.ny * c.dy, z12 = 0.5 * g.nz * c.dz;
+    double r0x = std::sqrt(x1 * x1 + y0 * y0 + z0 * z0);
+    double r0y = -y0 / r0x, r0z = -z0 / r0x;
+    r0x = -x1 / r0x;
+    double y0x, y0y, y0z = std::sqrt(r0x * r0x + r0y * r0y);
+    if (y0z != 0) { y0x = -r0y / y0z; y0y = r0x / y0z; y0z = 0; }
+    else { y0x = 0; y0y = 1; y0z = 0; }
+    double z0x = r0y * y0z - r0z * y0y, z0y = r0z * y0x - r0x * y0z, z0z = r0x * y0y - r0y * y0x;
+    if (phi != 0) {
+        const double cs = std::cos(phi), sn = std::sin(phi);
+        const double yx = y0x, yy = y0y, yz = y0z, zx = z0x, zy = z0y, zz = z0z;
+        y0x = yx * cs + zx * sn; y0y = yy * cs + zy * sn; y0z = yz * cs + zz * sn;
+        z0x = zx * cs - yx * sn; z0y = zy * cs - yy * sn; z0z = zz * cs - yz * sn;
+    }
+    for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+            for (int k = 0; k < g.nz; k++) {
+                const double X = i * c.dx - xc, Y = j * c.dy - y12 - y0, Z = k * c.dz - z12 - z0;
+                const double x = r0x * X + r0y * Y + r0z * Z;
+                const double y = y0x * X + y0y * Y + y0z * Z;
+                const double z = z0x * X + z0y * Y + z0z * Z;
+                if (!(x < xs && x > -xs && y < ys && y > -ys && z < zs && z > -zs)) continue;
+                const double xi = x + c.phase;
+                const double cosx = std::cos(PI * x / 2 / xs), cosy = std::cos(PI * y / 2 / ys), cosz = std::cos(PI * z / 2 / zs);
+                const double sinx = std::sin(PI * x / 2 / xs), siny = std::sin(PI * y / 2 / ys), sinz = std::sin(PI * z / 2 / zs);
+                const double tr = cosy * cosy * cosz * cosz;
+                const double ey = a0y * tr * (std::cos(xi) * cosx * cosx - PI / xs * std::sin(xi) * cosx * sinx);
+                const double ez = a0z * tr * (std::sin(xi) * cosx * cosx + PI / xs * std::cos(xi) * cosx * sinx);
+                double bz = ey, by = -ez;
+                const double ex = a0y * std::sin(xi) * cosx * cosx * cosz * cosz * PI / ys * cosy * siny -
+                                  a0z * std::cos(xi) * cosx * cosx * cosy * cosy * PI / zs * cosz * sinz;
+                double bx = a0z * std::cos(xi) * cosx * cosx * PI / ys * cosz * cosz * cosy * siny +
+                            a0y * std::sin(xi) * cosx * cosx * cosy * cosy * PI / zs * cosz * sinz;
+                if (!c.b_sign) { bx = -bx; by = -by; bz = -bz; }
+                const long a = g.at(i, j, k);
+                F[0][a] += ex * r0x + ey * y0x + ez * z0x;
+                F[1][a] += ex * r0y + ey * y0y + ez * z0y;
+                F[2][a] += ex * r0z + ey * y0z + ez * z0z;
+                F[3][a] += bx * r0x + by * y0x + bz * z0x;
+                F[4][a] += bx * r0y + by * y0y + bz * z0y;
+                F[5][a] += bx * r0z + by * y0z + bz * z0z;
+            }
+}
+
+struct Parts {
+    std::vector<double> x, y, z, ux, uy, uz, g, q;
+    void add(double X, double Y, double Z, double UX, double UY, double UZ, double G, double Q) {
+        x.push_back(X); y.push_back(Y); z.push_back(Z);
+        ux.push_back(UX); uy.push_back(UY); uz.push_back(UZ); g.push_back(G); q.push_back(Q);
+    }
+};
+
+// fill_cell_by_particles (init.cpp:402-478): a regular in-cell lattice of
+// xn*yn*zn particles; thermal momenta drawn like the reference (gamma from
+// an exponential by rejection, isotropic direction, boost by the drift);
+// a zero drift leaves the direction unrotated (the reference divides by it).
+void fill_cell(Parts& P, double cmr, int ci, int cj, int ck, int xn, int yn, int zn, double n, double ux0, double T,
+               std::mt19937_64& rng) {
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    const double x0 = 0.5 / xn, y0 = 0.5 / yn, z0 = 0.5 / zn;
+    double q0 = 1 / double(xn * yn * zn) * n;
+    if (cmr < 0) q0 = -q0;
+    for (int ip = 0; ip < xn; ip++)
+        for (int jp = 0; jp < yn; jp++)
+            for (int kp = 0; kp < zn; kp++) {
+                const double X = x0 + ci + double(ip) / xn, Y = y0 + cj + double(jp) / yn, Z = z0 + ck + double(kp) / zn;
+                double ux = ux0, uy = 0, uz = 0;
+                if (T != 0 && cmr != 0) {
+                    const double u0 = std::fabs(ux0), v0 = u0 / std::sqrt(1 + u0 * u0);
+                    double gamma, a, b, cc, r;
+                    do { gamma = 1 + U(rng) * 5 * T; } while (U(rng) > std::exp(-(gamma - 1) / T));
+                    do {
+                        a = 2 * U(rng) - 1; b = 2 * U(rng) - 1; cc = 2 * U(rng) - 1;
+                        r = std::sqrt(a * a + b * b + cc * cc);
+                    } while (r > 1 || r == 0);
+                    a /= r; b /= r; cc /= r;
+                    const double vv = std::sqrt(1 - 1 / (gamma * gamma));
+                    a *= vv; b *= vv; cc *= vv;
+                    b = b * std::sqrt(1 - v0 * v0) / (1 + a * v0);
+                    cc = cc * std::sqrt(1 - v0 * v0) / (1 + a * v0);
+                    a = (a + v0) / (1 + a * v0);
+                    const double gg = 1 / std::sqrt(1 - a * a - b * b - cc * cc);
+                    const double sx = ux0 < 0 ? -1.0 : 1.0;
+                    ux = sx * a * gg; uy = b * gg; uz = cc * gg;
+                }
+                const double G = cmr != 0 ? std::sqrt(1 + ux * ux + uy * uy + uz * uz) : std::sqrt(ux * ux + uy * uy + uz * uz);
+                P.add(X, Y, Z, ux, uy, uz, G, q0);
+            }
+}
+
+// film (init.cpp:537-646) without transverse profile or y-gradient.
+void film(const Config& c, const Grid3& g, const Film& f, Parts& e, Parts* ion, double ion_cmr, Parts* pos,
+          std::mt19937_64& rng) {
+    int i0 = (int)(f.x0 / c.dx), i1 = (int)((f.x0 + f.width) / c.dx);
+    i0 = std::max(0, std::min(i0, g.nx));
+    i1 = std::max(0, std::min(i1, g.nx));
+    const double n_norm = f.ne / (1.11485e+13 / c.lambda / c.lambda);
+    const double ux0 = f.vx / std::sqrt(1 - f.vx * f.vx);
+    for (int i = i0; i < i1; i++)
+        for (int j = (int)(f.y0 / c.dy) + 1; j < (int)(f.y1 / c.dy) - 1; j++)
+            for (int k = (int)(f.z0 / c.dz) + 1; k < (int)(f.z1 / c.dz) - 1; k++) {
+                double nes = n_norm;
+                if (f.grad >= 0) {
+                    if (!(i >= (int)((f.x0 + f.grad) / c.dx))) nes = nes * (i * c.dx - f.x0) / f.grad;
+                } else {
+                    if (!(i >= (int)((f.x0 - f.grad) / c.dx))) nes = nes * (1 + (i * c.dx - f.x0) / f.grad);
+                }
+                if (!(nes > 0)) continue;
+                fill_cell(e, -1, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T, rng);
+                if (ion) fill_cell(*ion, ion_cmr, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T * ion_cmr, rng);
+                if (pos) fill_cell(*pos, 1, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T, rng);
+            }
+}
+
+// ------------------------------------------------------------- schedule ----
+// OutputIterations (parameters.cpp:6-48)
+struct Schedule {
+    std::vector<int> it;
+    std::vector<double> t;
+    Schedule(const std::vector<double>& t_end, const std::vector<double>& period, double dt) {
+        int prev = -1;
+        double t_begin = 0;
+        for (size_t i = 0; i < t_end.size(); i++) {
+            const int count = (int)((t_end[i] + 0.5 * dt - t_begin) / period[i]) + 1;
+            for (int j = 0; j < count; j++) {
+                const double time = t_begin + j * period[i];
+                const int iter = (int)std::round(time / dt);
+                if (iter > prev) { t.push_back(time); it.push_back(iter); prev = iter; }
+            }
+            t_begin = t_end[i];
+        }
+        const int last = (int)std::round(t_end.back() / dt);
+        if (last > prev) { t.push_back(t_end.back()); it.push_back(last); }
+    }
+    static std::string suffix(double time) {
+        const double v = (int)std::round(time / 2 / PI * 100.) / 100.;
+        char b[64];
+        snprintf(b, sizeof b, "%g", v);
+        return b;
+    }
+};
+
+// ---------------------------------------------------------------- output ---
+// Field slice file (fout.cpp:180-235 and the yz plane writers): for each i
+// the xy line at k = nz/2 then the xz line at j = ny/2, then the yz plane at
+// i = ix.  Text: one value per line with the default ostream precision.
+void write_slice(const std::string& path, const double* F, const Grid3& g, int ix, bool binary) {
+    std::vector<double> a;
+    a.reserve((size_t)g.nx * (g.ny + g.nz) + (size_t)g.ny * g.nz);
+    for (int i = 0; i < g.nx; i++) {
+        for (int j = 0; j < g.ny; j++) a.push_back(F[g.at(i, j, g.nz / 2)]);
+        for (int k = 0; k < g.nz; k++) a.push_back(F[g.at(i, g.ny / 2, k)]);
+    }
+    for (int j = 0; j < g.ny; j++)
+        for (int k = 0; k < g.nz; k++) a.push_back(F[g.at(ix, j, k)]);
+    if (binary) {
+        std::ofstream f(path, std::ios::out | std::ios::binary);
+        f.write((const char*)a.data(), a.size() * sizeof(double));
+    } else {
+        std::ofstream f(path);
+        for (double v : a) f << v << "\n";
+    }
+}
+
+}  // namespace
+
+int main() {
+    std::ios::sync_with_stdio(false);
+    Config c;
+    try {
+        c = parse(read_stream(std::cin));
+    } catch (const std::exception& e) {
+        std::cerr << "qp_driver: " << e.what() << std::endl;
+        return 1;
+    }
+    Grid3 g{(int)(c.xlength / c.dx), (int)(c.ylength / c.dy), (int)(c.zlength / c.dz)};
+    mkdir(c.data_folder.c_str(), 0755);
+
+    // species table: electrons, then ions per film / positrons, then QED
+    qp_params p;
+    memset(&p, 0, sizeof p);
+    p.nx = g.nx; p.ny = g.ny; p.nz = g.nz;
+    p.dx = c.dx; p.dy = c.dy; p.dz = c.dz; p.dt = c.dt;
+    p.lambda_cm = c.lambda;
+    p.solver = c.solver; p.pusher = c.pusher; p.qed = c.qed; p.precision = c.precision;
+    p.seed = c.seed;
+    int n = 0;
+    const int sp_e = n; p.cmr[n++] = -1;
+    int sp_pos = -1, sp_ph = -1;
+    std::vector<int> sp_ion(c.films.size(), -1);
+    std::vector<double> icmr;
+    if (c.ions == "on")
+        for (size_t f = 0; f < c.films.size(); f++) {
+            sp_ion[f] = n;
+            icmr.push_back(1 / (PROTON_MASS * c.films[f].mcr));
+            p.cmr[n++] = icmr.back();
+        }
+    if (c.ions == "positrons" || c.qed) { sp_pos = n; p.cmr[n++] = 1; }
+    if (c.qed) { sp_ph = n; p.cmr[n++] = 0; }
+    p.n_species = n;
+    qp_handle* h = nullptr;
+    if (qp_create(&p, &h) != QP_OK) {
+        std::cerr << "qp_driver: " << qp_last_error(nullptr) << std::endl;
+        return 1;
+    }
+
+    // initial fields: the default call of init_fields (main.cpp:1186-1189),
+    // plus the counter-propagating pulse for phi != 0 (main.cpp:1190-1192)
+    std::vector<double> F[6];
+    for (auto& f : F) f.assign(g.nc(), 0.0);
+    if (c.a0y != 0 || c.a0z != 0) {
+        laser_cos(c, g, F, c.a0y, c.a0z, c.xlength / 2 + c.x0, c.x0, c.y00, c.z00, 0);
+        if (c.phi != 0) laser_cos(c, g, F, c.a0y, c.a0z, c.xlength / 2 - c.x0, -c.x0, -c.y00, -c.z00, c.phi);
+    }
+    int r = qp_load_fields(h, F[0].data(), F[1].data(), F[2].data(), F[3].data(), F[4].data(), F[5].data());
+    if (r == QP_OK) r = qp_init_boundaries(h);
+    // films, loaded species by species (cell order is sorted inside the library)
+    std::mt19937_64 rng(c.seed * 0x9E3779B97F4A7C15ull + 1);
+    Parts E;
+    std::vector<Parts> I(c.films.size());
+    Parts Pz;
+    for (size_t f = 0; f < c.films.size(); f++)
+        film(c, g, c.films[f], E, sp_ion[f] >= 0 ? &I[f] : nullptr, sp_ion[f] >= 0 ? icmr[f] : 0,
+             c.ions == "positrons" ? &Pz : nullptr, rng);
+    auto load = [&](int s, Parts& P) {
+        if (r != QP_OK || P.x.empty()) return;
+        r = qp_load_particles(h, s, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
+                              P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
+    };
+    load(sp_e, E);
+    for (size_t f = 0; f < c.films.size(); f++)
+        if (sp_ion[f] >= 0) load(sp_ion[f], I[f]);
+    if (sp_pos >= 0) load(sp_pos, Pz);
+    if (r != QP_OK) {
+        std::cerr << "qp_driver: " << qp_last_error(h) << std::endl;
+        qp_destroy(h);
+        return 1;
+    }
+
+    // log in the reference's name/value layout (main.cpp:3611-3785 subset)
+    {
+        std::ofstream L(c.data_folder + "/log");
+        L << "dx\n" << c.dx / 2 / PI << "\ndy\n" << c.dy / 2 / PI << "\ndz\n" << c.dz / 2 / PI << "\ndt\n" << c.dt / 2 / PI << "\n";
+        L << "nx\n" << g.nx << "\nny\n" << g.ny << "\nnz\n" << g.nz << "\n";
+        L << "lambda\n" << c.lambda << "\nne\n" << c.ne << "\n";
+        for (size_t i = 0; i < c.t_end.size(); i++)
+            L << "t_end\n" << c.t_end[i] / 2 / PI << "\noutput_period\n" << c.output_period[i] / 2 / PI << "\n";
+        L << "xsigma\n" << c.xsigma / 2 / PI << "\nysigma\n" << c.ysigma / 2 / PI << "\nzsigma\n" << c.zsigma / 2 / PI << "\n";
+        L << "x0fout\n" << c.xlength / 2 / 2 / PI << "\n";
+        L << "a0y\n" << c.a0y << "\na0z\n" << c.a0z << "\n";
+        L << "mwindow\noff\n";
+        L << "e_components_for_output\n" << c.e_out << "\nb_components_for_output\n" << c.b_out << "\n";
+        L << "n_ion_populations\n" << icmr.size() << "\n";
+        for (double v : icmr) L << "icmr\n" << v << "\n";
+        L << "xnpic\n" << c.xnpic << "\nynpic\n" << c.ynpic << "\nznpic\n" << c.znpic << "\n";
+        L << "particles_for_output\n" << c.particles_for_output << "\n";
+        L << "enthp\n" << c.enthp << "\n";
+        L << "n_sr\n1\n$\n";
+        L << "catching\noff\ndump_photons\noff\nqed\n" << (c.qed ? "on" : "off") << "\n";
+        L << "balancing\noff\noutput_mode\n" << (c.binary ? 1 : 0) << "\n";
+        L << "#------------------------------\n";
+        L << "polarization = " << c.polarization << "\n";
+        L << "solver = " << (c.solver == QP_SOLVER_FDTD ? "fdtd" : c.solver == QP_SOLVER_NDFX ? "ndfx" : "five_point") << "\n";
+        L << "pusher = " << (c.pusher == QP_PUSHER_BORIS ? "boris" : "vay") << "\n";
+        L << "precision = " << (c.precision == QP_PREC_MIXED ? "mixed" : "fp64") << "\n";
+    }
+
+    // time loop (main.cpp:2319-2432)
+    Schedule sch(c.t_end, c.output_period, c.dt);
+    std::ofstream fN(c.data_folder + "/N"), fE(c.data_folder + "/energy");
+    size_t out_i = 0;
+    std::vector<double> all(12 * (size_t)g.nc());
+    const int ix = (int)((c.xlength - c.xlength / 2) / c.dx);
+    for (int l = 0; l <= sch.it.back(); l++) {
+        qp_diag d;
+        if (qp_step(h, 1, c.external_bz, &d) != QP_OK) {
+            std::cerr << "qp_driver: step " << l << ": " << qp_last_error(h) << std::endl;
+            qp_destroy(h);
+            return 1;
+        }
+        fN << d.N_e << '\t' << d.N_p << '\t' << d.N_ph << std::endl;  // write_N, main.cpp:160-170
+        fE << d.energy_f << '\t' << d.energy_e << '\t' << d.energy_p << '\t' << d.energy_ph;  // write_energy
+        for (int m = 0; m < d.n_ion; m++) fE << '\t' << d.ienergy[m];
+        fE << std::endl;
+        if (out_i < sch.it.size() && l == sch.it[out_i]) {
+            const std::string sfx = Schedule::suffix(sch.t[out_i]);
+            qp_dump_fields(h, all.data());
+            const size_t NC = (size_t)g.nc();
+            const char* en[3] = {"ex", "ey", "ez"};
+            const char* bn[3] = {"bx", "by", "bz"};
+            for (int a = 0; a < 3; a++) {
+                const char comp = "xyz"[a];
+                if (c.e_out.find(comp) != std::string::npos)
+                    write_slice(c.data_folder + "/" + en[a] + sfx, all.data() + a * NC, g, ix, c.binary);
+                if (c.b_out.find(comp) != std::string::npos)
+                    write_slice(c.data_folder + "/" + bn[a] + sfx, all.data() + (3 + a) * NC, g, ix, c.binary);
+            }
+            // densities: CIC deposition of every species (rhodeposition,
+            // deposition.cpp:358-429) into rho / rho_p / rho_ph
+            const char* names[3] = {"rho", "rho_p", "rho_ph"};
+            const int sps[3] = {sp_e, sp_pos, sp_ph};
+            for (int w = 0; w < 3; w++) {
+                if (sps[w] < 0) continue;
+                int64_t np = 0;
+                qp_count_particles(h, sps[w], &np);
+                std::vector<double> x(np), y(np), z(np), q(np), rho(NC, 0.0);
+                if (np) qp_dump_particles(h, sps[w], np, x.data(), y.data(), z.data(), nullptr, nullptr, nullptr,
+                                          nullptr, q.data(), nullptr, nullptr);
+                for (int64_t t = 0; t < np; t++) {
+                    const int i = (int)std::floor(x[t]), j = (int)std::floor(y[t]), k = (int)std::floor(z[t]);
+                    if (!(i > 0 && i < g.nx - 2 && j > 0 && j < g.ny - 2 && k > 0 && k < g.nz - 2)) continue;
+                    const double xa = x[t] - i, xb = 1 - xa, ya = y[t] - j, yb = 1 - ya, za = z[t] - k, zb = 1 - za;
+                    const double qq = q[t];
+                    rho[g.at(i, j, k)] += qq * xb * yb * zb;
+                    rho[g.at(i + 1, j, k)] += qq * xa * yb * zb;
+                    rho[g.at(i, j + 1, k)] += qq * xb * ya * zb;
+                    rho[g.at(i, j, k + 1)] += qq * xb * yb * za;
+                    rho[g.at(i + 1, j + 1, k)] += qq * xa * ya * zb;
+                    rho[g.at(i + 1, j, k + 1)] += qq * xa * yb * za;
+                    rho[g.at(i, j + 1, k + 1)] += qq * xb * ya * za;
+                    rho[g.at(i + 1, j + 1, k + 1)] += qq * xa * ya * za;
+                }
+                write_slice(c.data_folder + "/" + names[w] + sfx, rho.data(), g, ix, c.binary);
+                // phasespace of the species selected by particles_for_output:
+                // q, x, y, z in lambda, ux, uy, uz, g, chi, every enthp-th
+                const char key = "epg"[w];
+                if (c.particles_for_output.find(key) != std::string::npos || (w == 2 && c.particles_for_output.find("ph") != std::string::npos)) {
+                    std::vector<double> ux(np), uy(np), uz(np), gg(np), chi(np);
+                    if (np) qp_dump_particles(h, sps[w], np, x.data(), y.data(), z.data(), ux.data(), uy.data(),
+                                              uz.data(), gg.data(), q.data(), chi.data(), nullptr);
+                    std::ofstream P(c.data_folder + "/phasespace" + std::string(w == 0 ? "" : (w == 1 ? "_p" : "_ph")) + sfx);
+                    for (int64_t t = 0; t < np; t += c.enthp)
+                        P << q[t] << '\n' << x[t] * c.dx / 2 / PI << '\n' << y[t] * c.dy / 2 / PI << '\n'
+                          << z[t] * c.dz / 2 / PI << '\n' << ux[t] << '\n' << uy[t] << '\n' << uz[t] << '\n'
+                          << gg[t] << '\n' << chi[t] << '\n';
+                }
+            }
+            out_i++;
+        }
+    }
+    qp_destroy(h);
+    return 0;
+}

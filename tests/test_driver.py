@@ -1,0 +1,93 @@
+"""The C++ driver (quill_b200/qp_driver) reads QUILL's parse.py record
+stream and writes QUILL's output files.  The stream is produced here the way
+parse.py produces it (name / value / units / "$"); the outputs are read back
+the way python/resread.py reads them (log name/value pairs, t_data rows,
+density slices of nx*ny + nx*nz + ny*nz values)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.conftest import gpu_available
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "quill_b200", "qp_driver")
+
+CONF = [  # (key, value, units) as parse.py emits them: plain numbers get '#' units
+    ("dx", "0.0625", "#"), ("dy", "0.0625", "#"), ("dz", "0.0625", "#"), ("dt", "0.03125", "#"),
+    ("lambda", "1", "um"), ("ne", "0.1", "ncr"),
+    ("xlength", "2", "lambda"), ("ylength", "1.5", "lambda"), ("zlength", "1.5", "lambda"),
+    ("t_end", "0.5", "lambda"), ("output_period", "0.25", "lambda"),
+    ("a0", "5", "#"), ("xsigma", "0.5", "lambda"), ("ysigma", "0.4", "lambda"), ("zsigma", "0.4", "lambda"),
+    ("x0", "-0.5", "lambda"),
+    ("solver", "#", "fdtd"), ("pusher", "#", "boris"), ("qed", "#", "off"), ("mwindow", "#", "off"),
+    ("film", "#", "on"), ("x0film", "1", "lambda"), ("filmwidth", "0.5", "lambda"), ("gradwidth", "0.1", "lambda"),
+    ("nfilm", "0.1", "ncr"), ("Tfilm", "0.01", "#"), ("xnpic_film", "2", "#"), ("ynpic_film", "1", "#"),
+    ("znpic_film", "1", "#"),
+    ("e_components_for_output", "#", "xyz"), ("b_components_for_output", "#", "z"),
+    ("particles_for_output", "#", "e"), ("seed", "3", "#"),
+]
+
+
+def stream(conf, folder):
+    lines = []
+    for k, v, u in conf + [("data_folder", "#", folder)]:
+        lines += [k, v, u, "$"]
+    lines.append("$")
+    return "\n".join(lines) + "\n"
+
+
+def read_log(path):
+    d = {}
+    with open(path) as f:
+        it = iter(f)
+        for line in it:
+            line = line.strip()
+            if line in ("nx", "ny", "nz"):
+                d[line] = int(next(it))
+            elif line in ("dx", "dy", "dz", "dt", "t_end", "output_period"):
+                d[line] = float(next(it))
+    return d
+
+
+@pytest.mark.gpu
+def test_driver_runs_conf_stream_and_writes_reference_formats(tmp_path):
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200 import build
+    build.build()
+    folder = str(tmp_path / "results")
+    r = subprocess.run([DRIVER], input=stream(CONF, folder), text=True, capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    log = read_log(os.path.join(folder, "log"))
+    nx, ny, nz = log["nx"], log["ny"], log["nz"]
+    assert (nx, ny, nz) == (32, 24, 24)
+    # N and energy: one tab-separated row per step, 0..last iteration (t_end / dt = 16)
+    for name, cols in (("N", 3), ("energy", 4)):
+        rows = [ln.split("\t") for ln in open(os.path.join(folder, name)).read().strip().splitlines()]
+        assert len(rows) == 17 and all(len(x) == cols for x in rows)
+    e = np.array([[float(v) for v in ln.split("\t")] for ln in open(os.path.join(folder, "energy"))])
+    assert e[0, 0] > 0 and e[:, 1].max() > 0
+    n = np.array([[float(v) for v in ln.split("\t")] for ln in open(os.path.join(folder, "N"))])
+    assert n[0, 0] > 0
+    # field and density slices at t = 0, 0.25, 0.5 lambda
+    for t in ("0", "0.25", "0.5"):
+        for name in ("ex", "ey", "ez", "bz", "rho"):
+            vals = np.loadtxt(os.path.join(folder, name + t))
+            assert vals.size == nx * ny + nx * nz + ny * nz
+        ps = open(os.path.join(folder, "phasespace" + t)).read().split()
+        assert len(ps) % 9 == 0 and len(ps) > 0
+    # the laser is in the box and the plasma moved: fields and density differ over time
+    ey0, ey1 = np.loadtxt(os.path.join(folder, "ey0")), np.loadtxt(os.path.join(folder, "ey0.5"))
+    assert np.abs(ey0).max() > 1 and not np.allclose(ey0, ey1)
+
+
+def test_driver_rejects_moving_window(tmp_path):
+    """The reference's default mwindow is on (main.cpp:2932-2938); without
+    mwindow = off the driver refuses before touching a device."""
+    from quill_b200 import build
+    build.build()
+    conf = [c for c in CONF if c[0] != "mwindow"]
+    r = subprocess.run([DRIVER], input=stream(conf, str(tmp_path / "r")), text=True, capture_output=True, timeout=60)
+    assert r.returncode != 0 and "mwindow" in r.stderr
