@@ -160,6 +160,16 @@ int qp_launch_count(qp_handle* h, int64_t* out);
  * mathcal_W(e,b)).  e_s = lambda_cm / 2.4263086e-10 (main.cpp:2276). */
 int qp_eval_qed_rates(int device, double lambda_cm, int64_t n, const double* in, double* out);
 
+/* Same results as qp_eval_qed_rates, for callers that cannot allocate GPU
+ * memory (their device memory is owned by another allocator, or they cannot
+ * afford the device-wide synchronisation of cudaFree).  No counterpart in
+ * the reference.  Allocates nothing: inputs and outputs are staged in a
+ * fixed array inside the library (at most 16384 samples per call; larger n
+ * is rejected with QP_ERR_ARG).  All calls share that array: calls that
+ * overlap on the GPU race.  The first call on a device looks the array up
+ * and should come before any stream capture.  Errors: qp_last_error(NULL). */
+int qp_eval_qed_rates_noalloc(int device, double lambda_cm, int64_t n, const double* in, double* out);
+
 /* Per-phase CUDA-event timing of qp_step on the handle's stream: enable
  * (resets the totals) or disable.  No reference counterpart (the reference
  * logs coarse times() wall clocks only, main.cpp:2228-2230). */

@@ -103,6 +103,7 @@ def load_library(path: str | None = None):
         "qp_launch_count": (C.c_int, [VP, I64P]),
         "qp_set_timing": (C.c_int, [VP, C.c_int]),
         "qp_eval_qed_rates": (C.c_int, [C.c_int, D, I64, DP, DP]),
+        "qp_eval_qed_rates_noalloc": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
     }
     for name, (res, args) in sig.items():

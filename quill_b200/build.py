@@ -32,6 +32,7 @@ SOURCES = [
     ("qp_mixed.cu", []),
     ("qp_rebin.cu", []),
     ("qp_load.cu", []),
+    ("qp_noalloc.cu", []),
     ("qp_api.cu", []),
 ]
 HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh"]

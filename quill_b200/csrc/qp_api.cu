@@ -155,6 +155,8 @@ static thread_local std::string g_create_error;
 
 namespace qp {
 cudaError_t launch_qed_rates(int n, const double* d_in, double* d_out, double e_s, cudaStream_t st);
+// Message for qp_last_error(NULL) from entry points without a handle.
+void set_global_error(const std::string& msg) { g_create_error = msg; }
 }
 
 #define QP_H_CHECK(h)                              \
