@@ -217,6 +217,7 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.grid.nynz = p.ny * p.nz;
     s.grid.nc = p.nx * p.ny * p.nz;
     s.field_elem = s.fp64 ? 8 : 4;
+    if (const char* mb = getenv("QP_PUSH_MINBLOCKS")) s.push_minblocks = atoi(mb) == 2 ? 2 : 3;
     cudaError_t e = cudaSetDevice(p.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;

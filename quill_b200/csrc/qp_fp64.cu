@@ -6,74 +6,56 @@
 
 namespace qp {
 
-// One particle: gather, push, displacement, current deposition, new cell
-// (-1 = erased; place(), plist.cpp:7-39).  A move that stays inside its cell
-// (one segment) returns its 12 contributions in v[] and its cell in *corner
-// for the warp-level run reduction; moves that cross faces deposit their
-// segments directly.  Photons fly straight without current.
-// advance.cpp:90-387 with QED off: photons :155-252, leptons and ions
-// :253-371.
-template <int PUSHER, int KIND>
-__device__ __forceinline__ int push_one64(const Fields<double>& f, const Grid& g, const PushArgs& a, double pos[3],
-                                          double& ux, double& uy, double& uz, double& gm, double q, int* corner,
-                                          double v[12]) {
-    const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
-    if (kill_layer(g, i0, j0, k0)) return -1;
-    double E[3], B[3];
-    gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
-    B[2] += a.ext_bz;
-    if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
-    // particle::get_displacement (containers.cpp:58-67), then per-axis
-    // division by the cell size (advance.cpp:281-284)
-    const double t = a.dt / gm;
-    double d[3] = {ux * t, uy * t, uz * t};
-    d[0] = d[0] / a.dx;
-    d[1] = d[1] / a.dy;
-    d[2] = d[2] / a.dz;
-    if (KIND == KIND_PHOTON) {
-        pos[0] = pos[0] + d[0];
-        pos[1] = pos[1] + d[1];
-        pos[2] = pos[2] + d[2];
-    } else {
-        const int w[3] = {ifloor(pos[0]), ifloor(pos[1]), ifloor(pos[2])};
-        if (w[0] == ifloor(pos[0] + d[0]) && w[1] == ifloor(pos[1] + d[1]) && w[2] == ifloor(pos[2] + d[2])) {
-            seg_values(pos, d, q, w, v);
-            *corner = cidx(g, w[0], w[1], w[2]);
-            pos[0] = pos[0] + d[0];
-            pos[1] = pos[1] + d[1];
-            pos[2] = pos[2] + d[2];
-        } else {
-            jdeposition(f, g, pos, d, q, 0, 0, 0, a.status);
-        }
-    }
-    if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
-    const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
-    const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
-    if (!moved || inside(g, i1, j1, k1)) return cidx(g, i1, j1, k1);
-    return -1;
-}
-
-// One thread per particle in traversal order.  The particle is read through
-// perm from the previous layout and written at its traversal position into
-// the other buffer; newcell and the particles-per-new-cell histogram
-// (count) feed the rebin.
-template <int PUSHER, int KIND>
-__global__ void __launch_bounds__(256, 3) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
+// One thread per particle in traversal order (advance.cpp:90-387 with QED
+// off: photons fly straight without current, :155-252; leptons and ions are
+// pushed and deposit, :253-371).  The particle is read through perm from the
+// previous layout and written at its traversal position into the other
+// buffer.  The current goes through the warp's segment-slot run reduction
+// (deposit_runs).  newcell (-1 = erased, place(), plist.cpp:7-39) and the
+// particles-per-new-cell histogram (count) feed the rebin.
+template <int PUSHER, int KIND, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
-    int corner = -1, nc = -1;
-    double v[12];
-#pragma unroll
-    for (int k = 0; k < 12; k++) v[k] = 0.0;
+    int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+    bool live = false, active = false;
+    double pos[3] = {0.0, 0.0, 0.0}, d[3] = {0.0, 0.0, 0.0};
+    double ux = 0.0, uy = 0.0, uz = 0.0, gm = 1.0, q = 0.0;
     if (s < a.n) {
-        const int p = perm[s];
-        double pos[3] = {src.x[p], src.y[p], src.z[p]};
-        double ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
-        const double q = src.q[p];
-        nc = push_one64<PUSHER, KIND>(f, g, a, pos, ux, uy, uz, gm, q, &corner, v);
+        p = perm[s];
+        pos[0] = src.x[p]; pos[1] = src.y[p]; pos[2] = src.z[p];
+        ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
+        q = src.q[p];
+        i0 = (int)pos[0]; j0 = (int)pos[1]; k0 = (int)pos[2];
+        live = !kill_layer(g, i0, j0, k0);  // p_boundary, plist.cpp:73-102
+        if (live) {
+            double E[3], B[3];
+            gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
+            B[2] += a.ext_bz;
+            if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
+            // particle::get_displacement (containers.cpp:58-67), then per-axis
+            // division by the cell size (advance.cpp:281-284)
+            const double t = a.dt / gm;
+            d[0] = ux * t; d[1] = uy * t; d[2] = uz * t;
+            d[0] = d[0] / a.dx; d[1] = d[1] / a.dy; d[2] = d[2] / a.dz;
+            if (KIND == KIND_PHOTON) {
+                pos[0] = pos[0] + d[0]; pos[1] = pos[1] + d[1]; pos[2] = pos[2] + d[2];
+            } else {
+                active = true;
+            }
+            if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+        }
+    }
+    deposit_runs(f, g, pos, d, q, 0, 0, 0, active, a.status);
+    if (s < a.n) {
+        if (live) {
+            const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
+            const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
+            if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
+        }
         newcell[s] = nc;
         if (nc >= 0) {
             dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
@@ -85,7 +67,6 @@ __global__ void __launch_bounds__(256, 3) k_push64(Fields<double> f, Grid g, PSt
             dc = 1;
         }
     }
-    warp_deposit_runs(f, g, corner, v);
     warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
 }
@@ -463,7 +444,11 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     const int nb = (int)((sp.n + 255) / 256);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LP(P, K) k_push64<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+#define QP_LP(P, K)                                                                                          \
+    if (s.push_minblocks == 2)                                                                                \
+        k_push64<P, K, 2><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
+    else                                                                                                      \
+        k_push64<P, K, 3><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
     if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
     else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);

@@ -97,6 +97,9 @@ struct State {
     int64_t step_index = 0;
     bool boundaries_done = false;
     int sp_e = -1, sp_p = -1, sp_ph = -1;  // QED species (cmr -1, +1, 0)
+    // CTAs per SM the FP64 push's register budget targets (2: no spills,
+    // 3: more warps with some spills); QP_PUSH_MINBLOCKS selects
+    int push_minblocks = 3;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
     // diagnostics + J reset)

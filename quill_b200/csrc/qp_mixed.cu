@@ -25,8 +25,8 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
 }
 
 // One thread per particle in traversal order (see k_push64): the move runs in
-// the particle's cell frame (offsets in [0, 1)); single-segment moves go
-// through the warp-level run reduction, crossing moves deposit directly.
+// the particle's cell frame (offsets in [0, 1)), the current through the
+// warp's segment-slot run reduction (deposit_runs).
 template <int PUSHER, int KIND>
 __global__ void __launch_bounds__(256, 3) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
@@ -34,35 +34,36 @@ __global__ void __launch_bounds__(256, 3) k_push32(Fields<float> f, Grid g, PSto
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
-    int corner = -1, nc = -1;
-    float v[12];
-#pragma unroll
-    for (int k = 0; k < 12; k++) v[k] = 0.0f;
+    int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+    bool live = false, active = false;
+    float o[3] = {0.f, 0.f, 0.f}, d[3] = {0.f, 0.f, 0.f};
+    float ux = 0.f, uy = 0.f, uz = 0.f, gm = 1.f, q = 0.f;
     if (s < a.n) {
-        const int p = perm[s];
+        p = perm[s];
         const int c0 = src.cell[p];
-        const int i0 = c0 / g.nynz, j0 = (c0 / g.nz) % g.ny, k0 = c0 - (c0 / g.nz) * g.nz;
-        float o[3] = {src.ox[p], src.oy[p], src.oz[p]};
-        float ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
-        const float q = src.q[p];
-        if (!kill_layer(g, i0, j0, k0)) {
+        i0 = c0 / g.nynz; j0 = (c0 / g.nz) % g.ny; k0 = c0 - (c0 / g.nz) * g.nz;
+        o[0] = src.ox[p]; o[1] = src.oy[p]; o[2] = src.oz[p];
+        ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
+        q = src.q[p];
+        live = !kill_layer(g, i0, j0, k0);
+        if (live) {
             float E[3], B[3];
             gather(f, g, i0, j0, k0, o[0], o[1], o[2], E, B);
             B[2] += a.ext_bz;
             if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
             const float t = a.dt / gm;
-            float d[3] = {ux * t * a.idx, uy * t * a.idy, uz * t * a.idz};
+            d[0] = ux * t * a.idx; d[1] = uy * t * a.idy; d[2] = uz * t * a.idz;
             if (KIND == KIND_PHOTON) {
                 o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
-            } else if (floorf(o[0] + d[0]) == 0.0f && floorf(o[1] + d[1]) == 0.0f && floorf(o[2] + d[2]) == 0.0f) {
-                const int w[3] = {0, 0, 0};
-                seg_values(o, d, q, w, v);
-                corner = c0;
-                o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
             } else {
-                jdeposition(f, g, o, d, q, i0, j0, k0, a.status);
+                active = true;
             }
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+        }
+    }
+    deposit_runs(f, g, o, d, q, i0, j0, k0, active, a.status);
+    if (s < a.n) {
+        if (live) {
             int si, sj, sk;
             o[0] = wrap_offset(o[0], si);
             o[1] = wrap_offset(o[1], sj);
@@ -83,7 +84,6 @@ __global__ void __launch_bounds__(256, 3) k_push32(Fields<float> f, Grid g, PSto
             dc = 1;
         }
     }
-    warp_deposit_runs(f, g, corner, v);
     warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
 }
