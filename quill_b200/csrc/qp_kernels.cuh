@@ -162,33 +162,36 @@ __device__ __forceinline__ void warp_deposit_runs(const Fields<T>& f, const Grid
     }
 }
 
-// Current deposition of the whole warp's moves, segment slot by segment slot
-// (deposition.cpp:41-356): slot 0 is every move's first segment (corner =
-// the particle's cell), slots 1..3 the segments after face crossings.  In
-// each slot the contributions are summed over runs of equal corner cells in
-// the warp and added to J by the run's first lane.  The segment arithmetic
-// per crossing case is the reference's (see jdeposition_to).  p is advanced
-// segment by segment.  Every lane of the warp must call this; lanes with
-// active == false take no part.
+// Current deposition of the whole warp's moves (deposition.cpp:41-356).
+// Every move's first segment starts in the particle's own cell, so the first
+// segments of a cell's particles share their 12 targets: they are summed over
+// runs of equal cells in the warp and added to J once per run.  Moves that
+// cross faces then deposit their further segments directly.  The segment
+// arithmetic per crossing case is the reference's (see jdeposition_to); p is
+// advanced segment by segment.  Every lane of the warp must call this; lanes
+// with active == false take no part.
 template <typename T>
 __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, T p[3], const T d[3], T q, int bi,
                                              int bj, int bk, bool active, unsigned int* status) {
-    const unsigned full = 0xffffffffu;
     int c1x = 0, c1y = 0, c1z = 0, c2x = 0, c2y = 0, c2z = 0;
-    int nseg = 0, nx_ = 0;
+    int nx_ = 0;
     bool cx = false, cy = false, cz = false;
     // case data: 1 crossing: u = first segment; 2: u0 = p1, u1 = p2 - p1,
     // u2 = 1 - p2, fa / sa2 = axes of the first / second crossing; 3: u =
-    // (vx, vy, vz) of the sorted crossing fractions
+    // (vx, vy, vz), the crossing fractions sorted descending
     T u0 = T(0), u1 = T(0), u2 = T(0);
     int fa = 0, sa2 = 0;
+    T v[12];
+    int corner = -1;
     if (active) {
         c1x = ifloor(p[0]); c1y = ifloor(p[1]); c1z = ifloor(p[2]);
         c2x = ifloor(p[0] + d[0]); c2y = ifloor(p[1] + d[1]); c2z = ifloor(p[2] + d[2]);
         cx = c1x != c2x; cy = c1y != c2y; cz = c1z != c2z;
         nx_ = (int)cx + (int)cy + (int)cz;
-        nseg = nx_ + 1;
-        if (nx_ == 1) {
+        T s[3];
+        if (nx_ == 0) {
+            s[0] = d[0]; s[1] = d[1]; s[2] = d[2];
+        } else if (nx_ == 1) {
             const T pa = cx ? p[0] : (cy ? p[1] : p[2]);
             const T da = cx ? d[0] : (cy ? d[1] : d[2]);
             const int ma = cx ? max(c1x, c2x) : (cy ? max(c1y, c2y) : max(c1z, c2z));
@@ -196,6 +199,7 @@ __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, 
             u0 = cx ? sa : d[0] * sa / da;
             u1 = cy ? sa : d[1] * sa / da;
             u2 = cz ? sa : d[2] * sa / da;
+            s[0] = u0; s[1] = u1; s[2] = u2;
         } else if (nx_ == 2) {
             const bool A0 = cx && !cy, B0 = cx && cy;
             const T pA = A0 ? p[0] : p[1], dA = A0 ? d[0] : d[1];
@@ -211,64 +215,56 @@ __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, 
             u0 = p1;
             u1 = p2 - p1;
             u2 = T(1) - p2;
-        } else if (nx_ == 3) {
+            s[0] = d[0] * u0; s[1] = d[1] * u0; s[2] = d[2] * u0;
+        } else {
             const T path0 = (T(max(c1x, c2x)) - p[0]) / d[0];
             const T path1 = (T(max(c1y, c2y)) - p[1]) / d[1];
             const T path2 = (T(max(c1z, c2z)) - p[2]) / d[2];
             sort3_desc(path0, path1, path2, u0, u1, u2);
+            s[0] = d[0] * u2; s[1] = d[1] * u2; s[2] = d[2] * u2;
         }
+        const int w0[3] = {c1x, c1y, c1z};
+        const int wi = bi + c1x, wj = bj + c1y, wk = bk + c1z;
+        if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= g.nx || wj + 1 >= g.ny || wk + 1 >= g.nz) {
+            atomicOr(status, (unsigned int)ST_BOUNDS);
+        } else {
+            seg_values(p, s, q, w0, v);
+            corner = cidx(g, wi, wj, wk);
+        }
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
     }
-    int w[3] = {c1x, c1y, c1z};
-    for (int sg = 0; sg < 4; sg++) {
-        const bool has = sg < nseg;
-        if (!__any_sync(full, has)) break;
-        T v[12];
-        int corner = -1;
-        if (has) {
+    if (corner < 0) {
+#pragma unroll
+        for (int k = 0; k < 12; k++) v[k] = T(0);
+    }
+    warp_deposit_runs(f, g, corner, v);
+    if (nx_ > 0) {
+        GlobalSink<T> sink{f};
+        int w[3] = {c1x, c1y, c1z};
+        for (int sg = 1; sg <= nx_; sg++) {
             T s[3];
-            if (nx_ == 0) {
-                s[0] = d[0]; s[1] = d[1]; s[2] = d[2];
-            } else if (nx_ == 1) {
-                if (sg == 0) { s[0] = u0; s[1] = u1; s[2] = u2; }
-                else {
-                    s[0] = d[0] - u0; s[1] = d[1] - u1; s[2] = d[2] - u2;
-                    if (cx) w[0] = c2x;
-                    if (cy) w[1] = c2y;
-                    if (cz) w[2] = c2z;
-                }
+            if (nx_ == 1) {
+                s[0] = d[0] - u0; s[1] = d[1] - u1; s[2] = d[2] - u2;
+                if (cx) w[0] = c2x;
+                if (cy) w[1] = c2y;
+                if (cz) w[2] = c2z;
             } else if (nx_ == 2) {
-                const T fr = sg == 0 ? u0 : (sg == 1 ? u1 : u2);
+                const T fr = sg == 1 ? u1 : u2;
                 s[0] = d[0] * fr; s[1] = d[1] * fr; s[2] = d[2] * fr;
                 const int ax = sg == 1 ? fa : sa2;
-                if (sg > 0) {
-                    if (ax == 0) w[0] = c2x;
-                    if (ax == 1) w[1] = c2y;
-                    if (ax == 2) w[2] = c2z;
-                }
+                if (ax == 0) w[0] = c2x;
+                if (ax == 1) w[1] = c2y;
+                if (ax == 2) w[2] = c2z;
             } else {
-                // fractions vz, vy - vz, vx - vy, 1 - vx (u0 = vx, u1 = vy, u2 = vz)
-                const T fr = sg == 0 ? u2 : (sg == 1 ? u1 - u2 : (sg == 2 ? u0 - u1 : T(1) - u0));
+                const T fr = sg == 1 ? u1 - u2 : (sg == 2 ? u0 - u1 : T(1) - u0);
                 s[0] = d[0] * fr; s[1] = d[1] * fr; s[2] = d[2] * fr;
-                if (sg > 0) {
-                    w[0] = ifloor(p[0] + T(0.5) * s[0]);
-                    w[1] = ifloor(p[1] + T(0.5) * s[1]);
-                    w[2] = ifloor(p[2] + T(0.5) * s[2]);
-                }
+                w[0] = ifloor(p[0] + T(0.5) * s[0]);
+                w[1] = ifloor(p[1] + T(0.5) * s[1]);
+                w[2] = ifloor(p[2] + T(0.5) * s[2]);
             }
-            const int wi = bi + w[0], wj = bj + w[1], wk = bk + w[2];
-            if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= g.nx || wj + 1 >= g.ny || wk + 1 >= g.nz) {
-                atomicOr(status, (unsigned int)ST_BOUNDS);
-            } else {
-                seg_values(p, s, q, w, v);
-                corner = cidx(g, wi, wj, wk);
-            }
+            seg_dep(sink, g, p, s, q, w, bi, bj, bk, status);
             p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
         }
-        if (corner < 0) {
-#pragma unroll
-            for (int k = 0; k < 12; k++) v[k] = T(0);
-        }
-        warp_deposit_runs(f, g, corner, v);
     }
 }
 
