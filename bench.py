@@ -51,6 +51,12 @@ def hbm_peak():
 # x y z ux uy uz g q and writes all but q; the fused field step reads E B J,
 # writes E B Bbar, the deposit flush writes J once)
 BYTES = {"fp64": (120, 168), "mixed": (68, 84)}
+# DRAM traffic of one push launch per particle (dram__bytes_read.sum +
+# dram__bytes_write.sum over the particles of the launch), from one ncu
+# capture of k_push64 / k_push32 on the same physics at 160^3 (15,250,622
+# particles).  At fixed ppc the traffic grows with the particle count, so the
+# figure is scaled by Np.
+TRAFFIC_PER_PARTICLE = {"fp64": 2498516000 / 15250622, "mixed": 1427013632 / 15250622}
 
 
 class Clocks:
@@ -380,7 +386,9 @@ def main():
                                                                      t["phase_ms"])},
             "roofline": {"kernel": "push_deposit (k_push64)" if prec == "fp64" else "push_deposit (k_push32)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": np_avg * TRAFFIC_PER_PARTICLE[prec],
+                         "traffic_source": "ncu capture at 160^3 scaled by the particle count",
                          "algorithmic_bytes_per_launch": np_avg * bp},
             "step_roofline_frac": (np_avg * bp + nc * bc) / (ms * 1e-3 / t["steps"]) / 1e9 / peak,
             "energy_drift": (w1 - w0) / w0 if w0 else None,
