@@ -180,6 +180,22 @@ int qp_set_timing(qp_handle* h, int enable);
  * diagnostics; *steps = timed steps (nullable). */
 int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
 
+/* Discrete adjoint (no reference counterpart): runs nsteps steps from the
+ * handle's current state and returns the loss L = energy_e after the last
+ * step (compute_energy's electron kinetic energy, fout.cpp:87-138) with its
+ * exact gradients with respect to the six field planes as loaded by
+ * qp_load_fields (grad_fields: 6*nx*ny*nz doubles, Ex Ey Ez Bx By Bz, the
+ * zeroing of qp_init_boundaries applied) and to every electron's weight q
+ * (grad_q: one double per particle, in the traversal order qp_dump_particles
+ * returns at the start).  Covers FP64, FDTD, Boris, QED off, one species of
+ * cmr -1; qp_init_boundaries must have run.  The state is saved every
+ * `every` steps and each segment is re-run forward once for the backward
+ * sweep (memory: about (nsteps/every) states + every step records).  The
+ * handle is left in its state at entry.  Pointers may be host or device
+ * memory; each of loss, grad_fields and grad_q is nullable. */
+int qp_adjoint_energy(qp_handle* h, int nsteps, int every, double external_bz, double* grad_fields,
+                      double* grad_q, double* loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,7 @@ def load_library(path: str | None = None):
         "qp_eval_qed_rates": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_eval_qed_rates_noalloc": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
+        "qp_adjoint_energy": (C.c_int, [VP, C.c_int, C.c_int, D, DP, DP, DP]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -254,6 +255,20 @@ class Region:
         n = C.c_int64()
         self._check(self.lib.qp_get_timing(self.h, _dp(ms), C.byref(n)))
         return ms, n.value
+
+    def adjoint_energy(self, nsteps: int, every: int = 32, external_bz: float = 0.0):
+        """Run nsteps steps from the current state and return (L, dL/dfields,
+        dL/dq): L = energy_e after the last step, dL/dfields of shape
+        (6, nx, ny, nz) for the planes as loaded (Ex Ey Ez Bx By Bz), dL/dq per
+        particle of species 0 in its traversal order at entry.  The region is
+        left in its state at entry."""
+        n = self.count(0)
+        gf = np.zeros((6,) + self.shape)
+        gq = np.zeros(max(n, 1))
+        loss = C.c_double()
+        self._check(self.lib.qp_adjoint_energy(self.h, nsteps, every, external_bz, _dp(gf), _dp(gq),
+                                               C.byref(loss)))
+        return loss.value, gf, gq[:n]
 
     def launch_count(self) -> int:
         n = C.c_int64()

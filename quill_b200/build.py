@@ -29,13 +29,15 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, extra flags)
 SOURCES = [
     ("qp_fp64.cu", ["--fmad=false"]),
-    ("qp_mixed.cu", []),
+    # FP32 path: approximate division / square root (within 2 ulp), denormals flushed
+    ("qp_mixed.cu", ["--prec-div=false", "--prec-sqrt=false", "--ftz=true"]),
     ("qp_rebin.cu", []),
     ("qp_load.cu", []),
     ("qp_noalloc.cu", []),
+    ("qp_adjoint.cu", ["--fmad=false"]),
     ("qp_api.cu", []),
 ]
-HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh"]
+HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh", "qp_dual.cuh"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

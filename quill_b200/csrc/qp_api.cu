@@ -107,6 +107,15 @@ static int ensure_capacity(State& s, int si, int64_t need) {
     if (sp.newcell) cudaFree(sp.newcell);
     QP_CUDA_CHECK(s, cudaMalloc(&sp.newcell, cap * sizeof(int32_t)));
     sp.cap = cap;
+    // the rebin's list of long cells: at most cap / (REBIN_LONG_SEG + 1)
+    const int64_t need_long = cap / (REBIN_LONG_SEG + 1) + 2;
+    if (s.long_cap < need_long) {
+        cudaFree(s.long_list);
+        s.long_list = nullptr;
+        s.long_cap = 0;
+        QP_CUDA_CHECK(s, cudaMalloc(&s.long_list, need_long * sizeof(int32_t)));
+        s.long_cap = need_long;
+    }
     return QP_OK;
 }
 
@@ -123,8 +132,6 @@ static void free_state(State* s) {
         cudaFree(sp.cell_start);
         cudaFree(sp.cell_next);
         cudaFree(sp.count);
-        cudaFree(sp.born);
-        cudaFree(sp.born_fill);
         cudaFree(sp.d_counter);
     }
     for (auto& sn : s->snap) {
@@ -136,6 +143,8 @@ static void free_state(State* s) {
     cudaFree(s->d_diag);
     cudaFreeHost(s->h_diag);
     cudaFree(s->d_status);
+    cudaFree(s->long_list);
+    s->long_list = nullptr;
     cudaFree(s->scan_tmp);
     for (auto& e : s->ev)
         if (e) cudaEventDestroy(e);
@@ -143,11 +152,85 @@ static void free_state(State* s) {
     s->stream = nullptr;
 }
 
+int snapshot_take(State& s, State::Snap& sn) {
+    const size_t nc = (size_t)s.grid.nc;
+    if (!sn.fields) QP_CUDA_CHECK(s, cudaMalloc(&sn.fields, 12 * nc * s.field_elem));
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.fields, s.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    for (auto& v : sn.arrays)
+        for (void* p : v) cudaFree(p);
+    sn.arrays.assign(s.sp.size(), std::vector<void*>(11, nullptr));
+    sn.n.assign(s.sp.size(), 0);
+    sn.cap.assign(s.sp.size(), 0);
+    sn.slots.assign(s.sp.size(), 0);
+    sn.cell_start.resize(s.sp.size(), nullptr);
+    for (size_t i = 0; i < s.sp.size(); i++) {
+        Species& sp = s.sp[i];
+        const int64_t cap = sp.cap;
+        sn.cap[i] = cap;
+        sn.n[i] = sp.n;
+        sn.slots[i] = sp.slots;
+        if (cap > 0) {
+            for (int a = 0; a < 10; a++) {
+                if (!sp.buf[sp.cur][a]) continue;
+                QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][a], cap * arr_elem(s, a)));
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][a], sp.buf[sp.cur][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
+            }
+            QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][10], cap * 4));
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][10], sp.perm, cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+        }
+        if (!sn.cell_start[i]) QP_CUDA_CHECK(s, cudaMalloc(&sn.cell_start[i], (nc + 1) * 4));
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.cell_start[i], sp.cell_start, (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
+    }
+    sn.step_index = s.step_index;
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    sn.valid = true;
+    return QP_OK;
+}
+
+int snapshot_restore(State& s, State::Snap& sn) {
+    if (!sn.valid) { s.err = "checkpoint slot is empty"; return QP_ERR_STATE; }
+    const size_t nc = (size_t)s.grid.nc;
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(s.fields, sn.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
+    for (size_t i = 0; i < s.sp.size(); i++) {
+        Species& sp = s.sp[i];
+        const int64_t cap = sn.cap[i];
+        int r = ensure_capacity(s, (int)i, cap);
+        if (r != QP_OK) return r;
+        if (cap > 0) {
+            for (int a = 0; a < 10; a++) {
+                if (!sp.buf[sp.cur][a] || !sn.arrays[i][a]) continue;
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.buf[sp.cur][a], sn.arrays[i][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
+            }
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.perm, sn.arrays[i][10], cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+        }
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.cell_start, sn.cell_start[i], (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
+        sp.n = sn.n[i];
+        sp.slots = sn.slots[i];
+    }
+    s.step_index = sn.step_index;
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    return QP_OK;
+}
+
+void snapshot_free(State::Snap& sn) {
+    cudaFree(sn.fields);
+    sn.fields = nullptr;
+    for (auto& v : sn.arrays)
+        for (void* p : v) cudaFree(p);
+    sn.arrays.clear();
+    for (auto* p : sn.cell_start) cudaFree(p);
+    sn.cell_start.clear();
+    sn.valid = false;
+}
+
 }  // namespace qp
 
 struct qp_handle {
     qp::State st;
 };
+
+qp::State* qp::state_of(qp_handle* h) { return &h->st; }
 
 using namespace qp;
 
@@ -216,8 +299,11 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.grid.nx = p.nx; s.grid.ny = p.ny; s.grid.nz = p.nz;
     s.grid.nynz = p.ny * p.nz;
     s.grid.nc = p.nx * p.ny * p.nz;
+    s.grid.div_nz.init((uint32_t)p.nz);
+    s.grid.div_nynz.init((uint32_t)(p.ny * p.nz));
     s.field_elem = s.fp64 ? 8 : 4;
-    if (const char* mb = getenv("QP_PUSH_MINBLOCKS")) s.push_minblocks = atoi(mb) == 2 ? 2 : 3;
+    if (const char* mb = getenv("QP_PUSH_MINBLOCKS")) s.push_minblocks = atoi(mb) == 2 ? 2 : (atoi(mb) == 4 ? 4 : 3);
+    if (const char* mb = getenv("QP_PUSH_MINBLOCKS_MIXED")) s.push_minblocks_mixed = atoi(mb) == 4 ? 4 : 3;
     cudaError_t e = cudaSetDevice(p.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;
@@ -241,8 +327,6 @@ int qp_create(const qp_params* prm, qp_handle** out) {
         if (sp.cmr == 1 && s.sp_p < 0) s.sp_p = i;
         if (sp.cmr == 0 && s.sp_ph < 0) s.sp_ph = i;
         if (p.qed) {
-            if (e == cudaSuccess) e = cudaMalloc(&sp.born, nc * sizeof(int32_t));
-            if (e == cudaSuccess) e = cudaMalloc(&sp.born_fill, nc * sizeof(int32_t));
             if (e == cudaSuccess) e = cudaMalloc(&sp.d_counter, sizeof(int));
             if (e == cudaSuccess) e = cudaMemsetAsync(sp.d_counter, 0, sizeof(int), s.stream);
         }
@@ -415,7 +499,6 @@ int qp_load_particles(qp_handle* h, int si, int64_t n, const double* x, const do
     if (n == 0) return QP_OK;
     if (!x || !y || !z || !ux || !uy || !uz || !g || !q) { s.err = "null particle array"; return QP_ERR_ARG; }
     Species& sp = s.sp[si];
-    const Grid gr = s.grid;
     const int64_t slot0 = sp.slots;
     if (slot0 + n >= (int64_t)INT32_MAX) { s.err = "particle count exceeds 2^31-1"; return QP_ERR_CAPACITY; }
     int r = ensure_capacity(s, si, slot0 + n);
@@ -780,71 +863,14 @@ int qp_dump_particles(qp_handle* h, int si, int64_t cap, double* x, double* y, d
 
 int qp_checkpoint(qp_handle* h, int slot) {
     QP_H_CHECK(h);
-    State& s = h->st;
     if (slot < 0 || slot > 3) return QP_ERR_ARG;
-    auto& sn = s.snap[slot];
-    const size_t nc = (size_t)s.grid.nc;
-    if (!sn.fields) QP_CUDA_CHECK(s, cudaMalloc(&sn.fields, 12 * nc * s.field_elem));
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.fields, s.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
-    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    for (auto& v : sn.arrays)
-        for (void* p : v) cudaFree(p);
-    sn.arrays.assign(s.sp.size(), std::vector<void*>(11, nullptr));
-    sn.n.assign(s.sp.size(), 0);
-    sn.cap.assign(s.sp.size(), 0);
-    sn.slots.assign(s.sp.size(), 0);
-    sn.cell_start.resize(s.sp.size(), nullptr);
-    for (size_t i = 0; i < s.sp.size(); i++) {
-        Species& sp = s.sp[i];
-        const int64_t cap = sp.cap;
-        sn.cap[i] = cap;
-        sn.n[i] = sp.n;
-        sn.slots[i] = sp.slots;
-        if (cap > 0) {
-            for (int a = 0; a < 10; a++) {
-                if (!sp.buf[sp.cur][a]) continue;
-                QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][a], cap * arr_elem(s, a)));
-                QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][a], sp.buf[sp.cur][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
-            }
-            QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][10], cap * 4));
-            QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][10], sp.perm, cap * 4, cudaMemcpyDeviceToDevice, s.stream));
-        }
-        if (!sn.cell_start[i]) QP_CUDA_CHECK(s, cudaMalloc(&sn.cell_start[i], (nc + 1) * 4));
-        QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.cell_start[i], sp.cell_start, (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
-    }
-    sn.step_index = s.step_index;
-    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    sn.valid = true;
-    return QP_OK;
+    return snapshot_take(h->st, h->st.snap[slot]);
 }
 
 int qp_restore(qp_handle* h, int slot) {
     QP_H_CHECK(h);
-    State& s = h->st;
     if (slot < 0 || slot > 3) return QP_ERR_ARG;
-    auto& sn = s.snap[slot];
-    if (!sn.valid) { s.err = "checkpoint slot is empty"; return QP_ERR_STATE; }
-    const size_t nc = (size_t)s.grid.nc;
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(s.fields, sn.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
-    for (size_t i = 0; i < s.sp.size(); i++) {
-        Species& sp = s.sp[i];
-        const int64_t cap = sn.cap[i];
-        int r = ensure_capacity(s, (int)i, cap);
-        if (r != QP_OK) return r;
-        if (cap > 0) {
-            for (int a = 0; a < 10; a++) {
-                if (!sp.buf[sp.cur][a] || !sn.arrays[i][a]) continue;
-                QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.buf[sp.cur][a], sn.arrays[i][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
-            }
-            QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.perm, sn.arrays[i][10], cap * 4, cudaMemcpyDeviceToDevice, s.stream));
-        }
-        QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.cell_start, sn.cell_start[i], (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
-        sp.n = sn.n[i];
-        sp.slots = sn.slots[i];
-    }
-    s.step_index = sn.step_index;
-    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    return QP_OK;
+    return snapshot_restore(h->st, h->st.snap[slot]);
 }
 
 }  // extern "C"

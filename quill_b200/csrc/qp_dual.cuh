@@ -4,11 +4,15 @@
 // local Jacobian-vector products they contract with the adjoint variables.
 // Branches (cell floors, crossing order) are taken on the value part, so the
 // derivative is that of the branch the forward step took.
+// The type and its functions live in qp::ad so that they are found by
+// argument-dependent lookup for Dual arguments only and do not hide the
+// math library's sqrt / floor for double inside namespace qp.
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace qp {
+namespace ad {
 
 template <int N>
 struct Dual {
@@ -94,4 +98,6 @@ template <int N> __device__ __forceinline__ bool operator<(const Dual<N>& a, con
 template <int N> __device__ __forceinline__ double floor(const Dual<N>& a) { return ::floor(a.v); }
 template <int N> __device__ __forceinline__ bool isfinite(const Dual<N>& a) { return ::isfinite(a.v); }
 
+}  // namespace ad
+using ad::Dual;
 }  // namespace qp

@@ -18,6 +18,9 @@ struct SolverCoef {
     double nax, nay, naz, nbx, nby, nbz;
 };
 
+// Coefficients of the three solvers for a parameter set (qp_api.cu).
+SolverCoef solver_coef(const qp_params& p);
+
 template <typename T>
 struct Coef {
     T dtdx, dtdy, dtdz, dx, dy, dz;

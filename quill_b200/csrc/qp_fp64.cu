@@ -447,6 +447,8 @@ void launch_push_fp64(State& s, int si, double external_bz) {
 #define QP_LP(P, K)                                                                                          \
     if (s.push_minblocks == 2)                                                                                \
         k_push64<P, K, 2><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
+    else if (s.push_minblocks == 4)                                                                           \
+        k_push64<P, K, 4><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
     else                                                                                                      \
         k_push64<P, K, 3><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
     if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);

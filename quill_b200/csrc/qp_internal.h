@@ -22,10 +22,28 @@ enum StatusBits {
     ST_CAPACITY = 1u << 2,  // append beyond a store's capacity (dropped)
 };
 
+// Division of a non-negative int32 by a fixed divisor d >= 2 with one
+// multiply-high and a shift (round-up reciprocal m = ceil(2^(31+l) / d),
+// l = ceil(log2 d); exact for every n < 2^31).
+struct FastDiv {
+    uint32_t m = 0;
+    int sh = 0;  // l - 1
+    void init(uint32_t d) {
+        int l = 0;
+        while ((1ull << l) < d) l++;
+        m = (uint32_t)(((1ull << (31 + l)) + d - 1) / d);
+        sh = l - 1;
+    }
+#ifdef __CUDACC__
+    __device__ __forceinline__ int div(int n) const { return (int)(__umulhi((uint32_t)n, m) >> sh); }
+#endif
+};
+
 struct Grid {
     int nx, ny, nz;
     int nynz;
     int nc;  // nx*ny*nz < 2^31
+    FastDiv div_nz, div_nynz;
 };
 
 // Fields: 12 planes of nc elements (E, B, J, Bbar), element type T.
@@ -60,12 +78,11 @@ struct Species {
     void* buf[2][10] = {{nullptr}};
     int cur = 0;
     int32_t* perm = nullptr;       // traversal position -> slot in buf[cur]
-    int32_t* newcell = nullptr;    // cell after this push (-1 = erased), by traversal position
+    int32_t* newcell = nullptr;    // cell after this push (-1 = erased), by traversal position;
+                                   // also the rebin's scratch (swapped with perm)
     int32_t* cell_start = nullptr; // nc+1, traversal order at the start of a step
     int32_t* cell_next = nullptr;  // nc+1, traversal order after the rebin
     int32_t* count = nullptr;      // nc, rebin histogram
-    int32_t* born = nullptr;       // nc, particles born per cell in a push (QED)
-    int32_t* born_fill = nullptr;  // nc, placement counters for the born
     int* d_counter = nullptr;      // device append counter (QED)
 };
 
@@ -97,9 +114,11 @@ struct State {
     int64_t step_index = 0;
     bool boundaries_done = false;
     int sp_e = -1, sp_p = -1, sp_ph = -1;  // QED species (cmr -1, +1, 0)
-    // CTAs per SM the FP64 push's register budget targets (2: no spills,
-    // 3: more warps with some spills); QP_PUSH_MINBLOCKS selects
+    // CTAs per SM the FP64 push's register budget targets (2, 3 or 4; more
+    // CTAs, fewer registers per thread); QP_PUSH_MINBLOCKS selects
     int push_minblocks = 3;
+    // the same for the mixed push (3 or 4; QP_PUSH_MINBLOCKS_MIXED)
+    int push_minblocks_mixed = 3;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
     // diagnostics + J reset)
@@ -107,16 +126,31 @@ struct State {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double phase_ms[4] = {0, 0, 0, 0};
     int64_t phase_steps = 0;
+    // cells whose new range is too long for the per-thread ordering of the
+    // rebin: entry 0 counts them, entries 1.. list them
+    int32_t* long_list = nullptr;
+    int64_t long_cap = 0;
     // checkpoints (device-resident copies)
     struct Snap {
         bool valid = false;
         void* fields = nullptr;
-        std::vector<std::vector<void*>> arrays;  // per species, 10 arrays
+        std::vector<std::vector<void*>> arrays;  // per species, 10 arrays + perm
         std::vector<int64_t> n, cap, slots;
         std::vector<int32_t*> cell_start;
         int64_t step_index = 0;
     } snap[4];
 };
+
+// Device copy of the full state into a snapshot / back (qp_checkpoint,
+// qp_restore, the adjoint's checkpoints); snapshot_free releases one.
+int snapshot_take(State& s, State::Snap& sn);
+int snapshot_restore(State& s, State::Snap& sn);
+void snapshot_free(State::Snap& sn);
+State* state_of(qp_handle* h);
+
+// Adjoint of qp_step's FP64 FDTD/Boris path (qp_adjoint.cu).
+int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz, double* grad6, double* grad_q,
+                   double* loss_out);
 
 // ---- kernels / launchers (FP64, qp_fp64.cu) ----
 void launch_fields_fp64(State& s, int phase);          // phase: 0 half B, 1 E, 2 half B, 3 Bbar
@@ -137,6 +171,8 @@ void launch_field_energy_mixed(State& s);
 // order in sp.perm / sp.cell_next and swaps buffers.  Returns the new count.
 // counted: sp.count already holds the particles per new cell (tiled push).
 int64_t rebin(State& s, int species, int64_t born, bool counted);
+// Cells with more particles than this are ordered by a block each.
+constexpr int REBIN_LONG_SEG = 64;
 // Loading (qp_load.cu)
 void launch_load_cells(State& s, const double* const* a, int n, int32_t* cells, unsigned int* flags,
                        int* first_bad, int base);
@@ -145,7 +181,7 @@ void launch_histogram(State& s, const int32_t* cells, int n, int32_t* count);
 void launch_to_mixed(State& s, const double* const* a, int n, PStore32 dst, int at);
 void launch_f64_to_f32(State& s, const double* a, float* b, size_t n);
 void launch_f32_to_f64(State& s, const float* a, double* b, size_t n);
-void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n);
+void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n, int32_t* copy = nullptr);
 
 }  // namespace qp
 

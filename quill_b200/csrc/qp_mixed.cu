@@ -27,8 +27,8 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
 // One thread per particle in traversal order (see k_push64): the move runs in
 // the particle's cell frame (offsets in [0, 1)), the current through the
 // warp's segment-slot run reduction (deposit_runs).
-template <int PUSHER, int KIND>
-__global__ void __launch_bounds__(256, 3) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
+template <int PUSHER, int KIND, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs32 a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -41,7 +41,10 @@ __global__ void __launch_bounds__(256, 3) k_push32(Fields<float> f, Grid g, PSto
     if (s < a.n) {
         p = perm[s];
         const int c0 = src.cell[p];
-        i0 = c0 / g.nynz; j0 = (c0 / g.nz) % g.ny; k0 = c0 - (c0 / g.nz) * g.nz;
+        i0 = g.div_nynz.div(c0);
+        const int r0 = c0 - i0 * g.nynz;
+        j0 = g.div_nz.div(r0);
+        k0 = r0 - j0 * g.nz;
         o[0] = src.ox[p]; o[1] = src.oy[p]; o[2] = src.oz[p];
         ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
         q = src.q[p];
@@ -155,7 +158,11 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     const int nb = (int)((sp.n + 255) / 256);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LP(P, K) k_push32<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+#define QP_LP(P, K)                                                                                          \
+    if (s.push_minblocks_mixed == 4)                                                                          \
+        k_push32<P, K, 4><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
+    else                                                                                                      \
+        k_push32<P, K, 3><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
     if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
     else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);

@@ -16,83 +16,120 @@
 
 namespace qp {
 
-// For a destination cell c = (i, j, k) inside the grid, the particles that
-// can arrive come from the 3x3 neighbouring lines (i-di, j-dj); on each line
-// the source cells k+1, k, k-1 form one contiguous traversal range
-// [cs[(i-di, j-dj, k-1)], cs[(i-di, j-dj, k+2)]).
+// The rebin runs in two passes over the new cells computed by the push:
+//  1. scatter (thread per old traversal position t): a particle that stays
+//     in its cell c (t in c's old range [cs[c], cs[c+1])) takes, from the end
+//     of c's new range, the slot given by the number of c's stayers after it
+//     (a warp ballot plus, for ranges continuing past the warp, a short
+//     scan), so the stayers land in ascending order with no atomics; an
+//     arrival or a born particle (t >= n) claims the next slot from the front
+//     of the range (one atomic per run of equal cells in the warp);
+//  2. front order (thread per cell): the claimed front part is put in list
+//     order, born ascending then arrivals DESCENDING by old position; it is
+//     short (the arrivals of one step), long parts go to a block each.
 
-// Number of particles whose new cell is c (one thread per destination cell).
-__global__ void __launch_bounds__(256) k_rebin_count(Grid g, const int32_t* __restrict__ cs,
-                                                     const int32_t* __restrict__ newcell,
+__device__ __forceinline__ long long front_key(int x, int n_old) {
+    if (x >= n_old) return (long long)x;                       // born
+    return (1ll << 32) | (long long)(0x7fffffff - x);          // arrival
+}
+
+// Particles per new cell (entries < 0 skipped), one atomic per run.
+__global__ void __launch_bounds__(256) k_rebin_count(const int32_t* __restrict__ newcell, int total,
                                                      int32_t* __restrict__ count) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.nc) return;
-    const int k = c % g.nz, j = (c / g.nz) % g.ny, i = c / g.nynz;
-    int n = 0;
-    if (inside(g, i, j, k)) {
-        for (int di = -1; di <= 1; di++)
-            for (int dj = -1; dj <= 1; dj++) {
-                const int l = c - di * g.nynz - dj * g.nz;
-                const int e = __ldg(cs + l + 2);
-                for (int p = __ldg(cs + l - 1); p < e; p++) n += (__ldg(newcell + p) == c);
-            }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    warp_count_runs(count, t < total ? __ldg(newcell + t) : -1);
+}
+
+__global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict__ newcell, int total,
+                                                       const int32_t* __restrict__ cs,
+                                                       const int32_t* __restrict__ start,
+                                                       int32_t* __restrict__ cursor, int32_t* __restrict__ perm) {
+    const unsigned full = 0xffffffffu;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int wb = t - lane;  // first position of this warp
+    const int key = t < total ? __ldg(newcell + t) : -1;
+    int e = 0;
+    bool stay = false;
+    if (key >= 0) {
+        e = __ldg(cs + key + 1);
+        stay = t >= __ldg(cs + key) && t < e;
     }
-    count[c] = n;
+    // stayers: slot counted from the end of the new range
+    const unsigned smask = __ballot_sync(full, stay);
+    if (stay) {
+        const int hi = min(e - wb, 32);
+        const unsigned below_hi = hi >= 32 ? full : ((1u << hi) - 1u);
+        const unsigned above_me = lane == 31 ? 0u : ~((2u << lane) - 1u);
+        int after = __popc(smask & below_hi & above_me);
+        for (int u = wb + 32; u < e; u++) after += __ldg(newcell + u) == key;
+        perm[__ldg(start + key + 1) - 1 - after] = t;
+    }
+    // arrivals and born: claimed from the front, one atomic per run
+    const int akey = (key >= 0 && !stay) ? key : -1;
+    const int ukey = akey >= 0 ? akey : -1 - lane;
+    const int prev = __shfl_up_sync(full, ukey, 1);
+    const bool head = lane == 0 || prev != ukey;
+    const unsigned heads = __ballot_sync(full, head);
+    const unsigned upto = lane == 31 ? full : ((2u << lane) - 1u);
+    const int hl = 31 - __clz(heads & upto);          // first lane of this lane's run
+    const unsigned above = heads & ~upto;
+    const int next = above ? __ffs(above) - 1 : 32;   // first lane of the next run
+    int base = 0;
+    if (head && akey >= 0) base = atomicAdd(cursor + akey, next - lane);
+    base = __shfl_sync(full, base, hl);
+    if (akey >= 0) perm[base + lane - hl] = t;
 }
 
-// Fill perm for destination cell c from start[c] (after the particles born
-// in c, if any): arrivals from the source cells in descending linear index
-// ((i+1, j+1, k+1) first), each scanned from its last particle down, then
-// the stayers in ascending order.
-__global__ void __launch_bounds__(256) k_rebin_assign(Grid g, const int32_t* __restrict__ cs,
-                                                      const int32_t* __restrict__ newcell,
-                                                      const int32_t* __restrict__ start,
-                                                      const int32_t* __restrict__ born,
-                                                      int32_t* __restrict__ perm) {
+// Front part [start[c], cursor[c]) of each cell into list order, in place
+// (insertion sort: the part holds one step's arrivals).  Long parts are
+// queued for k_rebin_front_long.
+__global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* __restrict__ start,
+                                                     const int32_t* __restrict__ cursor, int n_old,
+                                                     int32_t* __restrict__ perm, int32_t* __restrict__ long_list,
+                                                     int* __restrict__ n_long) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.nc) return;
-    const int k = c % g.nz, j = (c / g.nz) % g.ny, i = c / g.nynz;
-    if (!inside(g, i, j, k)) return;
-    int pos = start[c] + (born ? born[c] : 0);
-    const int end = start[c + 1];
-    if (pos == end) return;
-    const int own_b = __ldg(cs + c), own_e = __ldg(cs + c + 1);
-    for (int di = -1; di <= 1; di++)
-        for (int dj = -1; dj <= 1; dj++) {
-            const int l = c - di * g.nynz - dj * g.nz;
-            const int b = __ldg(cs + l - 1);
-            for (int p = __ldg(cs + l + 2) - 1; p >= b; p--) {
-                if (di == 0 && dj == 0 && p >= own_b && p < own_e) continue;  // the cell's own particles
-                if (__ldg(newcell + p) == c) perm[pos++] = p;
-            }
+    if (c >= ncell) return;
+    const int b = __ldg(start + c), f = __ldg(cursor + c) - b;
+    if (f < 2) return;
+    if (f > REBIN_LONG_SEG) {
+        long_list[atomicAdd(n_long, 1)] = c;
+        return;
+    }
+    for (int u = b + 1; u < b + f; u++) {
+        const int x = perm[u];
+        const long long kx = front_key(x, n_old);
+        int v = u - 1;
+        while (v >= b && front_key(perm[v], n_old) > kx) {
+            perm[v + 1] = perm[v];
+            v--;
         }
-    for (int p = own_b; p < own_e; p++)
-        if (__ldg(newcell + p) == c) perm[pos++] = p;
+        perm[v + 1] = x;
+    }
 }
 
-// Particles born during this step's pushes (QED) sit at slots [n, n + A) of
-// the output buffer with their cell in newcell.  They go first in their cell
-// (they were head-inserted when born, plist.cpp:22-39); among themselves in
-// claim order.
-__global__ void k_born_hist(const int32_t* __restrict__ newcell, int n, int A, int32_t* __restrict__ born) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= A) return;
-    const int c = newcell[n + t];
-    if (c >= 0) atomicAdd(born + c, 1);
-}
-
-__global__ void k_add_i32_inplace(int32_t* __restrict__ a, const int32_t* __restrict__ b, int n) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x < n) a[x] += b[x];
-}
-
-__global__ void k_born_place(const int32_t* __restrict__ newcell, int n, int A, const int32_t* __restrict__ start,
-                             int32_t* __restrict__ fill, int32_t* __restrict__ perm) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= A) return;
-    const int c = newcell[n + t];
-    if (c < 0) return;
-    perm[start[c] + atomicAdd(fill + c, 1)] = n + t;
+// A long front part per block: copied to scratch, each entry ranked by
+// counting the entries with a smaller key, written back.
+__global__ void __launch_bounds__(256) k_rebin_front_long(const int32_t* __restrict__ start,
+                                                          const int32_t* __restrict__ cursor, int n_old,
+                                                          int32_t* __restrict__ perm, int32_t* __restrict__ scratch,
+                                                          const int32_t* __restrict__ long_list,
+                                                          const int* __restrict__ n_long) {
+    const int nl = *n_long;
+    for (int li = blockIdx.x; li < nl; li += gridDim.x) {
+        const int c = long_list[li];
+        const int b = start[c], e = cursor[c];
+        for (int u = b + (int)threadIdx.x; u < e; u += blockDim.x) scratch[u] = perm[u];
+        __syncthreads();
+        for (int u = b + (int)threadIdx.x; u < e; u += blockDim.x) {
+            const int x = scratch[u];
+            const long long kx = front_key(x, n_old);
+            int r = 0;
+            for (int v = b; v < e; v++) r += front_key(scratch[v], n_old) < kx;
+            perm[b + r] = x;
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------- scan ----
@@ -166,19 +203,25 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int32_t* tile_sums, 
     if (threadIdx.x == 0) tile_sums[nt] = carry;
 }
 
-__global__ void __launch_bounds__(256) k_scan_add(int32_t* out, int n, const int32_t* tile_sums, int nt) {
+__global__ void __launch_bounds__(256) k_scan_add(int32_t* out, int n, const int32_t* tile_sums, int nt,
+                                                  int32_t* copy) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x < n) out[x] += tile_sums[x / SCAN_TILE];
+    if (x < n) {
+        const int v = out[x] + tile_sums[x / SCAN_TILE];
+        out[x] = v;
+        if (copy) copy[x] = v;
+    }
     if (x == 0) out[n] = tile_sums[nt];
 }
 
-// out[0..n] = exclusive scan of in[0..n), out[n] = total.
-void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n) {
+// out[0..n] = exclusive scan of in[0..n), out[n] = total; copy[0..n) (if
+// given, may alias in) receives out[0..n) as well.
+void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n, int32_t* copy) {
     const int nt = (n + SCAN_TILE - 1) / SCAN_TILE;
     int32_t* sums = (int32_t*)s.scan_tmp;
     k_scan_tiles<<<nt, SCAN_THREADS, 0, s.stream>>>(in, out, n, sums);
     k_scan_sums<<<1, SCAN_THREADS, 0, s.stream>>>(sums, nt);
-    k_scan_add<<<(n + 255) / 256, 256, 0, s.stream>>>(out, n, sums, nt);
+    k_scan_add<<<(n + 255) / 256, 256, 0, s.stream>>>(out, n, sums, nt, copy);
     s.launches += 3;
 }
 
@@ -187,33 +230,35 @@ int64_t rebin(State& s, int si, int64_t born, bool counted) {
     const Grid g = s.grid;
     const int nb = (g.nc + 255) / 256;
     const int n = (int)sp.n, A = (int)born;
+    const int total = n + A;
     if (!counted) {
-        k_rebin_count<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.count);
+        cudaMemsetAsync(sp.count, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
+        if (total > 0) {
+            k_rebin_count<<<(total + 255) / 256, 256, 0, s.stream>>>(sp.newcell, total, sp.count);
+            s.launches++;
+        }
+    }
+    // cell_next = exclusive scan of the counts; count becomes the claim cursor
+    exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc, sp.count);
+    if (total > 0) {
+        k_rebin_scatter<<<(total + 255) / 256, 256, 0, s.stream>>>(sp.newcell, total, sp.cell_start, sp.cell_next,
+                                                                   sp.count, sp.perm);
         s.launches++;
     }
-    if (A > 0) {
-        cudaMemsetAsync(sp.born, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
-        cudaMemsetAsync(sp.born_fill, 0, (size_t)g.nc * sizeof(int32_t), s.stream);
-        k_born_hist<<<(A + 255) / 256, 256, 0, s.stream>>>(sp.newcell, n, A, sp.born);
-        k_add_i32_inplace<<<nb, 256, 0, s.stream>>>(sp.count, sp.born, g.nc);
-        s.launches += 2;
-    }
-    exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc);
-    k_rebin_assign<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, sp.newcell, sp.cell_next, A > 0 ? sp.born : nullptr,
-                                             sp.perm);
-    s.launches++;
-    if (A > 0) {
-        k_born_place<<<(A + 255) / 256, 256, 0, s.stream>>>(sp.newcell, n, A, sp.cell_next, sp.born_fill, sp.perm);
-        s.launches++;
-    }
+    int* n_long = (int*)s.long_list;  // entry 0: count; cells from entry 1
+    cudaMemsetAsync(n_long, 0, sizeof(int), s.stream);
+    k_rebin_front<<<nb, 256, 0, s.stream>>>(g.nc, sp.cell_next, sp.count, n, sp.perm, s.long_list + 1, n_long);
+    k_rebin_front_long<<<2 * 148, 256, 0, s.stream>>>(sp.cell_next, sp.count, n, sp.perm, sp.newcell,
+                                                      s.long_list + 1, n_long);
+    s.launches += 2;
     std::swap(sp.cell_start, sp.cell_next);
     sp.cur = 1 - sp.cur;
-    sp.slots = (int64_t)n + A;  // the push wrote traversal positions [0, n), births after them
-    int32_t total = 0;
-    cudaMemcpyAsync(&total, sp.cell_start + g.nc, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream);
+    sp.slots = (int64_t)total;  // the push wrote traversal positions [0, n), births after them
+    int32_t tot = 0;
+    cudaMemcpyAsync(&tot, sp.cell_start + g.nc, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream);
     cudaStreamSynchronize(s.stream);
-    sp.n = total;
-    return total;
+    sp.n = tot;
+    return tot;
 }
 
 // Merge freshly uploaded particles (slots [slot0, slot0 + n_new) of the
@@ -243,7 +288,7 @@ int load_merge(State& s, int si, int64_t slot0, const int32_t* d_new_start, int3
     const Grid g = s.grid;
     const int nb = (g.nc + 255) / 256;
     k_add_i32<<<nb, 256, 0, s.stream>>>(sp.cell_start, d_new_start, sp.count, g.nc);
-    exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc);
+    exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc, nullptr);
     k_load_merge<<<nb, 256, 0, s.stream>>>(g, sp.cell_start, d_new_start, sp.cell_next, sp.perm, d_perm_out,
                                            (int)slot0);
     s.launches += 2;
