@@ -197,6 +197,19 @@ def _load_torch(reg, si, ch):
     reg._check(r)
 
 
+def reduce_over_ranks(dist, ms, units, device):
+    """Replicas: the job's time is the slowest rank's, its units the sum over
+    ranks (every rank takes the same two collectives)."""
+    if dist is None:
+        return ms, units
+    import torch
+    x = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    y = torch.tensor([float(units)], device=device, dtype=torch.float64)
+    dist.all_reduce(y)
+    return float(x.item()), float(y.item())
+
+
 def total_energy(d):
     return d.energy_f + d.energy_e + d.energy_p + d.energy_ph + sum(d.ienergy[m] for m in range(d.n_ion))
 
@@ -296,6 +309,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=30)
+    ap.add_argument("--drift-steps", type=int, default=0,
+                    help="also run this many untimed steps per precision and report the relative drift of the "
+                         "total energy (field + particles) over them")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -361,16 +377,7 @@ def main():
         reg.close()
         del reg
         torch.cuda.empty_cache()
-        ms = t["ms"]
-        if dist:
-            x = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
-            dist.all_reduce(x, op=dist.ReduceOp.MAX)
-            ms = float(x.item())
-            y = torch.tensor([float(t["pushed"])], device=f"cuda:{dev}", dtype=torch.float64)
-            dist.all_reduce(y)
-            pushed_all = float(y.item())
-        else:
-            pushed_all = float(t["pushed"])
+        ms, pushed_all = reduce_over_ranks(dist, t["ms"], t["pushed"], f"cuda:{dev}")
         bp, bc = BYTES[prec]
         np_avg = t["pushed"] / t["steps"]
         push_ms = t["phase_ms"][0] / t["steps"]
@@ -397,6 +404,22 @@ def main():
             "fields_end": t["fields_end"],
             "particles": t["n_after"],
         }
+    # long untimed runs for the energy drift (opt-in)
+    if args.drift_steps > 0:
+        for prec in results:
+            reg = build_region(case, prec, dev)
+            w = []
+            left = args.drift_steps
+            while left > 0:
+                k = min(left, 50)
+                w += [total_energy(x) for x in reg.step(k)]
+                left -= k
+            reg.close()
+            del reg
+            torch.cuda.empty_cache()
+            results[prec]["long_run_energy_drift"] = {"steps": args.drift_steps,
+                                                      "relative_drift": (w[-1] - w[0]) / w[0],
+                                                      "max_relative_excursion": max(abs(x - w[0]) for x in w) / w[0]}
     # mixed vs FP64 field error after the same steps from the same state
     if "mixed" in results:
         a, b = results["mixed"]["fields_end"], results["fp64"]["fields_end"]
@@ -410,9 +433,8 @@ def main():
         e2e = e2e_run(case, "fp64", args.steps, dev, host)
         del host
         if dist:
-            x = torch.tensor([e2e["seconds"]], device=f"cuda:{dev}", dtype=torch.float64)
-            dist.all_reduce(x, op=dist.ReduceOp.MAX)
-            e2e["value"] = e2e["value"] * e2e["seconds"] / float(x.item()) * world
+            sec, units = reduce_over_ranks(dist, e2e["seconds"], e2e["value"] * e2e["seconds"], f"cuda:{dev}")
+            e2e["value"] = units / sec
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

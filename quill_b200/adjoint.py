@@ -230,3 +230,68 @@ class SlabLaserProblem:
             return r.step(self.setup.nsteps, self.setup.external_bz)[-1].energy_e
         finally:
             r.close()
+
+
+def _main(argv=None):
+    """Time one loss + gradient evaluation of the adjoint workload and check
+    selected parameters against central finite differences of the FP64
+    forward (h = 1e-6 relative).  Prints one JSON line."""
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--grid", type=int, nargs=3, default=None, help="nx ny nz (default 256 128 128)")
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--every", type=int, default=None)
+    ap.add_argument("--transverse-gap", type=int, default=0)
+    ap.add_argument("--check", type=int, default=4, help="Gauss-Hermite coefficients checked (plus the 3 slab parameters)")
+    a = ap.parse_args(argv)
+    case = SlabLaserCase(transverse_gap=a.transverse_gap)
+    if a.grid:
+        case.nx, case.ny, case.nz = a.grid
+        case.centre = 0.5 * case.nx
+    if a.steps:
+        case.nsteps = a.steps
+    if a.every:
+        case.every = a.every
+    p = SlabLaserProblem(case)
+    coef, slab = p.nominal()
+    coef.requires_grad_(True)
+    slab.requires_grad_(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss = p.loss(coef, slab)
+    loss.backward()
+    t_grad = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    l_fwd = p.loss_value(coef.detach(), slab.detach())
+    t_fwd = time.perf_counter() - t0
+    c0, s0 = coef.detach(), slab.detach()
+    errs = {}
+    for t, name in enumerate(("height", "centre", "width")):
+        h = 1e-6 * abs(s0[t].item())
+        sp_, sm_ = s0.clone(), s0.clone()
+        sp_[t] += h
+        sm_[t] -= h
+        fd = (p.loss_value(c0, sp_) - p.loss_value(c0, sm_)) / (2 * h)
+        errs[name] = {"adjoint": slab.grad[t].item(), "fd": fd}
+    h = 1e-6 * case.a0
+    for m in range(min(a.check, case.n_modes * case.n_modes)):
+        mm, nn = divmod(m, case.n_modes)
+        cp_, cm_ = c0.clone(), c0.clone()
+        cp_[mm, nn] += h
+        cm_[mm, nn] -= h
+        fd = (p.loss_value(cp_, s0) - p.loss_value(cm_, s0)) / (2 * h)
+        errs[f"Re c{mm}{nn}"] = {"adjoint": coef.grad[mm, nn].real.item(), "fd": fd}
+    gmax = max(abs(v["adjoint"]) for v in errs.values())
+    for v in errs.values():
+        v["rel_err"] = abs(v["adjoint"] - v["fd"]) / max(abs(v["fd"]), 1e-300)
+    print(json.dumps({"workload": f"slab + Gauss-Hermite laser, {case.nx}x{case.ny}x{case.nz} cells, "
+                                  f"{p.n_particles} electrons, {case.nsteps} steps, checkpoint every {case.every}",
+                      "loss": loss.item(), "loss_forward_only": l_fwd, "seconds_loss_and_gradient": t_grad,
+                      "seconds_forward": t_fwd, "max_abs_gradient": gmax, "checks": errs}))
+
+
+if __name__ == "__main__":
+    _main()

@@ -145,15 +145,14 @@ __device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const 
     sink.add(2, wi, wj, wk, c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third));
 }
 
-// The 12 contributions of one segment (same arithmetic and order as
-// seg_dep), returned instead of deposited; targets relative to the corner
-// cell c: jx at c+nz+1, c+1, c+nz, c; jy at c+I+1, c+1, c+I, c; jz at
-// c+I+nz, c+nz, c+I, c (I = ny*nz).
+// The 12 contributions of one segment from its start offsets in the cell
+// (xa, ya, za) = p - w, its displacement d and charge q, with seg_dep's
+// arithmetic and order; targets relative to the corner cell c: jx at
+// c+nz+1, c+1, c+nz, c; jy at c+I+1, c+1, c+I, c; jz at c+I+nz, c+nz, c+I,
+// c (I = ny*nz).
 template <typename T>
-__device__ __forceinline__ void seg_values(const T p[3], const T d[3], T q, const int w[3], T v[12]) {
-    const T xa = p[0] - T(w[0]), xb = T(1) - xa;
-    const T ya = p[1] - T(w[1]), yb = T(1) - ya;
-    const T za = p[2] - T(w[2]), zb = T(1) - za;
+__device__ __forceinline__ void seg_values_at(T xa, T ya, T za, const T d[3], T q, T v[12]) {
+    const T xb = T(1) - xa, yb = T(1) - ya, zb = T(1) - za;
     const T dx = d[0], dy = d[1], dz = d[2];
     const T third = T(3);
     v[0] = dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third);
@@ -168,6 +167,12 @@ __device__ __forceinline__ void seg_values(const T p[3], const T d[3], T q, cons
     v[9] = dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third);
     v[10] = dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third);
     v[11] = dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third);
+}
+
+// The same from the start point p and the cell's lower corner w.
+template <typename T>
+__device__ __forceinline__ void seg_values(const T p[3], const T d[3], T q, const int w[3], T v[12]) {
+    seg_values_at(p[0] - T(w[0]), p[1] - T(w[1]), p[2] - T(w[2]), d, q, v);
 }
 
 // Three ratios sorted descending with the reference's tie handling

@@ -43,7 +43,8 @@ __global__ void __launch_bounds__(256) k_rebin_count(const int32_t* __restrict__
 __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict__ newcell, int total,
                                                        const int32_t* __restrict__ cs,
                                                        const int32_t* __restrict__ start,
-                                                       int32_t* __restrict__ cursor, int32_t* __restrict__ perm) {
+                                                       int32_t* __restrict__ cursor, int32_t* __restrict__ perm,
+                                                       unsigned int* status) {
     const unsigned full = 0xffffffffu;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -63,7 +64,9 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
         const unsigned above_me = lane == 31 ? 0u : ~((2u << lane) - 1u);
         int after = __popc(smask & below_hi & above_me);
         for (int u = wb + 32; u < e; u++) after += __ldg(newcell + u) == key;
-        perm[__ldg(start + key + 1) - 1 - after] = t;
+        const int pos = __ldg(start + key + 1) - 1 - after;
+        if (pos >= 0 && pos < total) perm[pos] = t;
+        else atomicOr(status, (unsigned int)ST_BOUNDS);  // counts inconsistent with the cells
     }
     // arrivals and born: claimed from the front, one atomic per run
     const int akey = (key >= 0 && !stay) ? key : -1;
@@ -78,20 +81,28 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
     int base = 0;
     if (head && akey >= 0) base = atomicAdd(cursor + akey, next - lane);
     base = __shfl_sync(full, base, hl);
-    if (akey >= 0) perm[base + lane - hl] = t;
+    if (akey >= 0) {
+        const int pos = base + lane - hl;
+        if (pos >= 0 && pos < total) perm[pos] = t;
+        else atomicOr(status, (unsigned int)ST_BOUNDS);
+    }
 }
 
 // Front part [start[c], cursor[c]) of each cell into list order, in place
 // (insertion sort: the part holds one step's arrivals).  Long parts are
 // queued for k_rebin_front_long.
 __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* __restrict__ start,
-                                                     const int32_t* __restrict__ cursor, int n_old,
+                                                     const int32_t* __restrict__ cursor, int n_old, int total,
                                                      int32_t* __restrict__ perm, int32_t* __restrict__ long_list,
-                                                     int* __restrict__ n_long) {
+                                                     int* __restrict__ n_long, unsigned int* status) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     const int b = __ldg(start + c), f = __ldg(cursor + c) - b;
     if (f < 2) return;
+    if (b < 0 || b + f > total) {  // counts inconsistent with the cells
+        atomicOr(status, (unsigned int)ST_BOUNDS);
+        return;
+    }
     if (f > REBIN_LONG_SEG) {
         long_list[atomicAdd(n_long, 1)] = c;
         return;
@@ -242,12 +253,13 @@ int64_t rebin(State& s, int si, int64_t born, bool counted) {
     exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc, sp.count);
     if (total > 0) {
         k_rebin_scatter<<<(total + 255) / 256, 256, 0, s.stream>>>(sp.newcell, total, sp.cell_start, sp.cell_next,
-                                                                   sp.count, sp.perm);
+                                                                   sp.count, sp.perm, s.d_status);
         s.launches++;
     }
     int* n_long = (int*)s.long_list;  // entry 0: count; cells from entry 1
     cudaMemsetAsync(n_long, 0, sizeof(int), s.stream);
-    k_rebin_front<<<nb, 256, 0, s.stream>>>(g.nc, sp.cell_next, sp.count, n, sp.perm, s.long_list + 1, n_long);
+    k_rebin_front<<<nb, 256, 0, s.stream>>>(g.nc, sp.cell_next, sp.count, n, total, sp.perm, s.long_list + 1, n_long,
+                                            s.d_status);
     k_rebin_front_long<<<2 * 148, 256, 0, s.stream>>>(sp.cell_next, sp.count, n, sp.perm, sp.newcell,
                                                       s.long_list + 1, n_long);
     s.launches += 2;
