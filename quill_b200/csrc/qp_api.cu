@@ -677,9 +677,7 @@ static void fill_diag(State& s, qp_diag* d) {
     for (const auto& sp : s.sp) nion += sp.kind == KIND_ION;
     d->n_ion = nion;
     d->N_e = Ne * aN; d->N_p = Np * aN; d->N_ph = Nph * aN;
-    double field = a.field;
-    for (int b = 0; b < FIELD_PARTS; b++) field += a.field_part[b];
-    d->energy_f = field * aE;
+    d->energy_f = a.field * aE;
     d->energy_e = ee * bE; d->energy_p = ep * bE; d->energy_ph = eph * bE;
 }
 
@@ -718,13 +716,14 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
             if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i], counted);
         QP_CUDA_CHECK(s, cudaGetLastError());
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[3], s.stream));
+        // compute_energy field term on E, B before fadvance (main.cpp:2327)
+        if (s.fp64) launch_field_energy_fp64(s);
+        else launch_field_energy_mixed(s);
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[4], s.stream));
-        // fadvance: half B, E, half B, Bbar (maxwell.cpp:10-22, advance.cpp:13-18);
-        // the first half-B kernel also sums compute_energy's field term on E,
-        // B before they change (main.cpp:2327)
+        // fadvance: half B, E, half B, Bbar (maxwell.cpp:10-22, advance.cpp:13-18)
         for (int ph = 0; ph < 4; ph++) {
-            if (s.fp64) launch_fields_fp64(s, ph == 2 ? 0 : ph, ph == 0);
-            else launch_fields_mixed(s, ph == 2 ? 0 : ph, ph == 0);
+            if (s.fp64) launch_fields_fp64(s, ph == 2 ? 0 : ph);
+            else launch_fields_mixed(s, ph == 2 ? 0 : ph);
         }
         QP_CUDA_CHECK(s, cudaGetLastError());
         QP_CUDA_CHECK(s, cudaMemcpyAsync(s.h_diag, s.d_diag, sizeof(DiagAccum), cudaMemcpyDeviceToHost, s.stream));

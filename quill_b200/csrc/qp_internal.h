@@ -86,17 +86,12 @@ struct Species {
     int* d_counter = nullptr;      // device append counter (QED)
 };
 
-// Spread of the field-energy accumulation over this many addresses (fewer
-// same-address atomics); the host adds them up.
-constexpr int FIELD_PARTS = 32;
-
 struct DiagAccum {
     // per species: live count, sum q, sum of (g-1)q (or g q for photons)
     double sum_q[QP_MAX_SPECIES];
     double sum_e[QP_MAX_SPECIES];
     unsigned long long cnt[QP_MAX_SPECIES];
     double field;  // sum over cells of E^2 + B^2
-    double field_part[FIELD_PARTS];  // the same, spread over addresses by the fused field kernel
 };
 
 struct State {
@@ -158,17 +153,18 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
                    double* loss_out);
 
 // ---- kernels / launchers (FP64, qp_fp64.cu) ----
-// phase: 0 half B (with energy: also the field-energy sum), 1 E, 3 Bbar
-void launch_fields_fp64(State& s, int phase, bool energy = false);
+void launch_fields_fp64(State& s, int phase);          // phase: 0 half B, 1 E, 2 half B, 3 Bbar
 void launch_init_boundaries_fp64(State& s);
 void launch_push_fp64(State& s, int species, double external_bz);
 int launch_push_fp64_qed(State& s, int species, double external_bz);
 int launch_vacuum_fp64(State& s);
+void launch_field_energy_fp64(State& s);
 
 // ---- mixed precision (qp_mixed.cu) ----
-void launch_fields_mixed(State& s, int phase, bool energy = false);
+void launch_fields_mixed(State& s, int phase);
 void launch_init_boundaries_mixed(State& s);
 void launch_push_mixed(State& s, int species, double external_bz);
+void launch_field_energy_mixed(State& s);
 
 // ---- rebin and scans (qp_rebin.cu) ----
 // Rebin after a push: count -> scan -> assign; leaves the new traversal

@@ -6,55 +6,23 @@
 
 namespace qp {
 
-// One thread per (k, j) line segment of `ipb` cells along i; (k, j, i-block)
-// = (x, y, z) launch axes.  With ENERGY (first half-B update only) the
-// thread also sums E^2 + B^2 of its cells before updating them
-// (compute_energy's field term, fout.cpp:101-102, taken before fadvance as
-// main.cpp:2327-2331 orders it), FP64 accumulation, one atomic per block.
-template <typename T, int SOLVER, int PHASE, bool ENERGY>
-__global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c, int ipb, DiagAccum* acc) {
+// One thread per cell, (k, j, i) = (x, y, z) launch axes.
+template <typename T, int SOLVER, int PHASE>
+__global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int ib = blockIdx.z * ipb, ie = min(g.nx, ib + ipb);
-    double en = 0.0;
-    if (k < g.nz && j < g.ny) {
-        for (int i = ib; i < ie; i++) {
-            if (ENERGY) {
-                const int x = cidx(g, i, j, k);
-                const double ex = f.ex[x], ey = f.ey[x], ez = f.ez[x], bx = f.bx[x], by = f.by[x], bz = f.bz[x];
-                en += ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
-            }
-            if (PHASE == 0) {
-                if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
-                else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
-                else fp_b(f, g, c, i, j, k);
-            } else if (PHASE == 1) {
-                if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
-                else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
-                else fp_e(f, g, c, i, j, k);
-            } else {
-                bbar(f, g, i, j, k);
-            }
-        }
-    }
-    if (ENERGY) {
-        __shared__ double sh[32];
-        const int t = threadIdx.y * blockDim.x + threadIdx.x;
-        const int lane = t & 31, wid = t >> 5;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) en += __shfl_down_sync(0xffffffffu, en, o);
-        if (lane == 0) sh[wid] = en;
-        __syncthreads();
-        if (wid == 0) {
-            const int nw = (blockDim.x * blockDim.y) >> 5;
-            en = lane < nw ? sh[lane] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) en += __shfl_down_sync(0xffffffffu, en, o);
-            if (lane == 0) {
-                const int b = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-                atomicAdd(&acc->field_part[b % FIELD_PARTS], en);
-            }
-        }
+    const int i = blockIdx.z;
+    if (k >= g.nz || j >= g.ny) return;
+    if (PHASE == 0) {
+        if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
+        else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
+        else fp_b(f, g, c, i, j, k);
+    } else if (PHASE == 1) {
+        if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
+        else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
+        else fp_e(f, g, c, i, j, k);
+    } else {
+        bbar(f, g, i, j, k);
     }
 }
 
@@ -114,6 +82,26 @@ __device__ __forceinline__ void block_diag(DiagAccum* acc, int sp, double dq, do
     }
 }
 
+// Sum of E^2 + B^2 over all cells (compute_energy's field term,
+// fout.cpp:101-102), FP64 accumulation.
+template <typename T>
+__global__ void __launch_bounds__(256) k_field_energy(Fields<T> f, int nc, DiagAccum* acc) {
+    double s = 0.0;
+    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nc; x += gridDim.x * blockDim.x) {
+        const double ex = f.ex[x], ey = f.ey[x], ez = f.ez[x], bx = f.bx[x], by = f.by[x], bz = f.bz[x];
+        s += ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
+    }
+    __shared__ double sh[32];
+    s = warp_sum(s);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = s;
+    __syncthreads();
+    if (wid == 0) {
+        s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        s = warp_sum(s);
+        if (lane == 0) atomicAdd(&acc->field, s);
+    }
+}
 
 // Erased by p_boundary (plist.cpp:73-102): layers {0, n-2, n-1} of each axis.
 __device__ __forceinline__ bool kill_layer(const Grid& g, int i, int j, int k) {
@@ -155,42 +143,33 @@ __device__ __forceinline__ bool warp_run_sum(int key, T v[NV]) {
 
 // The 12 J contributions of single-segment moves, summed per run of equal
 // corner cell in the warp and added to J by the run's first lane.
-// The 12 contributions of one segment with corner cell c added to J.
-template <typename T>
-__device__ __forceinline__ void add_segment(const Fields<T>& f, const Grid& g, int c, const T v[12]) {
-    const int I = g.nynz, J = g.nz;
-    atomicAdd(f.jx + c + J + 1, v[0]);
-    atomicAdd(f.jx + c + 1, v[1]);
-    atomicAdd(f.jx + c + J, v[2]);
-    atomicAdd(f.jx + c, v[3]);
-    atomicAdd(f.jy + c + I + 1, v[4]);
-    atomicAdd(f.jy + c + 1, v[5]);
-    atomicAdd(f.jy + c + I, v[6]);
-    atomicAdd(f.jy + c, v[7]);
-    atomicAdd(f.jz + c + I + J, v[8]);
-    atomicAdd(f.jz + c + J, v[9]);
-    atomicAdd(f.jz + c + I, v[10]);
-    atomicAdd(f.jz + c, v[11]);
-}
-
 template <typename T>
 __device__ __forceinline__ void warp_deposit_runs(const Fields<T>& f, const Grid& g, int corner, T v[12]) {
-    if (warp_run_sum<T, 12>(corner, v)) add_segment(f, g, corner, v);
+    if (warp_run_sum<T, 12>(corner, v)) {
+        const int c = corner, I = g.nynz, J = g.nz;
+        atomicAdd(f.jx + c + J + 1, v[0]);
+        atomicAdd(f.jx + c + 1, v[1]);
+        atomicAdd(f.jx + c + J, v[2]);
+        atomicAdd(f.jx + c, v[3]);
+        atomicAdd(f.jy + c + I + 1, v[4]);
+        atomicAdd(f.jy + c + 1, v[5]);
+        atomicAdd(f.jy + c + I, v[6]);
+        atomicAdd(f.jy + c, v[7]);
+        atomicAdd(f.jz + c + I + J, v[8]);
+        atomicAdd(f.jz + c + J, v[9]);
+        atomicAdd(f.jz + c + I, v[10]);
+        atomicAdd(f.jz + c, v[11]);
+    }
 }
 
 // Current deposition of the whole warp's moves (deposition.cpp:41-356).
 // Every move's first segment starts in the particle's own cell, so the first
 // segments of a cell's particles share their 12 targets: they are summed over
-// runs of equal cells in the warp and added to J once per run.  The further
-// 1-3 segments of face-crossing moves are then described by their lanes
-// (start offsets in the cell, displacement, charge, corner cell), packed over
-// the warp in shared memory, and deposited one per lane: one round per 32
-// segments instead of one per crossing of the warp's most-crossing lane.  The
-// segment arithmetic per crossing case is the reference's (see
-// jdeposition_to); p is advanced segment by segment.  Every lane of the warp
-// must call this, in blocks of DEPOSIT_WARPS warps; lanes with active ==
-// false take no part.
-constexpr int DEPOSIT_WARPS = 8;
+// runs of equal cells in the warp and added to J once per run.  Moves that
+// cross faces then deposit their further segments directly.  The segment
+// arithmetic per crossing case is the reference's (see jdeposition_to); p is
+// advanced segment by segment.  Every lane of the warp must call this; lanes
+// with active == false take no part.
 template <typename T>
 __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, T p[3], const T d[3], T q, int bi,
                                              int bj, int bk, bool active, unsigned int* status) {
@@ -259,20 +238,8 @@ __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, 
         for (int k = 0; k < 12; k++) v[k] = T(0);
     }
     warp_deposit_runs(f, g, corner, v);
-    const unsigned full = 0xffffffffu;
-    if (!__any_sync(full, nx_ > 0)) return;
-    __shared__ T sd[DEPOSIT_WARPS][7][96];  // xa ya za, s, q per segment
-    __shared__ int scorner[DEPOSIT_WARPS][96];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int incl = nx_;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(full, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const int total = __shfl_sync(full, incl, 31);
     if (nx_ > 0) {
-        int slot = incl - nx_;
+        GlobalSink<T> sink{f};
         int w[3] = {c1x, c1y, c1z};
         for (int sg = 1; sg <= nx_; sg++) {
             T s[3];
@@ -295,38 +262,10 @@ __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, 
                 w[1] = ifloor(p[1] + T(0.5) * s[1]);
                 w[2] = ifloor(p[2] + T(0.5) * s[2]);
             }
-            const int wi = bi + w[0], wj = bj + w[1], wk = bk + w[2];
-            int cc = -1;
-            if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= g.nx || wj + 1 >= g.ny || wk + 1 >= g.nz)
-                atomicOr(status, (unsigned int)ST_BOUNDS);
-            else
-                cc = cidx(g, wi, wj, wk);
-            sd[wid][0][slot] = p[0] - T(w[0]);
-            sd[wid][1][slot] = p[1] - T(w[1]);
-            sd[wid][2][slot] = p[2] - T(w[2]);
-            sd[wid][3][slot] = s[0];
-            sd[wid][4][slot] = s[1];
-            sd[wid][5][slot] = s[2];
-            sd[wid][6][slot] = q;
-            scorner[wid][slot] = cc;
-            slot++;
+            seg_dep(sink, g, p, s, q, w, bi, bj, bk, status);
             p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
         }
     }
-    __syncwarp();
-    for (int b = 0; b < total; b += 32) {
-        const int it = b + lane;
-        if (it < total) {
-            const int cc = scorner[wid][it];
-            if (cc >= 0) {
-                const T ds[3] = {sd[wid][3][it], sd[wid][4][it], sd[wid][5][it]};
-                T vv[12];
-                seg_values_at(sd[wid][0][it], sd[wid][1][it], sd[wid][2][it], ds, sd[wid][6][it], vv);
-                add_segment(f, g, cc, vv);
-            }
-        }
-    }
-    __syncwarp();
 }
 
 // Particles per new cell for the rebin, one atomic per run of equal cells.

@@ -102,28 +102,23 @@ static Fields<float> fields32(State& s) {
 
 SolverCoef solver_coef(const qp_params& p);
 
-void launch_fields_mixed(State& s, int phase, bool energy) {
+void launch_fields_mixed(State& s, int phase) {
     Fields<float> f = fields32(s);
     Coef<float> c(solver_coef(s.prm));
-    const int ipb = 1;  // cells along i per thread
     dim3 blk(32, 8, 1);
-    dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, (s.grid.nx + ipb - 1) / ipb);
+    dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, s.grid.nx);
     const int sol = s.prm.solver;
-#define QP_LF(SOL, PH, EN) k_field<float, SOL, PH, EN><<<grd, blk, 0, s.stream>>>(f, s.grid, c, ipb, s.d_diag)
-    if (phase == 0 && energy) {
-        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 0, true);
-        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 0, true);
-        else QP_LF(QP_SOLVER_FIVE_POINT, 0, true);
-    } else if (phase == 0 || phase == 2) {
-        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 0, false);
-        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 0, false);
-        else QP_LF(QP_SOLVER_FIVE_POINT, 0, false);
+#define QP_LF(SOL, PH) k_field<float, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c)
+    if (phase == 0 || phase == 2) {
+        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 0);
+        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 0);
+        else QP_LF(QP_SOLVER_FIVE_POINT, 0);
     } else if (phase == 1) {
-        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 1, false);
-        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 1, false);
-        else QP_LF(QP_SOLVER_FIVE_POINT, 1, false);
+        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 1);
+        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 1);
+        else QP_LF(QP_SOLVER_FIVE_POINT, 1);
     } else {
-        QP_LF(QP_SOLVER_FDTD, 3, false);
+        QP_LF(QP_SOLVER_FDTD, 3);
     }
 #undef QP_LF
     s.launches++;
@@ -175,5 +170,10 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     s.launches++;
 }
 
+void launch_field_energy_mixed(State& s) {
+    Fields<float> f = fields32(s);
+    k_field_energy<float><<<148 * 4, 256, 0, s.stream>>>(f, s.grid.nc, s.d_diag);
+    s.launches++;
+}
 
 }  // namespace qp
