@@ -76,6 +76,10 @@ typedef struct {
     int64_t n_macro[QP_MAX_SPECIES];     /* live particles per species (table order) */
     int32_t status;                      /* qp_status raised on the device in this step */
     int32_t pad_;
+    double energy_erased;                /* Joules carried off by the particles erased in this step
+                                            (p_boundary and place), with the normalisation and
+                                            species signs of the energy terms; 0 unless enabled by
+                                            qp_set_erased_tracking.  No reference counterpart. */
 } qp_diag;
 
 typedef struct qp_handle qp_handle;
@@ -179,6 +183,14 @@ int qp_set_timing(qp_handle* h, int enable);
  * current deposition, [1] rebin, [2] Maxwell solver + Bbar, [3] J reset and
  * diagnostics; *steps = timed steps (nullable). */
 int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
+
+/* Sum the energy of the particles each step erases (p_boundary before the
+ * push, place() after it) into qp_diag.energy_erased, so that
+ * energy_f + energy_e + energy_p + energy_ph + ienergy plus the erased energy
+ * accumulated over the steps is the closed energy balance of the region.
+ * QED-off steps only.  No reference counterpart (the reference drops erased
+ * particles' energy unless it catches them, main.cpp:1516-1689). */
+int qp_set_erased_tracking(qp_handle* h, int enable);
 
 /* Discrete adjoint (no reference counterpart): runs nsteps steps from the
  * handle's current state and returns the loss L = energy_e after the last

@@ -57,6 +57,7 @@ class Diag(C.Structure):
         ("ienergy", C.c_double * QP_MAX_SPECIES),
         ("n_macro", C.c_int64 * QP_MAX_SPECIES),
         ("status", C.c_int32), ("pad_", C.c_int32),
+        ("energy_erased", C.c_double),
     ]
 
     def as_array(self) -> np.ndarray:
@@ -105,6 +106,7 @@ def load_library(path: str | None = None):
         "qp_eval_qed_rates": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_eval_qed_rates_noalloc": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
+        "qp_set_erased_tracking": (C.c_int, [VP, C.c_int]),
         "qp_adjoint_energy": (C.c_int, [VP, C.c_int, C.c_int, D, DP, DP, DP]),
     }
     for name, (res, args) in sig.items():
@@ -245,6 +247,11 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_erased_tracking(self, enable: bool = True):
+        """Report in Diag.energy_erased the energy of the particles each step
+        erases (QED-off steps)."""
+        self._check(self.lib.qp_set_erased_tracking(self.h, int(bool(enable))))
 
     def set_timing(self, enable: bool = True):
         self._check(self.lib.qp_set_timing(self.h, int(bool(enable))))

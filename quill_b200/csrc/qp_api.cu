@@ -403,6 +403,12 @@ int qp_eval_qed_rates(int device, double lambda_cm, int64_t n, const double* in,
     return QP_OK;
 }
 
+int qp_set_erased_tracking(qp_handle* h, int enable) {
+    QP_H_CHECK(h);
+    h->st.track_erased = enable != 0;
+    return QP_OK;
+}
+
 int qp_set_timing(qp_handle* h, int enable) {
     QP_H_CHECK(h);
     State& s = h->st;
@@ -660,10 +666,14 @@ static void fill_diag(State& s, qp_diag* d) {
     const double bE = 8.2e-14 * dV * 1.11485e13 * p.lambda_cm / (8 * PI * PI * PI);
     memset(d, 0, sizeof(*d));
     const DiagAccum& a = *s.h_diag;
-    double Ne = 0, Np = 0, Nph = 0, ee = 0, ep = 0, eph = 0;
+    double Ne = 0, Np = 0, Nph = 0, ee = 0, ep = 0, eph = 0, er = 0;
     for (size_t i = 0; i < s.sp.size(); i++) {
         const Species& sp = s.sp[i];
         d->n_macro[i] = (int64_t)a.cnt[i];
+        // erased energy with each species' sign and scale (as energy_e/p/ph, ienergy)
+        if (sp.cmr == -1) er -= a.sum_erased[i];
+        else if (sp.cmr == 1 || sp.cmr == 0) er += a.sum_erased[i];
+        else if (sp.ion_index >= 0) er += a.sum_erased[i] / sp.cmr;
         // compute_N / compute_energy species tests (fout.cpp:62-77, 105-126)
         if (sp.cmr == -1) { Ne -= a.sum_q[i]; ee -= a.sum_e[i]; d->N_qp_e += a.cnt[i]; }
         else if (sp.cmr == 1) { Np += a.sum_q[i]; ep += a.sum_e[i]; d->N_qp_p += a.cnt[i]; }
@@ -679,6 +689,7 @@ static void fill_diag(State& s, qp_diag* d) {
     d->N_e = Ne * aN; d->N_p = Np * aN; d->N_ph = Nph * aN;
     d->energy_f = a.field * aE;
     d->energy_e = ee * bE; d->energy_p = ep * bE; d->energy_ph = eph * bE;
+    d->energy_erased = er * bE;
 }
 
 int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {

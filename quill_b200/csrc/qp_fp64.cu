@@ -69,6 +69,10 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
     }
     warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
+    if (a.track) {  // uniform: energy of the particles erased in this push
+        const double er = (s < a.n && nc < 0) ? (KIND == KIND_PHOTON ? gm * q : (gm - 1) * q) : 0.0;
+        block_sum(&a.diag->sum_erased[a.sp], er);
+    }
 }
 
 // Particle born during a push: appended to the target species' output
@@ -388,6 +392,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
+    a.track = 0;
     QedArgs qa = qed_args(s);
     AppendTarget<PStore64> t0, t1;
     if (sp.kind == KIND_PHOTON) {
@@ -441,6 +446,7 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
+    a.track = s.track_erased ? 1 : 0;
     const int nb = (int)((sp.n + 255) / 256);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;

@@ -92,6 +92,7 @@ struct DiagAccum {
     double sum_e[QP_MAX_SPECIES];
     unsigned long long cnt[QP_MAX_SPECIES];
     double field;  // sum over cells of E^2 + B^2
+    double sum_erased[QP_MAX_SPECIES];  // sum of (g-1)q (g q for photons) of erased particles
 };
 
 struct State {
@@ -123,6 +124,7 @@ struct State {
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
     // diagnostics + J reset)
     bool timing = false;
+    bool track_erased = false;  // qp_set_erased_tracking
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double phase_ms[4] = {0, 0, 0, 0};
     int64_t phase_steps = 0;

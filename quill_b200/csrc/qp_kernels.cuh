@@ -82,6 +82,20 @@ __device__ __forceinline__ void block_diag(DiagAccum* acc, int sp, double dq, do
     }
 }
 
+// Block-wide sum of one value, one atomic per block.
+__device__ __forceinline__ void block_sum(double* acc, double v) {
+    __shared__ double s_v[32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s_v[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < (int)((blockDim.x + 31) >> 5) ? s_v[lane] : 0.0;
+        v = warp_sum(v);
+        if (lane == 0 && v != 0.0) atomicAdd(acc, v);
+    }
+}
+
 // Sum of E^2 + B^2 over all cells (compute_energy's field term,
 // fout.cpp:101-102), FP64 accumulation.
 template <typename T>
@@ -277,6 +291,7 @@ __device__ __forceinline__ void warp_count_runs(int32_t* count, int cell) {
 struct PushArgs {
     double cmr, dt, dx, dy, dz, ext_bz;
     int n, sp, kind;
+    int track;  // sum the energy of erased particles into diag->sum_erased
     unsigned int* status;
     DiagAccum* diag;
 };

@@ -10,6 +10,7 @@ namespace qp {
 struct PushArgs32 {
     float cmr, dt, idx, idy, idz, ext_bz;
     int n, sp, kind;
+    int track;  // sum the energy of erased particles into diag->sum_erased
     unsigned int* status;
     DiagAccum* diag;
 };
@@ -89,6 +90,12 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
     }
     warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
+    if (a.track) {  // uniform: energy of the particles erased in this push
+        const double er = (s < a.n && nc < 0)
+                              ? (KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q)
+                              : 0.0;
+        block_sum(&a.diag->sum_erased[a.sp], er);
+    }
 }
 
 static Fields<float> fields32(State& s) {
@@ -155,6 +162,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.idx = (float)(1.0 / s.prm.dx); a.idy = (float)(1.0 / s.prm.dy); a.idz = (float)(1.0 / s.prm.dz);
     a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
+    a.track = s.track_erased ? 1 : 0;
     const int nb = (int)((sp.n + 255) / 256);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;

@@ -50,11 +50,15 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
     const int lane = threadIdx.x & 31;
     const int wb = t - lane;  // first position of this warp
     const int key = t < total ? __ldg(newcell + t) : -1;
-    int e = 0;
+    int e = 0, end = 0;
     bool stay = false;
     if (key >= 0) {
+        // independent loads, issued together: the old range of the new cell
+        // and the end of its new range (used if the particle stayed)
+        const int b = __ldg(cs + key);
         e = __ldg(cs + key + 1);
-        stay = t >= __ldg(cs + key) && t < e;
+        end = __ldg(start + key + 1);
+        stay = t >= b && t < e;
     }
     // stayers: slot counted from the end of the new range
     const unsigned smask = __ballot_sync(full, stay);
@@ -64,7 +68,7 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
         const unsigned above_me = lane == 31 ? 0u : ~((2u << lane) - 1u);
         int after = __popc(smask & below_hi & above_me);
         for (int u = wb + 32; u < e; u++) after += __ldg(newcell + u) == key;
-        const int pos = __ldg(start + key + 1) - 1 - after;
+        const int pos = end - 1 - after;
         if (pos >= 0 && pos < total) perm[pos] = t;
         else atomicOr(status, (unsigned int)ST_BOUNDS);  // counts inconsistent with the cells
     }
@@ -88,9 +92,10 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
     }
 }
 
-// Front part [start[c], cursor[c]) of each cell into list order, in place
-// (insertion sort: the part holds one step's arrivals).  Long parts are
-// queued for k_rebin_front_long.
+// Front part [start[c], cursor[c]) of each cell into list order, in place.
+// The part holds one step's arrivals: up to 8 entries are sorted in
+// registers, up to REBIN_LONG_SEG by insertion sort in place, longer parts
+// are queued for k_rebin_front_long.
 __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* __restrict__ start,
                                                      const int32_t* __restrict__ cursor, int n_old, int total,
                                                      int32_t* __restrict__ perm, int32_t* __restrict__ long_list,
@@ -105,6 +110,38 @@ __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* _
     }
     if (f > REBIN_LONG_SEG) {
         long_list[atomicAdd(n_long, 1)] = c;
+        return;
+    }
+    if (f == 2) {
+        const int x0 = perm[b], x1 = perm[b + 1];
+        if (front_key(x0, n_old) > front_key(x1, n_old)) {
+            perm[b] = x1;
+            perm[b + 1] = x0;
+        }
+        return;
+    }
+    if (f <= 8) {
+        // in registers: all loads issued together, odd-even transposition sort
+        int x[8];
+        long long k[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            x[u] = u < f ? perm[b + u] : 0;
+            k[u] = u < f ? front_key(x[u], n_old) : 0x7fffffffffffffffll;
+        }
+#pragma unroll
+        for (int r = 0; r < 8; r++) {
+#pragma unroll
+            for (int u = r & 1; u + 1 < 8; u += 2) {
+                if (k[u] > k[u + 1]) {
+                    const long long tk = k[u]; k[u] = k[u + 1]; k[u + 1] = tk;
+                    const int tx = x[u]; x[u] = x[u + 1]; x[u + 1] = tx;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (u < f) perm[b + u] = x[u];
         return;
     }
     for (int u = b + 1; u < b + f; u++) {

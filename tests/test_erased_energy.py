@@ -1,0 +1,103 @@
+"""Energy carried off by erased particles (qp_set_erased_tracking): with it,
+the region's energy balance closes.
+
+* Photons move ballistically with constant energy g q, so the photon energy
+  left in the region plus the energy of the photons erased so far equals the
+  initial photon energy to round-off, whichever boundary they cross.
+* Electrons loaded in the p_boundary layers are erased before their first
+  push with their loaded energy: the erased energy of that step is
+  -b sum (g - 1) q, with compute_energy's normalisation b (main.cpp:2327).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from tests.conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+N = (20, 18, 16)
+DX = 2 * math.pi / 16
+DT = 0.5 * DX
+
+
+def _b(lambda_cm=1e-4):
+    return 8.2e-14 * DX ** 3 * 1.11485e13 * lambda_cm / (8 * math.pi ** 3)
+
+
+def _sorted(parts):
+    cells = (parts["x"].astype(int) * N[1] + parts["y"].astype(int)) * N[2] + parts["z"].astype(int)
+    o = np.argsort(cells, kind="stable")
+    return {k: v[o] for k, v in parts.items()}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_photon_energy_balance_closes(precision):
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    from quill_b200.api import Region
+    rng = np.random.default_rng(3)
+    m = 4000
+    u = rng.standard_normal((3, m)) * 5.0
+    g = np.sqrt((u * u).sum(0))
+    parts = _sorted({"x": rng.uniform(1, N[0] - 3, m), "y": rng.uniform(1, N[1] - 3, m),
+                     "z": rng.uniform(1, N[2] - 3, m), "ux": u[0], "uy": u[1], "uz": u[2], "g": g,
+                     "q": rng.uniform(0.01, 0.1, m)})
+    r = Region(*N, DX, DX, DX, DT, species_cmr=(0.0,), precision=precision)
+    r.set_fields(*np.zeros((6,) + N))
+    r.init_boundaries()
+    r.add_particles(0, parts)
+    r.set_erased_tracking(True)
+    w0 = _b() * float(np.sum(parts["g"] * parts["q"]))
+    d = r.step(24)
+    lost = np.cumsum([x.energy_erased for x in d])
+    left = np.array([x.energy_ph for x in d])
+    r.close()
+    assert d[-1].n_macro[0] < m // 2          # most photons left the region
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    np.testing.assert_allclose(left + lost, w0, rtol=tol)
+
+
+def test_electrons_in_boundary_layers_erased_with_their_energy():
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    from quill_b200.api import Region
+    rng = np.random.default_rng(4)
+    m = 300
+    # positions in the layers p_boundary erases: 0, n-2, n-1 on one axis each
+    x = rng.uniform(2, N[0] - 3, m)
+    y = rng.uniform(2, N[1] - 3, m)
+    z = rng.uniform(2, N[2] - 3, m)
+    which = rng.integers(0, 3, m)
+    x[which == 0] = rng.choice([0.5, N[0] - 1.5, N[0] - 0.5], (which == 0).sum())
+    y[which == 1] = rng.choice([0.5, N[1] - 1.5, N[1] - 0.5], (which == 1).sum())
+    z[which == 2] = rng.choice([0.5, N[2] - 1.5, N[2] - 0.5], (which == 2).sum())
+    u = rng.standard_normal((3, m))
+    g = np.sqrt(1 + (u * u).sum(0))
+    q = -rng.uniform(0.01, 0.1, m)
+    parts = _sorted({"x": x, "y": y, "z": z, "ux": u[0], "uy": u[1], "uz": u[2], "g": g, "q": q})
+    r = Region(*N, DX, DX, DX, DT)
+    r.set_fields(*np.zeros((6,) + N))
+    r.init_boundaries()
+    r.add_particles(0, parts)
+    r.set_erased_tracking(True)
+    d = r.step(1)[0]
+    r.close()
+    assert d.n_macro[0] == 0
+    want = -_b() * float(np.sum((parts["g"] - 1) * parts["q"]))
+    assert abs(d.energy_erased - want) <= 1e-12 * abs(want)
+
+
+def test_tracking_off_reports_zero():
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    from quill_b200.api import Region
+    r = Region(*N, DX, DX, DX, DT)
+    r.set_fields(*np.zeros((6,) + N))
+    r.init_boundaries()
+    r.add_particles(0, {"x": np.array([0.5]), "y": np.array([5.5]), "z": np.array([5.5]), "ux": np.zeros(1),
+                        "uy": np.zeros(1), "uz": np.zeros(1), "g": np.ones(1) * 2, "q": -np.ones(1)})
+    d = r.step(1)[0]
+    r.close()
+    assert d.energy_erased == 0.0 and d.n_macro[0] == 0
