@@ -246,6 +246,7 @@ def _main(argv=None):
     ap.add_argument("--every", type=int, default=None)
     ap.add_argument("--transverse-gap", type=int, default=0)
     ap.add_argument("--check", type=int, default=4, help="Gauss-Hermite coefficients checked (plus the 3 slab parameters)")
+    ap.add_argument("--a0", type=float, default=None)
     a = ap.parse_args(argv)
     case = SlabLaserCase(transverse_gap=a.transverse_gap)
     if a.grid:
@@ -255,6 +256,8 @@ def _main(argv=None):
         case.nsteps = a.steps
     if a.every:
         case.every = a.every
+    if a.a0:
+        case.a0 = a.a0
     p = SlabLaserProblem(case)
     coef, slab = p.nominal()
     coef.requires_grad_(True)
@@ -267,6 +270,13 @@ def _main(argv=None):
     t0 = time.perf_counter()
     l_fwd = p.loss_value(coef.detach(), slab.detach())
     t_fwd = time.perf_counter() - t0
+    # particles erased during the run make the loss jump: the difference
+    # quotients are only meaningful when this is 0
+    with torch.no_grad():
+        r = p.setup.region(p.fields(coef).numpy(), p.weights(slab).numpy())
+        r.step(case.nsteps)
+        erased = p.n_particles - r.count(0)
+        r.close()
     c0, s0 = coef.detach(), slab.detach()
     errs = {}
     for t, name in enumerate(("height", "centre", "width")):
@@ -290,7 +300,8 @@ def _main(argv=None):
     print(json.dumps({"workload": f"slab + Gauss-Hermite laser, {case.nx}x{case.ny}x{case.nz} cells, "
                                   f"{p.n_particles} electrons, {case.nsteps} steps, checkpoint every {case.every}",
                       "loss": loss.item(), "loss_forward_only": l_fwd, "seconds_loss_and_gradient": t_grad,
-                      "seconds_forward": t_fwd, "max_abs_gradient": gmax, "checks": errs}))
+                      "seconds_forward": t_fwd, "particles_erased": erased, "max_abs_gradient": gmax,
+                      "checks": errs}))
 
 
 if __name__ == "__main__":
