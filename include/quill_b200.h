@@ -192,6 +192,21 @@ int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
  * particles' energy unless it catches them, main.cpp:1516-1689). */
 int qp_set_erased_tracking(qp_handle* h, int enable);
 
+/* Particle merging modes (the reference's `pmerging` parameter, main.cpp:3397). */
+enum { QP_MERGE_TI = 1, QP_MERGE_NL = 2 };
+
+/* spatial_region::pmerging (mc.cpp:198-462), called by the time loop before
+ * a step when evaluate_merging_condition (main.cpp:1691-1748) found too many
+ * macro-particles.  ppd holds one deletion probability per species in table
+ * order ([0, 1)); QP_MERGE_TI deletes every particle with ppd[0],
+ * QP_MERGE_NL each species' particles with ppd[s] / (1 + (2|q|/<|q|>)^4)
+ * and rescales the survivors by 1 / (1 - that probability).  The weights
+ * of each species are then renormalised to keep its total charge.  The
+ * survivors keep their traversal order.  The random numbers are the
+ * counter-based stream of the handle's seed, so the deletions match the
+ * reference in distribution, not particle for particle. */
+int qp_pmerging(qp_handle* h, int mode, const double* ppd);
+
 /* Discrete adjoint (no reference counterpart): runs nsteps steps from the
  * handle's current state and returns the loss L = energy_e after the last
  * step (compute_energy's electron kinetic energy, fout.cpp:87-138) with its

@@ -96,6 +96,7 @@ def _load(kind: str, flavour: str):
         "tilde_w": fn("tilde_w", _D, C.c_void_p, _D, _D, _D),
         "mathcal_W": fn("mathcal_W", _D, C.c_void_p, _DP, _DP),
         "get_rand": fn("get_rand", _D, C.c_void_p),
+        "pmerging": fn("pmerging", None, C.c_void_p, C.c_int, _DP),
     }
     _LIBS[key] = api
     return api
@@ -125,6 +126,7 @@ class Region:
         else:
             n_ion = ic.size
         self._icmr = ic
+        self.n_ion = n_ion
         self.h = self.api["create"](nx, ny, nz, dx, dy, dz, dt, lambda_cm, solver, pusher,
                                     int(bool(qed)), n_ion, _dp(ic), int(seed))
 
@@ -231,6 +233,14 @@ class Region:
 
     def get_rand(self):
         return self.api["get_rand"](self.h)
+
+    def pmerging(self, mode: str, ppd):
+        """spatial_region::pmerging; mode "ti" or "nl", ppd per class
+        (electrons, positrons, photons, then the ion populations)."""
+        p = np.zeros(3 + self.n_ion)
+        v = np.asarray(ppd, dtype=np.float64).reshape(-1)
+        p[:min(v.size, p.size)] = v[:p.size]
+        self.api["pmerging"](self.h, 1 if mode == "ti" else 2, _dp(p))
 
 
 def push(pusher, cmr, state, e, b, dt, kind="port", flavour="parity"):

@@ -783,6 +783,104 @@ double qor_get_rand(qor_region* r) {
     return a;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Particle merging (mc.cpp:198-462)                                           */
+/* ------------------------------------------------------------------------ */
+/* class index of a particle: 0 electrons, 1 positrons, 2 photons, 3+ii ions;
+ * -1 for an ion cmr not in the table (the reference skips those) */
+static int merge_class(const qor_region* r, double cmr) {
+    if (cmr == -1) return 0;
+    if (cmr == 1) return 1;
+    if (cmr == 0) return 2;
+    for (int ii = 0; ii < r->n_ion; ii++)
+        if (cmr == r->icmr[ii]) return 3 + ii;
+    return -1;
+}
+
+/* _ppd (mc.cpp:198-200) */
+static double merge_ppd(double q, double q0) { return 1 / (1 + pow(2 * q / q0, 4)); }
+
+static void merge_erase(qor_region* r, const char* keep) {
+    long m = 0;
+    for (long t = 0; t < r->n; t++) {
+        if (!keep[t]) continue;
+        r->x[m] = r->x[t]; r->y[m] = r->y[t]; r->z[m] = r->z[t];
+        r->ux[m] = r->ux[t]; r->uy[m] = r->uy[t]; r->uz[m] = r->uz[t];
+        r->g[m] = r->g[t]; r->q[m] = r->q[t]; r->cmr[m] = r->cmr[t]; r->chi[m] = r->chi[t];
+        r->cell[m] = r->cell[t];
+        m++;
+    }
+    r->n = m;
+}
+
+/* spatial_region::pmerging: particles are deleted with probability ppd
+ * ("ti": ppd[0] for all; "nl": ppd of the class times _ppd of the weight
+ * relative to the class's mean weight), drawing one random number per
+ * particle in traversal order; the weights are then rescaled so that the
+ * total charge of each class is kept. */
+void qor_pmerging(qor_region* r, int mode, const double* ppd) {
+    const int nk = 3 + r->n_ion;
+    double qs[19], a[19];
+    for (int i = 0; i < nk; i++) { qs[i] = 0; a[i] = 0; }
+    for (long t = 0; t < r->n; t++) {
+        const int c = merge_class(r, r->cmr[t]);
+        if (c == 0) a[0] -= r->q[t];
+        else if (c > 0) a[c] += r->q[t];
+    }
+    char* keep = (char*)malloc(r->n > 0 ? (size_t)r->n : 1);
+    if (mode == 1) {
+        for (long t = 0; t < r->n; t++) {
+            keep[t] = 1;
+            if (qor_get_rand(r) < ppd[0]) {
+                const int c = merge_class(r, r->cmr[t]);
+                if (c == 0) qs[0] -= r->q[t];
+                else if (c > 0) qs[c] += r->q[t];
+                keep[t] = 0;
+            }
+        }
+        merge_erase(r, keep);
+        for (int i = 0; i < nk; i++)
+            if (a[i] - qs[i] != 0) a[i] = a[i] / (a[i] - qs[i]);
+        for (long t = 0; t < r->n; t++) {
+            const int c = merge_class(r, r->cmr[t]);
+            if (c >= 0) r->q[t] = a[c] * r->q[t];
+        }
+    } else {
+        double av_q[19];
+        for (int i = 0; i < nk; i++) av_q[i] = 0;
+        for (long t = 0; t < r->n; t++) {
+            const int c = merge_class(r, r->cmr[t]);
+            if (c >= 0) av_q[c] += 1;
+        }
+        for (int i = 0; i < nk; i++) av_q[i] = a[i] / av_q[i];
+        for (long t = 0; t < r->n; t++) {
+            keep[t] = 1;
+            const int c = merge_class(r, r->cmr[t]);
+            if (c < 0) continue;
+            const double qq = c == 0 ? -r->q[t] : r->q[t];
+            if (qor_get_rand(r) < ppd[c] * merge_ppd(qq, av_q[c])) keep[t] = 0;
+        }
+        merge_erase(r, keep);
+        for (long t = 0; t < r->n; t++) {
+            const int c = merge_class(r, r->cmr[t]);
+            if (c < 0) continue;
+            if (c == 0) {
+                r->q[t] = r->q[t] / (1 - ppd[0] * merge_ppd(-r->q[t], av_q[0]));
+                qs[0] -= r->q[t];
+            } else {
+                r->q[t] = r->q[t] / (1 - ppd[c] * merge_ppd(r->q[t], av_q[c]));
+                qs[c] += r->q[t];
+            }
+        }
+        for (int i = 0; i < nk; i++) a[i] = qs[i] != 0 ? a[i] / qs[i] : 0;
+        for (long t = 0; t < r->n; t++) {
+            const int c = merge_class(r, r->cmr[t]);
+            if (c >= 0) r->q[t] = a[c] * r->q[t];
+        }
+    }
+    free(keep);
+}
+
 /* quantum parameter chi = |gamma E + u x B|^2 - (u.E)^2, square-rooted and
  * divided by the Sauter field (mc.cpp:26-38) */
 double qor_chi(qor_region* r, const double* e, const double* b, const double* u, double g) {

@@ -320,4 +320,12 @@ double qref_mathcal_W(void* h, const double* e, const double* b) {
 // Lagged-Fibonacci stream (mc.cpp:12-23) seeded by create_arrays(seed).
 double qref_get_rand(void* h) { return ((RefRegion*)h)->sr.get_rand(); }
 
+// spatial_region::pmerging (mc.cpp:202-462).  mode 1 = "ti", 2 = "nl";
+// ppd has 3 + n_ion entries (electrons, positrons, photons, ion populations).
+void qref_pmerging(void* h, int mode, const double* ppd) {
+    RefRegion* r = (RefRegion*)h;
+    std::vector<double> p(ppd, ppd + 3 + r->icmr.size());
+    r->sr.pmerging(p.data(), mode == 1 ? "ti" : "nl");
+}
+
 }  // extern "C"

@@ -107,6 +107,7 @@ def load_library(path: str | None = None):
         "qp_eval_qed_rates_noalloc": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
         "qp_set_erased_tracking": (C.c_int, [VP, C.c_int]),
+        "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
         "qp_adjoint_energy": (C.c_int, [VP, C.c_int, C.c_int, D, DP, DP, DP]),
     }
     for name, (res, args) in sig.items():
@@ -247,6 +248,14 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def pmerging(self, mode: str, ppd):
+        """Particle merging ("ti" or "nl"); ppd per species in table order
+        ("ti" uses ppd[0] for all)."""
+        p = np.zeros(self.n_species)
+        v = np.asarray(ppd, dtype=np.float64).reshape(-1)
+        p[:min(v.size, p.size)] = v[:p.size]
+        self._check(self.lib.qp_pmerging(self.h, 1 if mode == "ti" else 2, _dp(p)))
 
     def set_erased_tracking(self, enable: bool = True):
         """Report in Diag.energy_erased the energy of the particles each step

@@ -35,6 +35,7 @@ SOURCES = [
     ("qp_load.cu", []),
     ("qp_noalloc.cu", []),
     ("qp_adjoint.cu", ["--fmad=false"]),
+    ("qp_merge.cu", []),
     ("qp_api.cu", []),
 ]
 HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh", "qp_dual.cuh"]

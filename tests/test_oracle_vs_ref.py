@@ -103,3 +103,32 @@ def test_unit_functions_equal_reference():
         assert ref.mathcal_W(e2, b) == port.mathcal_W(e2, b)
     for _ in range(500):
         assert ref.get_rand() == port.get_rand()
+
+
+@needs_ref
+@pytest.mark.parametrize("mode,ppd", [("ti", [0.3]), ("nl", [0.6, 0.4, 0.8, 0.5])])
+def test_merging_equals_reference(mode, ppd):
+    """spatial_region::pmerging (mc.cpp:202-462): the same particles deleted
+    (one draw of the lagged-Fibonacci stream per particle, traversal order),
+    the same rescaled weights, then the same steps."""
+    _ensure_port()
+    species = (-1.0, 1.0, 0.0, 1 / 1836.15)
+    case, fields, parts = small_case(species=species, ppc=3)
+    # weights spread over a decade so that "nl" prefers the light ones
+    rng = np.random.default_rng(11)
+    for p in parts:
+        p["q"] = p["q"] * rng.uniform(0.3, 3.0, p["q"].size)
+    ref, port = _region("ref", case, icmr=(1 / 1836.15,)), _region("port", case, icmr=(1 / 1836.15,))
+    for r in (ref, port):
+        _load(r, fields, parts)
+        r.step(1)
+    n0 = ref.count()
+    for r in (ref, port):
+        r.pmerging(mode, ppd)
+    a, b = ref.get_particles(), port.get_particles()
+    assert 0 < ref.count() < n0
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    dr, dp = ref.step(2), port.step(2)
+    np.testing.assert_array_equal(dr, dp)
+    np.testing.assert_array_equal(ref.get_fields(), port.get_fields())
