@@ -20,7 +20,8 @@
 // y0film y1film z0film z1film nfilm mcr Tfilm vxfilm xnpic_film ynpic_film
 // znpic_film xnpic ynpic znpic ions data_folder output_mode
 // e_components_for_output b_components_for_output particles_for_output enthp
-// mwindow (off only) and two additions: precision (fp64 | mixed) and seed.
+// pmerging crpc mwindow (off only) and two additions: precision (fp64 |
+// mixed) and seed.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -112,6 +113,8 @@ struct Config {
     int precision = QP_PREC_FP64;
     uint64_t seed = 0;
     std::string polarization = "linear";
+    std::string pmerging = "off";  // off | ti | nl (main.cpp:3397-3399)
+    double crpc = 0;               // critical macro-particles per cell (main.cpp:3400-3401)
 };
 
 Config parse(const std::vector<Var>& v) {
@@ -230,6 +233,11 @@ Config parse(const std::vector<Var>& v) {
     const std::string pr = find(v, "precision").units;
     if (pr == "mixed") c.precision = QP_PREC_MIXED;
     c.seed = (uint64_t)find(v, "seed").value;
+    c.pmerging = find(v, "pmerging").units;
+    if (c.pmerging.empty()) c.pmerging = "off";
+    if (c.pmerging != "off" && c.pmerging != "ti" && c.pmerging != "nl")
+        throw std::runtime_error("pmerging must be off, ti or nl");
+    c.crpc = find(v, "crpc").value;
     return c;
 }
 
@@ -513,7 +521,42 @@ int main() {
         L << "solver = " << (c.solver == QP_SOLVER_FDTD ? "fdtd" : c.solver == QP_SOLVER_NDFX ? "ndfx" : "five_point") << "\n";
         L << "pusher = " << (c.pusher == QP_PUSHER_BORIS ? "boris" : "vay") << "\n";
         L << "precision = " << (c.precision == QP_PREC_MIXED ? "mixed" : "fp64") << "\n";
+        L << "pmerging\n" << c.pmerging << "\ncrpc\n" << c.crpc << "\n";
     }
+
+    // particle merging: evaluate_merging_condition (main.cpp:1691-1748) after
+    // each step, pmerging before the next (main.cpp:2321-2322); ppd is kept
+    // per class (electrons, positrons, photons, ion populations) and mapped
+    // onto the species table
+    const int n_ion = (int)icmr.size();
+    const double crnp = c.crpc * c.xlength * c.ylength * c.zlength / (c.dx * c.dy * c.dz);
+    bool merge_now = false;
+    std::vector<double> ppd(3 + n_ion, 0.0), ppd_sp(QP_MAX_SPECIES, 0.0);
+    auto evaluate_merging = [&](const qp_diag& d) {
+        merge_now = false;
+        if (c.pmerging == "ti") {
+            int64_t nq = d.N_qp_e + d.N_qp_p + d.N_qp_g;
+            for (int i = 0; i < n_ion; i++) nq += d.N_qp_i[i];
+            if (nq > (3 + n_ion) * crnp) {
+                merge_now = true;
+                ppd[0] = (nq - (3 + n_ion) * crnp) / nq;
+                for (int s2 = 0; s2 < QP_MAX_SPECIES; s2++) ppd_sp[s2] = ppd[0];
+            }
+        } else if (c.pmerging == "nl") {
+            std::vector<int64_t> nq = {d.N_qp_e, d.N_qp_p, d.N_qp_g};
+            for (int i = 0; i < n_ion; i++) nq.push_back(d.N_qp_i[i]);
+            for (size_t k = 0; k < nq.size(); k++) {
+                ppd[k] = nq[k] > crnp ? (nq[k] - crnp) / nq[k] : 0.0;
+                if (nq[k] > crnp) merge_now = true;
+            }
+            ppd_sp.assign(QP_MAX_SPECIES, 0.0);
+            ppd_sp[sp_e] = ppd[0];
+            if (sp_pos >= 0) ppd_sp[sp_pos] = ppd[1];
+            if (sp_ph >= 0) ppd_sp[sp_ph] = ppd[2];
+            for (size_t f = 0; f < sp_ion.size(); f++)
+                if (sp_ion[f] >= 0) ppd_sp[sp_ion[f]] = ppd[3 + (int)(std::find(icmr.begin(), icmr.end(), p.cmr[sp_ion[f]]) - icmr.begin())];
+        }
+    };
 
     // time loop (main.cpp:2319-2432)
     Schedule sch(c.t_end, c.output_period, c.dt);
@@ -523,6 +566,11 @@ int main() {
     const int ix = (int)((c.xlength - c.xlength / 2) / c.dx);
     for (int l = 0; l <= sch.it.back(); l++) {
         qp_diag d;
+        if (merge_now && qp_pmerging(h, c.pmerging == "ti" ? QP_MERGE_TI : QP_MERGE_NL, ppd_sp.data()) != QP_OK) {
+            std::cerr << "qp_driver: merging before step " << l << ": " << qp_last_error(h) << std::endl;
+            qp_destroy(h);
+            return 1;
+        }
         if (qp_step(h, 1, c.external_bz, &d) != QP_OK) {
             std::cerr << "qp_driver: step " << l << ": " << qp_last_error(h) << std::endl;
             qp_destroy(h);
@@ -532,6 +580,7 @@ int main() {
         fE << d.energy_f << '\t' << d.energy_e << '\t' << d.energy_p << '\t' << d.energy_ph;  // write_energy
         for (int m = 0; m < d.n_ion; m++) fE << '\t' << d.ienergy[m];
         fE << std::endl;
+        evaluate_merging(d);
         if (out_i < sch.it.size() && l == sch.it[out_i]) {
             const std::string sfx = Schedule::suffix(sch.t[out_i]);
             qp_dump_fields(h, all.data());

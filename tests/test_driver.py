@@ -91,3 +91,31 @@ def test_driver_rejects_moving_window(tmp_path):
     conf = [c for c in CONF if c[0] != "mwindow"]
     r = subprocess.run([DRIVER], input=stream(conf, str(tmp_path / "r")), text=True, capture_output=True, timeout=60)
     assert r.returncode != 0 and "mwindow" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_particle_merging(tmp_path):
+    """pmerging = ti with a low crpc: the driver merges before the steps that
+    follow an over-full one (main.cpp:1691-1748, 2321-2322).  Merging keeps
+    the charge (the weighted count N_e agrees with a run without merging:
+    exactly while no particle has left the box, within a few per cent after)
+    and thins the macro-particles."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200 import build
+    build.build()
+    out = {}
+    for name, extra in (("plain", []), ("merged", [("pmerging", "#", "ti"), ("crpc", "0.05", "#")])):
+        folder = str(tmp_path / name)
+        r = subprocess.run([DRIVER], input=stream(CONF + extra, folder), text=True, capture_output=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        n = np.array([[float(v) for v in ln.split("\t")] for ln in open(os.path.join(folder, "N"))])
+        ps = len(open(os.path.join(folder, "phasespace0.5")).read().split()) // 9
+        out[name] = (n, ps, open(os.path.join(folder, "log")).read())
+    (n0, ps0, _), (n1, ps1, log1) = out["plain"], out["merged"]
+    assert "pmerging\nti\n" in log1 and "crpc\n0.05\n" in log1
+    lossless = n0[:, 0] == n0[0, 0]
+    assert lossless[:3].all()
+    np.testing.assert_allclose(n1[lossless, 0], n0[lossless, 0], rtol=1e-9)
+    np.testing.assert_allclose(n1[:, 0], n0[:, 0], rtol=0.05)
+    assert ps1 < 0.5 * ps0
