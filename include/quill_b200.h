@@ -192,6 +192,15 @@ int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
  * particles' energy unless it catches them, main.cpp:1516-1689). */
 int qp_set_erased_tracking(qp_handle* h, int enable);
 
+/* spatial_region::moving_window (advance.cpp:389-454), called by the time
+ * loop after a step when check_moving_window (main.cpp:1953-1979) says so:
+ * the particles of the layer i = 0 are erased, E, B and Bbar move one cell
+ * towards -x (the last layer becomes zero; J is left as it is) and every
+ * particle moves one cell towards -x with them.  New plasma for the front
+ * layer is the caller's (qp_load_particles), as add_moving_window_particles
+ * (main.cpp:1750-1883). */
+int qp_moving_window(qp_handle* h);
+
 /* Particle merging modes (the reference's `pmerging` parameter, main.cpp:3397). */
 enum { QP_MERGE_TI = 1, QP_MERGE_NL = 2 };
 

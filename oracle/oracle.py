@@ -97,6 +97,7 @@ def _load(kind: str, flavour: str):
         "mathcal_W": fn("mathcal_W", _D, C.c_void_p, _DP, _DP),
         "get_rand": fn("get_rand", _D, C.c_void_p),
         "pmerging": fn("pmerging", None, C.c_void_p, C.c_int, _DP),
+        "moving_window": fn("moving_window", None, C.c_void_p),
     }
     _LIBS[key] = api
     return api
@@ -233,6 +234,10 @@ class Region:
 
     def get_rand(self):
         return self.api["get_rand"](self.h)
+
+    def moving_window(self):
+        """spatial_region::moving_window: shift everything one cell towards -x."""
+        self.api["moving_window"](self.h)
 
     def pmerging(self, mode: str, ppd):
         """spatial_region::pmerging; mode "ti" or "nl", ppd per class

@@ -784,6 +784,33 @@ double qor_get_rand(qor_region* r) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* Moving window (advance.cpp:389-454)                                          */
+/* ------------------------------------------------------------------------ */
+/* The particles of the layer i = 0 are erased, E, B and Bbar move one cell
+ * towards -x (the layer nx-1 becomes zero; J is left as it is), the cell
+ * lists move with them and every particle's x decreases by 1.  The list
+ * order inside a cell is kept. */
+void qor_moving_window(qor_region* r) {
+    const long ynz = (long)r->ny * r->nz;
+    long m = 0;
+    for (long t = 0; t < r->n; t++) {
+        if (r->cell[t] < ynz) continue;
+        r->x[m] = r->x[t] - 1; r->y[m] = r->y[t]; r->z[m] = r->z[t];
+        r->ux[m] = r->ux[t]; r->uy[m] = r->uy[t]; r->uz[m] = r->uz[t];
+        r->g[m] = r->g[t]; r->q[m] = r->q[t]; r->cmr[m] = r->cmr[t]; r->chi[m] = r->chi[t];
+        r->cell[m] = r->cell[t] - ynz;
+        m++;
+    }
+    r->n = m;
+    const int planes[9] = {0, 1, 2, 3, 4, 5, 9, 10, 11};
+    for (int a = 0; a < 9; a++) {
+        double* f = r->f[planes[a]];
+        memmove(f, f + ynz, sizeof(double) * (size_t)(r->nc - ynz));
+        memset(f + (r->nc - ynz), 0, sizeof(double) * (size_t)ynz);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Particle merging (mc.cpp:198-462)                                           */
 /* ------------------------------------------------------------------------ */
 /* class index of a particle: 0 electrons, 1 positrons, 2 photons, 3+ii ions;

@@ -42,6 +42,8 @@ double qor_w(qor_region* r, double g, double* rr, double chi);
 double qor_tilde_w(qor_region* r, double g, double rr, double chi);
 double qor_mathcal_W(qor_region* r, const double* e, const double* b);
 double qor_get_rand(qor_region* r);
+/* spatial_region::moving_window: shift by one cell towards -x */
+void qor_moving_window(qor_region* r);
 /* particle merging, mode 1 "ti", 2 "nl"; ppd[3 + n_ion] */
 void qor_pmerging(qor_region* r, int mode, const double* ppd);
 

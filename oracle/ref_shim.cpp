@@ -320,6 +320,9 @@ double qref_mathcal_W(void* h, const double* e, const double* b) {
 // Lagged-Fibonacci stream (mc.cpp:12-23) seeded by create_arrays(seed).
 double qref_get_rand(void* h) { return ((RefRegion*)h)->sr.get_rand(); }
 
+// spatial_region::moving_window (advance.cpp:389-454).
+void qref_moving_window(void* h) { ((RefRegion*)h)->sr.moving_window(); }
+
 // spatial_region::pmerging (mc.cpp:202-462).  mode 1 = "ti", 2 = "nl";
 // ppd has 3 + n_ion entries (electrons, positrons, photons, ion populations).
 void qref_pmerging(void* h, int mode, const double* ppd) {

@@ -108,6 +108,7 @@ def load_library(path: str | None = None):
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
         "qp_set_erased_tracking": (C.c_int, [VP, C.c_int]),
         "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
+        "qp_moving_window": (C.c_int, [VP]),
         "qp_adjoint_energy": (C.c_int, [VP, C.c_int, C.c_int, D, DP, DP, DP]),
     }
     for name, (res, args) in sig.items():
@@ -248,6 +249,10 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def moving_window(self):
+        """Shift the region one cell towards -x (spatial_region::moving_window)."""
+        self._check(self.lib.qp_moving_window(self.h))
 
     def pmerging(self, mode: str, ppd):
         """Particle merging ("ti" or "nl"); ppd per species in table order

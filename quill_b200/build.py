@@ -36,6 +36,7 @@ SOURCES = [
     ("qp_noalloc.cu", []),
     ("qp_adjoint.cu", ["--fmad=false"]),
     ("qp_merge.cu", []),
+    ("qp_window.cu", []),
     ("qp_api.cu", []),
 ]
 HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh", "qp_dual.cuh"]

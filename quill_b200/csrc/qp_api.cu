@@ -144,6 +144,8 @@ static void free_state(State* s) {
     cudaFreeHost(s->h_diag);
     cudaFree(s->d_status);
     cudaFree(s->long_list);
+    cudaFree(s->window_scratch);
+    s->window_scratch = nullptr;
     s->long_list = nullptr;
     cudaFree(s->scan_tmp);
     for (auto& e : s->ev)

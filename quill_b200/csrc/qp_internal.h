@@ -125,6 +125,7 @@ struct State {
     // diagnostics + J reset)
     bool timing = false;
     bool track_erased = false;  // qp_set_erased_tracking
+    void* window_scratch = nullptr;  // one field plane, for the moving window's shift
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double phase_ms[4] = {0, 0, 0, 0};
     int64_t phase_steps = 0;

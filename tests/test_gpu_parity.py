@@ -164,3 +164,49 @@ def test_mixed_precision_close(solver):
         # a particle within FP32 round-off of a face may land in the
         # neighbouring cell; counts must still agree closely
         assert abs(gp["x"].size - cp[0]["x"].size) <= max(2, gp["x"].size // 2000)
+
+
+def test_moving_window_fp64():
+    """spatial_region::moving_window (advance.cpp:389-454) on the GPU: exact
+    data movement (bit-identical right after loading), then steps and
+    shifts alternating stay within the step parity tolerance."""
+    species = (-1.0, 1 / 1836.15)
+    case, fields, parts = small_case("fdtd", "boris", species=species)
+    g, c = _load_both(case, fields, parts, species)
+    g.moving_window()
+    c.moving_window()
+    assert np.array_equal(g.get_fields()[[0, 1, 2, 3, 4, 5, 9, 10, 11]], c.get_fields()[[0, 1, 2, 3, 4, 5, 9, 10, 11]])
+    cp = _split_by_species(c.get_particles(), species)
+    for i in range(len(species)):
+        gp = g.get_particles(i)
+        for k in ("x", "y", "z", "ux", "q", "cell"):
+            assert np.array_equal(gp[k], cp[i][k]), (i, k)
+    for _ in range(3):
+        g.step(1)
+        c.step(1)
+        g.moving_window()
+        c.moving_window()
+        fg, fc = g.get_fields(), c.get_fields()
+        for a in range(12):
+            assert _rel(fg[a], fc[a]) <= RTOL64, a
+        cp = _split_by_species(c.get_particles(), species)
+        for i in range(len(species)):
+            gp = g.get_particles(i)
+            assert np.array_equal(gp["cell"], cp[i]["cell"])
+            for k in ("x", "ux", "q"):
+                assert _rel(gp[k], cp[i][k]) <= RTOL64
+
+
+def test_moving_window_mixed():
+    species = (-1.0,)
+    case, fields, parts = small_case("fdtd", "boris", species=species)
+    g, c = _load_both(case, fields, parts, species, precision="mixed")
+    for _ in range(3):
+        g.step(1)
+        c.step(1)
+        g.moving_window()
+        c.moving_window()
+    fg, fc = g.get_fields(), c.get_fields()
+    for a in range(6):
+        assert _rel(fg[a], fc[a]) <= 1e-4, a
+    assert abs(g.count(0) - c.count()) <= max(2, c.count() // 2000)

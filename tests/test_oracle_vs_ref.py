@@ -132,3 +132,27 @@ def test_merging_equals_reference(mode, ppd):
     dr, dp = ref.step(2), port.step(2)
     np.testing.assert_array_equal(dr, dp)
     np.testing.assert_array_equal(ref.get_fields(), port.get_fields())
+
+
+@needs_ref
+def test_moving_window_equals_reference():
+    """spatial_region::moving_window (advance.cpp:389-454) between steps."""
+    _ensure_port()
+    species = (-1.0, 1 / 1836.15)
+    case, fields, parts = small_case(species=species, ppc=2)
+    ref, port = _region("ref", case, icmr=(1 / 1836.15,)), _region("port", case, icmr=(1 / 1836.15,))
+    for r in (ref, port):
+        _load(r, fields, parts)
+    for _ in range(3):
+        dr, dp = ref.step(1), port.step(1)
+        np.testing.assert_array_equal(dr, dp)
+        before = ref.get_particles()
+        ynz = case.ny * case.nz
+        ref.moving_window()
+        port.moving_window()
+        assert ref.count() == int(np.sum(before["cell"] >= ynz))
+        np.testing.assert_array_equal(ref.get_particles()["x"], before["x"][before["cell"] >= ynz] - 1)
+        a, b = ref.get_particles(), port.get_particles()
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+        np.testing.assert_array_equal(ref.get_fields(), port.get_fields())
