@@ -20,8 +20,10 @@
 // y0film y1film z0film z1film nfilm mcr Tfilm vxfilm xnpic_film ynpic_film
 // znpic_film xnpic ynpic znpic ions data_folder output_mode
 // e_components_for_output b_components_for_output particles_for_output enthp
-// pmerging crpc mwindow (off only) and two additions: precision (fp64 |
-// mixed) and seed.
+// pmerging crpc mwindow (off | on) mwspeed mwseed t_add_mw and two
+// additions: precision (fp64 | mixed) and seed.  Not supported (the driver
+// stops with a message): mwindow = auto, mwseed_ions, neutral flows, density
+// profile arrays.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -113,6 +115,10 @@ struct Config {
     int precision = QP_PREC_FP64;
     uint64_t seed = 0;
     std::string polarization = "linear";
+    bool mwindow = false;          // main.cpp:2932-2938 (on only)
+    double mwspeed = 1;            // main.cpp:2944-2947
+    bool mwseed = true;            // main.cpp:2948-2950
+    double t_add_mw = 0;           // main.cpp:2665-2679, 1/omega (0: last output time)
     std::string pmerging = "off";  // off | ti | nl (main.cpp:3397-3399)
     double crpc = 0;               // critical macro-particles per cell (main.cpp:3400-3401)
 };
@@ -194,8 +200,27 @@ Config parse(const std::vector<Var>& v) {
     else throw std::runtime_error("Pusher unknown: " + pu);
     const std::string q = find(v, "qed").units;
     c.qed = !(q == "off");
-    if (find(v, "mwindow").units != "off")
-        throw std::runtime_error("set mwindow = off: the moving window is not part of this build");
+    const std::string mw = find(v, "mwindow").units;
+    if (mw == "auto" || (mw != "off" && mw != "on" && !mw.empty()))
+        throw std::runtime_error("mwindow must be off or on (auto is not part of this build)");
+    if (mw.empty() || mw == "on") {  // the reference's default is on
+        c.mwindow = true;
+        c.mwspeed = find(v, "mwspeed").value;
+        if (c.mwspeed == 0) c.mwspeed = 1;
+        c.mwseed = find(v, "mwseed").units != "off";
+        const Var& ta = find(v, "t_add_mw");
+        double tv = ta.value;
+        if (ta.units == "um") tv = tv * 1e-4 / c.lambda;
+        else if (ta.units == "mm") tv = tv / (10 * c.lambda);
+        else if (ta.units == "cm") tv = tv / c.lambda;
+        c.t_add_mw = tv * 2 * PI;
+        if (find(v, "mwseed_ions").units == "on")
+            throw std::runtime_error("mwseed_ions is not part of this build");
+        if (find(v, "nelflow").value != 0 || find(v, "nerflow").value != 0)
+            throw std::runtime_error("neutral flows are not part of this build");
+        if (!find(v, "ne_profile_x_coords").units.empty() || !find(v, "ne_profile_r_coords").units.empty())
+            throw std::runtime_error("density profile arrays are not part of this build");
+    }
     // films (main.cpp:3055-3229)
     c.xnpic = (int)find(v, "xnpic").value; if (c.xnpic <= 0) c.xnpic = 1;
     c.ynpic = (int)find(v, "ynpic").value; if (c.ynpic <= 0) c.ynpic = 1;
@@ -347,21 +372,31 @@ void fill_cell(Parts& P, double cmr, int ci, int cj, int ck, int xn, int yn, int
 }
 
 // film (init.cpp:537-646) without transverse profile or y-gradient.
+// shift: how far the window has moved (x0 of the film in window coordinates
+// is x0 - shift); append: fill only the layer nx-3 the window just exposed,
+// if the film covers it (append_for_moving_window, init.cpp:559-570)
 void film(const Config& c, const Grid3& g, const Film& f, Parts& e, Parts* ion, double ion_cmr, Parts* pos,
-          std::mt19937_64& rng) {
-    int i0 = (int)(f.x0 / c.dx), i1 = (int)((f.x0 + f.width) / c.dx);
-    i0 = std::max(0, std::min(i0, g.nx));
-    i1 = std::max(0, std::min(i1, g.nx));
+          std::mt19937_64& rng, double shift = 0, bool append = false) {
+    int i0 = (int)((f.x0 - shift) / c.dx), i1 = (int)((f.x0 + f.width - shift) / c.dx);
+    if (append) {
+        i0 = g.nx - 3;
+        if (i0 < g.nx - 2 && i1 >= g.nx - 2) i1 = g.nx - 2;
+        else i1 = i0;
+    } else {
+        i0 = std::max(0, std::min(i0, g.nx));
+        i1 = std::max(0, std::min(i1, g.nx));
+    }
     const double n_norm = f.ne / (1.11485e+13 / c.lambda / c.lambda);
     const double ux0 = f.vx / std::sqrt(1 - f.vx * f.vx);
     for (int i = i0; i < i1; i++)
         for (int j = (int)(f.y0 / c.dy) + 1; j < (int)(f.y1 / c.dy) - 1; j++)
             for (int k = (int)(f.z0 / c.dz) + 1; k < (int)(f.z1 / c.dz) - 1; k++) {
                 double nes = n_norm;
+                const double fx0 = f.x0 - shift;
                 if (f.grad >= 0) {
-                    if (!(i >= (int)((f.x0 + f.grad) / c.dx))) nes = nes * (i * c.dx - f.x0) / f.grad;
+                    if (!(i >= (int)((fx0 + f.grad) / c.dx))) nes = nes * (i * c.dx - fx0) / f.grad;
                 } else {
-                    if (!(i >= (int)((f.x0 - f.grad) / c.dx))) nes = nes * (1 + (i * c.dx - f.x0) / f.grad);
+                    if (!(i >= (int)((fx0 - f.grad) / c.dx))) nes = nes * (1 + (i * c.dx - fx0) / f.grad);
                 }
                 if (!(nes > 0)) continue;
                 fill_cell(e, -1, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T, rng);
@@ -506,7 +541,7 @@ int main() {
         L << "xsigma\n" << c.xsigma / 2 / PI << "\nysigma\n" << c.ysigma / 2 / PI << "\nzsigma\n" << c.zsigma / 2 / PI << "\n";
         L << "x0fout\n" << c.xlength / 2 / 2 / PI << "\n";
         L << "a0y\n" << c.a0y << "\na0z\n" << c.a0z << "\n";
-        L << "mwindow\noff\n";
+        L << "mwindow\n" << (c.mwindow ? "on" : "off") << "\n";
         L << "e_components_for_output\n" << c.e_out << "\nb_components_for_output\n" << c.b_out << "\n";
         L << "n_ion_populations\n" << icmr.size() << "\n";
         for (double v : icmr) L << "icmr\n" << v << "\n";
@@ -564,6 +599,39 @@ int main() {
     size_t out_i = 0;
     std::vector<double> all(12 * (size_t)g.nc());
     const int ix = (int)((c.xlength - c.xlength / 2) / c.dx);
+    // moving window state (main.cpp:122, 2665-2679)
+    int nmw = 1;
+    const double t_add_mw = c.t_add_mw != 0 ? c.t_add_mw : sch.it.back() * c.dt;
+    std::ofstream fMW;
+    if (c.mwindow) fMW.open(c.data_folder + "/mwcoordinate");
+    // add_moving_window_particles (main.cpp:1750-1883): the layer nx-3 the
+    // window exposed gets uniform plasma (mwseed, density ne) and the part of
+    // every film it now covers
+    auto add_window_particles = [&](int l) -> int {
+        if (!((l + 1) * c.dt < t_add_mw)) return QP_OK;
+        Parts Em, Pm;
+        std::vector<Parts> Im(c.films.size());
+        if (c.mwseed && c.ne > 0) {
+            const double n = c.ne / (1.11485e+13 / c.lambda / c.lambda);  // 1 / k0^2 (main.cpp:2602)
+            for (int j = 0; j < (int)(c.ylength / c.dy); j++)
+                for (int k = 0; k < (int)(c.zlength / c.dz); k++)
+                    fill_cell(Em, -1, g.nx - 3, j, k, c.xnpic, c.ynpic, c.znpic, n, 0, 0, rng);
+        }
+        for (size_t f = 0; f < c.films.size(); f++)
+            film(c, g, c.films[f], Em, sp_ion[f] >= 0 ? &Im[f] : nullptr, sp_ion[f] >= 0 ? icmr[f] : 0,
+                 c.ions == "positrons" ? &Pm : nullptr, rng, nmw * c.dx, true);
+        int rr = QP_OK;
+        auto put = [&](int sp, Parts& P) {
+            if (rr == QP_OK && !P.x.empty())
+                rr = qp_load_particles(h, sp, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
+                                       P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
+        };
+        put(sp_e, Em);
+        for (size_t f = 0; f < c.films.size(); f++)
+            if (sp_ion[f] >= 0) put(sp_ion[f], Im[f]);
+        if (sp_pos >= 0) put(sp_pos, Pm);
+        return rr;
+    };
     for (int l = 0; l <= sch.it.back(); l++) {
         qp_diag d;
         if (merge_now && qp_pmerging(h, c.pmerging == "ti" ? QP_MERGE_TI : QP_MERGE_NL, ppd_sp.data()) != QP_OK) {
@@ -580,6 +648,17 @@ int main() {
         fE << d.energy_f << '\t' << d.energy_e << '\t' << d.energy_p << '\t' << d.energy_ph;  // write_energy
         for (int m = 0; m < d.n_ion; m++) fE << '\t' << d.ienergy[m];
         fE << std::endl;
+        // check_moving_window, mode on (main.cpp:1953-1959, 2333-2336)
+        const bool mw_now = c.mwindow && (l + 1) * c.dt * c.mwspeed > nmw * c.dx;
+        if (mw_now) {
+            if (qp_moving_window(h) != QP_OK) {
+                std::cerr << "qp_driver: moving window after step " << l << ": " << qp_last_error(h) << std::endl;
+                qp_destroy(h);
+                return 1;
+            }
+            nmw++;
+        }
+        if (c.mwindow) fMW << ((nmw - 1) * c.dx / 2 / PI) << std::endl;  // write_mwcoordinate
         evaluate_merging(d);
         if (out_i < sch.it.size() && l == sch.it[out_i]) {
             const std::string sfx = Schedule::suffix(sch.t[out_i]);
@@ -635,6 +714,11 @@ int main() {
                 }
             }
             out_i++;
+        }
+        if (mw_now && add_window_particles(l) != QP_OK) {
+            std::cerr << "qp_driver: window plasma after step " << l << ": " << qp_last_error(h) << std::endl;
+            qp_destroy(h);
+            return 1;
         }
     }
     qp_destroy(h);

@@ -83,14 +83,36 @@ def test_driver_runs_conf_stream_and_writes_reference_formats(tmp_path):
     assert np.abs(ey0).max() > 1 and not np.allclose(ey0, ey1)
 
 
-def test_driver_rejects_moving_window(tmp_path):
-    """The reference's default mwindow is on (main.cpp:2932-2938); without
-    mwindow = off the driver refuses before touching a device."""
+def test_driver_rejects_automatic_window(tmp_path):
+    """mwindow = auto (main.cpp:1961-1977) is not part of this build: the
+    driver refuses before touching a device."""
     from quill_b200 import build
     build.build()
-    conf = [c for c in CONF if c[0] != "mwindow"]
+    conf = [c for c in CONF if c[0] != "mwindow"] + [("mwindow", "#", "auto")]
     r = subprocess.run([DRIVER], input=stream(conf, str(tmp_path / "r")), text=True, capture_output=True, timeout=60)
     assert r.returncode != 0 and "mwindow" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_moving_window(tmp_path):
+    """Without mwindow the reference's default, on, applies: the window moves
+    one cell whenever (l + 1) dt mwspeed passes nmw dx (main.cpp:1953-1959),
+    the mwcoordinate file follows it, and the exposed front layer is seeded
+    with the uniform plasma ne (add_moving_window_particles)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200 import build
+    build.build()
+    folder = str(tmp_path / "results")
+    conf = [c for c in CONF if c[0] != "mwindow"]
+    r = subprocess.run([DRIVER], input=stream(conf, folder), text=True, capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "mwindow\non\n" in open(os.path.join(folder, "log")).read()
+    mw = np.loadtxt(os.path.join(folder, "mwcoordinate"))
+    assert mw.size == 17 and np.all(np.diff(mw) >= 0)
+    np.testing.assert_allclose(mw[-1], 8 * 0.0625, rtol=1e-12)   # 8 shifts of dx = lambda/16
+    n = np.array([[float(v) for v in ln.split("\t")] for ln in open(os.path.join(folder, "N"))])
+    assert n[-1, 0] > 1.05 * n[0, 0]   # new plasma entered at the front
 
 
 @pytest.mark.gpu
