@@ -80,6 +80,8 @@ typedef struct {
                                             (p_boundary and place), with the normalisation and
                                             species signs of the energy terms; 0 unless enabled by
                                             qp_set_erased_tracking.  No reference counterpart. */
+    double energy_erased_sp[QP_MAX_SPECIES]; /* the same per species (table order), as
+                                            update_energy_deleted (low-level.cpp:288-313) */
 } qp_diag;
 
 typedef struct qp_handle qp_handle;
@@ -200,6 +202,25 @@ int qp_set_erased_tracking(qp_handle* h, int enable);
  * layer is the caller's (qp_load_particles), as add_moving_window_particles
  * (main.cpp:1750-1883). */
 int qp_moving_window(qp_handle* h);
+
+/* Catching (catching = on: delete_particle, low-level.cpp:247-259): record
+ * every particle the steps erase (p_boundary before the push, place() after
+ * it) into a device buffer of `capacity` records; enable = 0 frees it.
+ * Records beyond the capacity are dropped and counted.  Use with
+ * qp_set_erased_tracking for the energy_deleted output.  Photons or pairs
+ * born outside the region (QED) are not recorded. */
+int qp_set_catching(qp_handle* h, int enable, int64_t capacity);
+
+/* The recorded particles (species index, position in cell units, u, g, q,
+ * chi), ordered by species, then as the reference deletes them: by step,
+ * the p_boundary erasures before the moves out of the region, each in
+ * traversal order.  With every array pointer NULL only *n_out (and
+ * *dropped) are set and the buffer is kept; otherwise cap must be at least
+ * *n_out, the records are copied (host or device arrays, each nullable) and
+ * the buffer is emptied, as write_deleted_particles clears its list
+ * (main.cpp:189-330). */
+int qp_get_caught(qp_handle* h, int64_t cap, int32_t* species, double* x, double* y, double* z, double* ux,
+                  double* uy, double* uz, double* g, double* q, double* chi, int64_t* n_out, int64_t* dropped);
 
 /* Particle merging modes (the reference's `pmerging` parameter, main.cpp:3397). */
 enum { QP_MERGE_TI = 1, QP_MERGE_NL = 2 };

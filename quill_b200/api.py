@@ -58,6 +58,7 @@ class Diag(C.Structure):
         ("n_macro", C.c_int64 * QP_MAX_SPECIES),
         ("status", C.c_int32), ("pad_", C.c_int32),
         ("energy_erased", C.c_double),
+        ("energy_erased_sp", C.c_double * QP_MAX_SPECIES),
     ]
 
     def as_array(self) -> np.ndarray:
@@ -109,6 +110,8 @@ def load_library(path: str | None = None):
         "qp_set_erased_tracking": (C.c_int, [VP, C.c_int]),
         "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
         "qp_moving_window": (C.c_int, [VP]),
+        "qp_set_catching": (C.c_int, [VP, C.c_int, I64]),
+        "qp_get_caught": (C.c_int, [VP, I64, C.POINTER(C.c_int32)] + [DP] * 9 + [I64P, I64P]),
         "qp_adjoint_energy": (C.c_int, [VP, C.c_int, C.c_int, D, DP, DP, DP]),
     }
     for name, (res, args) in sig.items():
@@ -249,6 +252,27 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_catching(self, enable: bool = True, capacity: int = 1 << 20):
+        """Record the particles the steps erase (catching)."""
+        self._check(self.lib.qp_set_catching(self.h, int(bool(enable)), int(capacity)))
+
+    def get_caught(self) -> dict:
+        """The recorded particles (empties the buffer): species, x y z (cell
+        units), ux uy uz g q chi, and the number dropped for lack of room."""
+        n, dropped = C.c_int64(), C.c_int64()
+        null = [None] * 9
+        self._check(self.lib.qp_get_caught(self.h, 0, None, *null, C.byref(n), C.byref(dropped)))
+        m = max(n.value, 1)
+        sp = np.zeros(m, dtype=np.int32)
+        arrs = {k: np.zeros(m) for k in ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")}
+        self._check(self.lib.qp_get_caught(self.h, m, sp.ctypes.data_as(C.POINTER(C.c_int32)),
+                                           *[_dp(arrs[k]) for k in ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")],
+                                           C.byref(n), C.byref(dropped)))
+        out = {k: v[:n.value] for k, v in arrs.items()}
+        out["species"] = sp[:n.value]
+        out["dropped"] = dropped.value
+        return out
 
     def moving_window(self):
         """Shift the region one cell towards -x (spatial_region::moving_window)."""

@@ -37,6 +37,7 @@ SOURCES = [
     ("qp_adjoint.cu", ["--fmad=false"]),
     ("qp_merge.cu", []),
     ("qp_window.cu", []),
+    ("qp_catch.cu", []),
     ("qp_api.cu", []),
 ]
 HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh", "qp_dual.cuh"]

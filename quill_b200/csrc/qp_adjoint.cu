@@ -441,6 +441,8 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
     pa.cmr = -1.0; pa.dt = P.dt; pa.dx = P.dx; pa.dy = P.dy; pa.dz = P.dz; pa.ext_bz = ext_bz;
     pa.n = 0; pa.sp = 0; pa.kind = KIND_LEPTON; pa.status = s.d_status; pa.diag = s.d_diag;
     pa.track = 0;
+    pa.step = 0;
+    pa.cat = nullptr;
     const int nbc = nblk(nc, 256);
     double* lE = lE6;
     double* lB = lE6 + 3 * nc;

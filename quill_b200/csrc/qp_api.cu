@@ -145,6 +145,7 @@ static void free_state(State* s) {
     cudaFree(s->d_status);
     cudaFree(s->long_list);
     cudaFree(s->window_scratch);
+    catch_release(*s);
     s->window_scratch = nullptr;
     s->long_list = nullptr;
     cudaFree(s->scan_tmp);
@@ -673,9 +674,12 @@ static void fill_diag(State& s, qp_diag* d) {
         const Species& sp = s.sp[i];
         d->n_macro[i] = (int64_t)a.cnt[i];
         // erased energy with each species' sign and scale (as energy_e/p/ph, ienergy)
-        if (sp.cmr == -1) er -= a.sum_erased[i];
-        else if (sp.cmr == 1 || sp.cmr == 0) er += a.sum_erased[i];
-        else if (sp.ion_index >= 0) er += a.sum_erased[i] / sp.cmr;
+        double ers = 0;
+        if (sp.cmr == -1) ers = -a.sum_erased[i];
+        else if (sp.cmr == 1 || sp.cmr == 0) ers = a.sum_erased[i];
+        else if (sp.ion_index >= 0) ers = a.sum_erased[i] / sp.cmr;
+        er += ers;
+        d->energy_erased_sp[i] = ers * bE;
         // compute_N / compute_energy species tests (fout.cpp:62-77, 105-126)
         if (sp.cmr == -1) { Ne -= a.sum_q[i]; ee -= a.sum_e[i]; d->N_qp_e += a.cnt[i]; }
         else if (sp.cmr == 1) { Np += a.sum_q[i]; ep += a.sum_e[i]; d->N_qp_p += a.cnt[i]; }

@@ -57,6 +57,9 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
             if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
         newcell[s] = nc;
+        if (nc < 0 && a.cat)
+            catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, pos[0], pos[1], pos[2], ux, uy, uz, gm, q,
+                           src.chi ? src.chi[p] : 0.0);
         if (nc >= 0) {
             dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
@@ -238,6 +241,9 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
         }
         newcell[s] = nc;
+        if (nc < 0 && a.cat)
+            catch_particle(*a.cat, a.sp, a.step, kill_layer(g, i0, j0, k0) ? 0 : 1, s, pos[0], pos[1], pos[2], ux, uy,
+                           uz, gm, q, chi);
         if (nc >= 0) {
             dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
@@ -393,6 +399,8 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
     a.track = 0;
+    a.step = (uint32_t)s.step_index;
+    a.cat = s.d_cat;
     QedArgs qa = qed_args(s);
     AppendTarget<PStore64> t0, t1;
     if (sp.kind == KIND_PHOTON) {
@@ -447,6 +455,8 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
     a.track = s.track_erased ? 1 : 0;
+    a.step = (uint32_t)s.step_index;
+    a.cat = s.d_cat;
     const int nb = (int)((sp.n + 255) / 256);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;

@@ -95,6 +95,20 @@ struct DiagAccum {
     double sum_erased[QP_MAX_SPECIES];  // sum of (g-1)q (g q for photons) of erased particles
 };
 
+// Erased particles recorded for catching (delete_particle with
+// catching_enabled, low-level.cpp:247-259): one slot per particle claimed with
+// *counter; slots beyond cap are dropped (the counter keeps counting).  key
+// orders the records as the reference deletes them: step, then the
+// p_boundary erasures before the push (phase 0) ahead of the moves out of the
+// region (phase 1), each in traversal order.
+struct CatchBuf {
+    double *x, *y, *z, *ux, *uy, *uz, *g, *q, *chi;
+    int32_t* sp;
+    int64_t* key;
+    int* counter;  // nullptr: catching off
+    int cap;
+};
+
 struct State {
     qp_params prm;
     Grid grid;
@@ -126,6 +140,8 @@ struct State {
     bool timing = false;
     bool track_erased = false;  // qp_set_erased_tracking
     void* window_scratch = nullptr;  // one field plane, for the moving window's shift
+    CatchBuf cat{};                  // catching: erased particles (counter null = off)
+    CatchBuf* d_cat = nullptr;       // its device copy, passed to the push kernels
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double phase_ms[4] = {0, 0, 0, 0};
     int64_t phase_steps = 0;
@@ -150,6 +166,7 @@ int snapshot_take(State& s, State::Snap& sn);
 int snapshot_restore(State& s, State::Snap& sn);
 void snapshot_free(State::Snap& sn);
 State* state_of(qp_handle* h);
+void catch_release(State& s);  // frees the catching buffer (qp_catch.cu)
 
 // Adjoint of qp_step's FP64 FDTD/Boris path (qp_adjoint.cu).
 int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz, double* grad6, double* grad_q,

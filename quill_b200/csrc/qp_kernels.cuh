@@ -288,10 +288,24 @@ __device__ __forceinline__ void warp_count_runs(int32_t* count, int cell) {
     if (warp_run_sum<int, 1>(cell, n)) atomicAdd(count + cell, n[0]);
 }
 
+__device__ __forceinline__ void catch_particle(const CatchBuf& c, int sp, uint32_t step, int phase, int s,
+                                               double x, double y, double z, double ux, double uy, double uz,
+                                               double g, double q, double chi) {
+    const int slot = atomicAdd(c.counter, 1);
+    if (slot >= c.cap) return;
+    c.x[slot] = x; c.y[slot] = y; c.z[slot] = z;
+    c.ux[slot] = ux; c.uy[slot] = uy; c.uz[slot] = uz;
+    c.g[slot] = g; c.q[slot] = q; c.chi[slot] = chi;
+    c.sp[slot] = sp;
+    c.key[slot] = ((int64_t)step << 33) | ((int64_t)phase << 32) | (int64_t)(uint32_t)s;
+}
+
 struct PushArgs {
     double cmr, dt, dx, dy, dz, ext_bz;
     int n, sp, kind;
     int track;  // sum the energy of erased particles into diag->sum_erased
+    uint32_t step;
+    const CatchBuf* cat;  // device copy; nullptr: catching off
     unsigned int* status;
     DiagAccum* diag;
 };

@@ -13,6 +13,8 @@ struct PushArgs32 {
     int track;  // sum the energy of erased particles into diag->sum_erased
     unsigned int* status;
     DiagAccum* diag;
+    uint32_t step;
+    const CatchBuf* cat;  // device copy; nullptr: catching off
 };
 
 __device__ __forceinline__ float wrap_offset(float o, int& shift) {
@@ -67,16 +69,20 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
     }
     deposit_runs(f, g, o, d, q, i0, j0, k0, active, a.status);
     if (s < a.n) {
+        int i1 = i0, j1 = j0, k1 = k0;
         if (live) {
             int si, sj, sk;
             o[0] = wrap_offset(o[0], si);
             o[1] = wrap_offset(o[1], sj);
             o[2] = wrap_offset(o[2], sk);
-            const int i1 = i0 + si, j1 = j0 + sj, k1 = k0 + sk;
+            i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
             const bool moved = si | sj | sk;
             if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
         newcell[s] = nc;
+        if (nc < 0 && a.cat)
+            catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, (double)i1 + (double)o[0], (double)j1 + (double)o[1],
+                           (double)k1 + (double)o[2], ux, uy, uz, gm, q, src.chi ? (double)src.chi[p] : 0.0);
         if (nc >= 0) {
             dst.cell[s] = nc;
             dst.ox[s] = o[0]; dst.oy[s] = o[1]; dst.oz[s] = o[2];
@@ -163,6 +169,8 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
     a.track = s.track_erased ? 1 : 0;
+    a.step = (uint32_t)s.step_index;
+    a.cat = s.d_cat;
     const int nb = (int)((sp.n + 255) / 256);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;

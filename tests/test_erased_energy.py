@@ -101,3 +101,57 @@ def test_tracking_off_reports_zero():
     d = r.step(1)[0]
     r.close()
     assert d.energy_erased == 0.0 and d.n_macro[0] == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_catching_records_every_erased_photon(precision):
+    """Catching (delete_particle with catching_enabled, low-level.cpp:247-259):
+    one record per erased particle, outside the region, carrying the energy
+    the erased-energy sum counted."""
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    from quill_b200.api import Region
+    rng = np.random.default_rng(5)
+    m = 3000
+    u = rng.standard_normal((3, m)) * 5.0
+    parts = _sorted({"x": rng.uniform(1, N[0] - 3, m), "y": rng.uniform(1, N[1] - 3, m),
+                     "z": rng.uniform(1, N[2] - 3, m), "ux": u[0], "uy": u[1], "uz": u[2],
+                     "g": np.sqrt((u * u).sum(0)), "q": rng.uniform(0.01, 0.1, m)})
+    r = Region(*N, DX, DX, DX, DT, species_cmr=(0.0,), precision=precision)
+    r.set_fields(*np.zeros((6,) + N))
+    r.init_boundaries()
+    r.add_particles(0, parts)
+    r.set_erased_tracking(True)
+    r.set_catching(True, capacity=m)
+    d = r.step(24)
+    c = r.get_caught()
+    again = r.get_caught()
+    n_end = r.count(0)
+    r.close()
+    assert c["dropped"] == 0 and again["x"].size == 0
+    assert c["x"].size == m - n_end and np.all(c["species"] == 0)
+    i, j, k = (np.floor(c[a]).astype(int) for a in ("x", "y", "z"))
+    inside = (i > 0) & (i < N[0] - 2) & (j > 0) & (j < N[1] - 2) & (k > 0) & (k < N[2] - 2)
+    assert not inside.any()
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    np.testing.assert_allclose(_b() * np.sum(c["g"] * c["q"]), sum(x.energy_erased for x in d), rtol=tol)
+    np.testing.assert_allclose(sum(x.energy_erased_sp[0] for x in d), sum(x.energy_erased for x in d), rtol=1e-14)
+
+
+def test_catching_capacity_overflow_is_counted():
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    from quill_b200.api import Region
+    m = 300
+    x = np.full(m, 0.5)  # all in the layer p_boundary erases
+    parts = {"x": x, "y": np.linspace(2.1, 12.9, m), "z": np.full(m, 5.5), "ux": np.zeros(m), "uy": np.zeros(m),
+             "uz": np.zeros(m), "g": np.ones(m) * 1.5, "q": -np.ones(m) * 0.01}
+    r = Region(*N, DX, DX, DX, DT)
+    r.set_fields(*np.zeros((6,) + N))
+    r.init_boundaries()
+    r.add_particles(0, _sorted(parts))
+    r.set_catching(True, capacity=100)
+    r.step(1)
+    c = r.get_caught()
+    r.close()
+    assert c["x"].size == 100 and c["dropped"] == m - 100
