@@ -119,6 +119,10 @@ struct Config {
     double mwspeed = 1;            // main.cpp:2944-2947
     bool mwseed = true;            // main.cpp:2948-2950
     double t_add_mw = 0;           // main.cpp:2665-2679, 1/omega (0: last output time)
+    bool catching = false;         // main.cpp:3531-3534
+    double deps_ph = 0;            // MeV, photon spectrum bin (main.cpp:3337-3359)
+    int neps_ph = 0;               // photon spectrum bins (main.cpp:3363-3370)
+    int enthp_p = 0, enthp_ph = 0, enthp_i = 0;  // main.cpp:3374-3385
     std::string pmerging = "off";  // off | ti | nl (main.cpp:3397-3399)
     double crpc = 0;               // critical macro-particles per cell (main.cpp:3400-3401)
 };
@@ -255,6 +259,16 @@ Config parse(const std::vector<Var>& v) {
     if (!find(v, "b_components_for_output").units.empty()) c.b_out = find(v, "b_components_for_output").units;
     if (!find(v, "particles_for_output").units.empty()) c.particles_for_output = find(v, "particles_for_output").units;
     c.enthp = (int)find(v, "enthp").value; if (c.enthp <= 0) c.enthp = 1;
+    c.enthp_p = (int)find(v, "enthp_p").value; if (c.enthp_p == 0) c.enthp_p = c.enthp;
+    c.enthp_ph = (int)find(v, "enthp_ph").value; if (c.enthp_ph == 0) c.enthp_ph = c.enthp;
+    c.enthp_i = (int)find(v, "enthp_i").value; if (c.enthp_i == 0) c.enthp_i = c.enthp;
+    c.catching = find(v, "catching").units == "on";
+    if (find(v, "dump_photons").units == "on") throw std::runtime_error("dump_photons is not part of this build");
+    auto mev = [&](const char* n) { const Var& w = find(v, n); return w.units == "mc^2" ? w.value * 0.511 : w.value; };
+    c.deps_ph = mev("deps_ph");
+    if (c.deps_ph == 0) c.deps_ph = mev("deps");
+    c.neps_ph = (int)find(v, "neps_ph").value;
+    if (c.neps_ph == 0) c.neps_ph = (int)find(v, "neps").value;
     const std::string pr = find(v, "precision").units;
     if (pr == "mixed") c.precision = QP_PREC_MIXED;
     c.seed = (uint64_t)find(v, "seed").value;
@@ -530,6 +544,28 @@ int main() {
         return 1;
     }
 
+    // catching: erased particles recorded on the device, drained every step
+    // into the host list the reference keeps (deleted_particles), cumulative
+    // deleted energies per class (update_energy_deleted)
+    struct Caught { int32_t sp; double q, x, y, z, ux, uy, uz, g, chi; };
+    std::vector<Caught> caught;
+    double e_del = 0, p_del = 0, ph_del = 0;
+    std::vector<double> i_del(icmr.size(), 0.0);
+    int i_particle = 0, i_particle_p = 0, i_particle_ph = 0, i_particle_i = 0;
+    std::ofstream fED;
+    if (r == QP_OK && c.catching) {
+        int64_t total = 0, np = 0;
+        for (int s2 = 0; s2 < n; s2++) { qp_count_particles(h, s2, &np); total += np; }
+        r = qp_set_erased_tracking(h, 1);
+        if (r == QP_OK) r = qp_set_catching(h, 1, std::max<int64_t>(total, 1 << 16));
+        fED.open(c.data_folder + "/energy_deleted");
+    }
+    if (r != QP_OK) {
+        std::cerr << "qp_driver: " << qp_last_error(h) << std::endl;
+        qp_destroy(h);
+        return 1;
+    }
+
     // log in the reference's name/value layout (main.cpp:3611-3785 subset)
     {
         std::ofstream L(c.data_folder + "/log");
@@ -557,6 +593,7 @@ int main() {
         L << "pusher = " << (c.pusher == QP_PUSHER_BORIS ? "boris" : "vay") << "\n";
         L << "precision = " << (c.precision == QP_PREC_MIXED ? "mixed" : "fp64") << "\n";
         L << "pmerging\n" << c.pmerging << "\ncrpc\n" << c.crpc << "\n";
+        L << "catching\n" << (c.catching ? "on" : "off") << "\n";
     }
 
     // particle merging: evaluate_merging_condition (main.cpp:1691-1748) after
@@ -659,6 +696,31 @@ int main() {
             nmw++;
         }
         if (c.mwindow) fMW << ((nmw - 1) * c.dx / 2 / PI) << std::endl;  // write_mwcoordinate
+        if (c.catching) {
+            // drain the device records (deletion order inside a species)
+            int64_t m = 0, dropped = 0;
+            qp_get_caught(h, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          nullptr, &m, &dropped);
+            if (m > 0) {
+                std::vector<int32_t> sp(m);
+                std::vector<double> a[9];
+                for (auto& v2 : a) v2.resize(m);
+                qp_get_caught(h, m, sp.data(), a[0].data(), a[1].data(), a[2].data(), a[3].data(), a[4].data(),
+                              a[5].data(), a[6].data(), a[7].data(), a[8].data(), &m, &dropped);
+                for (int64_t t = 0; t < m; t++)
+                    caught.push_back({sp[t], a[7][t], a[0][t], a[1][t], a[2][t], a[3][t], a[4][t], a[5][t], a[6][t], a[8][t]});
+            }
+            if (dropped > 0) std::cerr << "qp_driver: step " << l << ": " << dropped << " erased particles not recorded" << std::endl;
+            // write_energy_deleted (main.cpp:353-367): cumulative, per class
+            e_del += d.energy_erased_sp[sp_e];
+            if (sp_pos >= 0) p_del += d.energy_erased_sp[sp_pos];
+            if (sp_ph >= 0) ph_del += d.energy_erased_sp[sp_ph];
+            for (size_t f = 0; f < sp_ion.size(); f++)
+                if (sp_ion[f] >= 0) i_del[f] += d.energy_erased_sp[sp_ion[f]];
+            fED << e_del << '\t' << p_del << '\t' << ph_del;
+            for (double v2 : i_del) fED << '\t' << v2;
+            fED << std::endl;
+        }
         evaluate_merging(d);
         if (out_i < sch.it.size() && l == sch.it[out_i]) {
             const std::string sfx = Schedule::suffix(sch.t[out_i]);
@@ -711,6 +773,52 @@ int main() {
                         P << q[t] << '\n' << x[t] * c.dx / 2 / PI << '\n' << y[t] * c.dy / 2 / PI << '\n'
                           << z[t] * c.dz / 2 / PI << '\n' << ux[t] << '\n' << uy[t] << '\n' << uz[t] << '\n'
                           << gg[t] << '\n' << chi[t] << '\n';
+                }
+            }
+            if (c.catching) {
+                // write_deleted_particles (main.cpp:189-345): 9 values per
+                // written particle, the reference's every-n-th counters, and
+                // the deleted photons' spectrum; the list is then cleared
+                // main.cpp:3392-3395
+                const std::string& pf = c.particles_for_output;
+                const bool write_p = pf == "ep" || pf == "epph";
+                const bool write_ph = pf == "eph" || pf == "epph";
+                std::ofstream De(c.data_folder + "/deleted" + sfx), Dp(c.data_folder + "/deleted_p" + sfx),
+                    Dph(c.data_folder + "/deleted_ph" + sfx);
+                std::vector<std::ofstream> Di(icmr.size());
+                for (size_t m = 0; m < icmr.size(); m++) {
+                    char b[32];
+                    snprintf(b, sizeof b, "%g", icmr[m]);
+                    Di[m].open(c.data_folder + "/deleted_" + b + "_" + sfx);
+                }
+                std::vector<double> spec(std::max(c.neps_ph, 0), 0.0);
+                auto put = [&](std::ofstream& o, const Caught& k) {
+                    o << k.q << '\n' << c.dx * k.x / (2 * PI) << '\n' << c.dy * k.y / (2 * PI) << '\n'
+                      << c.dz * k.z / (2 * PI) << '\n' << k.ux << '\n' << k.uy << '\n' << k.uz << '\n' << k.g << '\n'
+                      << k.chi << '\n';
+                };
+                for (const Caught& k : caught) {
+                    if (k.sp == sp_e) {
+                        if (++i_particle > c.enthp) { i_particle = 0; put(De, k); }
+                    } else if (write_p && k.sp == sp_pos) {
+                        if (++i_particle_p > c.enthp_p) { i_particle_ph = 0; put(Dp, k); }
+                    } else if (write_ph && k.sp == sp_ph) {
+                        const int ie = c.deps_ph > 0 ? (int)(k.g * 0.511 / c.deps_ph) : -1;
+                        if (ie > -1 && ie < c.neps_ph) spec[ie] += k.q;
+                        if (++i_particle_ph > c.enthp_ph) { i_particle_ph = 0; put(Dph, k); }
+                    } else {
+                        for (size_t f = 0; f < sp_ion.size(); f++)
+                            if (k.sp == sp_ion[f]) {
+                                if (++i_particle_i > c.enthp_i) { i_particle_i = 0; put(Di[f], k); }
+                                break;
+                            }
+                    }
+                }
+                caught.clear();
+                if (write_ph && c.deps_ph > 0) {
+                    std::ofstream S(c.data_folder + "/spectrum_deleted_ph" + sfx);
+                    const double norm = 1.11485e13 * c.lambda * c.dx * c.dy * c.dz / (8 * PI * PI * PI) / c.deps_ph;
+                    for (double v2 : spec) S << v2 * norm << '\n';
                 }
             }
             out_i++;

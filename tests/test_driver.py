@@ -141,3 +141,34 @@ def test_driver_particle_merging(tmp_path):
     np.testing.assert_allclose(n1[lossless, 0], n0[lossless, 0], rtol=1e-9)
     np.testing.assert_allclose(n1[:, 0], n0[:, 0], rtol=0.05)
     assert ps1 < 0.5 * ps0
+
+
+@pytest.mark.gpu
+def test_driver_catching(tmp_path):
+    """catching = on: energy_deleted gets one row per step with the
+    cumulative energy of the erased particles per class (e, p, ph), and the
+    deleted<t> files carry 9 values per written particle, positioned outside
+    the region (main.cpp:189-367)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200 import build
+    build.build()
+    folder = str(tmp_path / "results")
+    conf = CONF + [("catching", "#", "on")]
+    r = subprocess.run([DRIVER], input=stream(conf, folder), text=True, capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ed = np.loadtxt(os.path.join(folder, "energy_deleted"))
+    assert ed.shape == (17, 3)
+    assert np.all(np.diff(ed[:, 0]) >= 0) and ed[-1, 0] > 0     # electrons leave and are counted
+    log = read_log(os.path.join(folder, "log"))
+    total = 0
+    for t in ("0", "0.25", "0.5"):
+        vals = open(os.path.join(folder, "deleted" + t)).read().split()
+        assert len(vals) % 9 == 0
+        rec = np.array(vals, dtype=float).reshape(-1, 9)
+        total += rec.shape[0]
+        # positions in lambda: outside the inner cells [1, n-3] on some axis
+        cells = np.floor(rec[:, 1:4] / np.array([log["dx"], log["dy"], log["dz"]])).astype(int)
+        n = np.array([log["nx"], log["ny"], log["nz"]])
+        assert np.all(((cells <= 0) | (cells >= n - 2)).any(axis=1))
+    assert total > 0
