@@ -222,6 +222,26 @@ int qp_set_catching(qp_handle* h, int enable, int64_t capacity);
 int qp_get_caught(qp_handle* h, int64_t cap, int32_t* species, double* x, double* y, double* z, double* ux,
                   double* uy, double* uz, double* g, double* q, double* chi, int64_t* n_out, int64_t* dropped);
 
+/* Particle tracks (start_tracking, main.cpp:1516-1612; fout_tracks,
+ * fout.cpp:706-734): enable = 1 gives every particle a track number, 0 =
+ * untracked, carried by the steps; enable = 0 drops them.  Particles that
+ * join later (loads, QED births) are untracked. */
+int qp_set_tracking(qp_handle* h, int enable);
+
+/* Traversal position of the first particle of `species` in each of the n
+ * cells (linear index (i*ny + j)*nz + k), -1 for an empty cell: the head of
+ * the reference's cell list restricted to that species. */
+int qp_first_in_cells(qp_handle* h, int species, int64_t n, const int64_t* cells, int64_t* first);
+
+/* Give the particles at the n traversal positions the track numbers given. */
+int qp_set_track_numbers(qp_handle* h, int species, int64_t n, const int64_t* positions, const int64_t* numbers);
+
+/* The tracked particles of a species in traversal order (at most 65536):
+ * track number, position in cell units, u, g, q, chi (arrays host or
+ * device, nullable; all NULL: count only into *n_out). */
+int qp_get_tracked(qp_handle* h, int species, int64_t cap, int64_t* trn, double* x, double* y, double* z,
+                   double* ux, double* uy, double* uz, double* g, double* q, double* chi, int64_t* n_out);
+
 /* Particle merging modes (the reference's `pmerging` parameter, main.cpp:3397). */
 enum { QP_MERGE_TI = 1, QP_MERGE_NL = 2 };
 

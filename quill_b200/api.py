@@ -111,6 +111,10 @@ def load_library(path: str | None = None):
         "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
         "qp_moving_window": (C.c_int, [VP]),
         "qp_set_catching": (C.c_int, [VP, C.c_int, I64]),
+        "qp_set_tracking": (C.c_int, [VP, C.c_int]),
+        "qp_first_in_cells": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
+        "qp_set_track_numbers": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
+        "qp_get_tracked": (C.c_int, [VP, C.c_int, I64, I64P] + [DP] * 9 + [I64P]),
         "qp_get_caught": (C.c_int, [VP, I64, C.POINTER(C.c_int32)] + [DP] * 9 + [I64P, I64P]),
         "qp_adjoint_energy": (C.c_int, [VP, C.c_int, C.c_int, D, DP, DP, DP]),
     }
@@ -252,6 +256,36 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_tracking(self, enable: bool = True):
+        self._check(self.lib.qp_set_tracking(self.h, int(bool(enable))))
+
+    def first_in_cells(self, species: int, cells) -> np.ndarray:
+        c = np.ascontiguousarray(np.asarray(cells, dtype=np.int64))
+        out = np.zeros(max(c.size, 1), dtype=np.int64)
+        lp = C.POINTER(C.c_int64)
+        self._check(self.lib.qp_first_in_cells(self.h, species, c.size, c.ctypes.data_as(lp), out.ctypes.data_as(lp)))
+        return out[:c.size]
+
+    def set_track_numbers(self, species: int, positions, numbers):
+        p = np.ascontiguousarray(np.asarray(positions, dtype=np.int64))
+        nn = np.ascontiguousarray(np.asarray(numbers, dtype=np.int64))
+        lp = C.POINTER(C.c_int64)
+        self._check(self.lib.qp_set_track_numbers(self.h, species, p.size, p.ctypes.data_as(lp), nn.ctypes.data_as(lp)))
+
+    def get_tracked(self, species: int) -> dict:
+        n = C.c_int64()
+        lp = C.POINTER(C.c_int64)
+        self._check(self.lib.qp_get_tracked(self.h, species, 0, None, *([None] * 9), C.byref(n)))
+        m = max(n.value, 1)
+        trn = np.zeros(m, dtype=np.int64)
+        arrs = {k: np.zeros(m) for k in ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")}
+        self._check(self.lib.qp_get_tracked(self.h, species, m, trn.ctypes.data_as(lp),
+                                            *[_dp(arrs[k]) for k in ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")],
+                                            C.byref(n)))
+        out = {k: v[:n.value] for k, v in arrs.items()}
+        out["trn"] = trn[:n.value]
+        return out
 
     def set_catching(self, enable: bool = True, capacity: int = 1 << 20):
         """Record the particles the steps erase (catching)."""

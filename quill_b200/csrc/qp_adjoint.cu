@@ -443,6 +443,8 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
     pa.track = 0;
     pa.step = 0;
     pa.cat = nullptr;
+    pa.trn_src = nullptr;
+    pa.trn_dst = nullptr;
     const int nbc = nblk(nc, 256);
     double* lE = lE6;
     double* lB = lE6 + 3 * nc;

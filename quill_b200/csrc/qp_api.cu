@@ -60,6 +60,7 @@ static int merge_sorted_slots(State& s, int si, int64_t slot0, int64_t n_new, co
     QP_CUDA_CHECK(s, cudaMalloc(&d_perm, sp.cap * sizeof(int32_t)));
     launch_histogram(s, d_cells, (int)n_new, sp.count);
     exclusive_scan_i32(s, sp.count, nstart, gr.nc);
+    if (sp.trn[sp.cur]) QP_CUDA_CHECK(s, cudaMemsetAsync(sp.trn[sp.cur] + slot0, 0, n_new * sizeof(int32_t), s.stream));
     load_merge(s, si, slot0, nstart, d_perm);
     QP_CUDA_CHECK(s, cudaGetLastError());
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
@@ -106,6 +107,18 @@ static int ensure_capacity(State& s, int si, int64_t need) {
     sp.perm = np;
     if (sp.newcell) cudaFree(sp.newcell);
     QP_CUDA_CHECK(s, cudaMalloc(&sp.newcell, cap * sizeof(int32_t)));
+    if (s.tracking)
+        for (int b = 0; b < 2; b++) {
+            int32_t* t = nullptr;
+            QP_CUDA_CHECK(s, cudaMalloc(&t, cap * sizeof(int32_t)));
+            QP_CUDA_CHECK(s, cudaMemsetAsync(t, 0, cap * sizeof(int32_t), s.stream));
+            if (sp.trn[b]) {
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(t, sp.trn[b], sp.cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream));
+                QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+                cudaFree(sp.trn[b]);
+            }
+            sp.trn[b] = t;
+        }
     sp.cap = cap;
     // the rebin's list of long cells: at most cap / (REBIN_LONG_SEG + 1)
     const int64_t need_long = cap / (REBIN_LONG_SEG + 1) + 2;
@@ -129,6 +142,8 @@ static void free_state(State* s) {
             for (int a = 0; a < 10; a++) cudaFree(sp.buf[b][a]);
         cudaFree(sp.perm);
         cudaFree(sp.newcell);
+        cudaFree(sp.trn[0]);
+        cudaFree(sp.trn[1]);
         cudaFree(sp.cell_start);
         cudaFree(sp.cell_next);
         cudaFree(sp.count);
@@ -162,7 +177,7 @@ int snapshot_take(State& s, State::Snap& sn) {
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
     for (auto& v : sn.arrays)
         for (void* p : v) cudaFree(p);
-    sn.arrays.assign(s.sp.size(), std::vector<void*>(11, nullptr));
+    sn.arrays.assign(s.sp.size(), std::vector<void*>(12, nullptr));
     sn.n.assign(s.sp.size(), 0);
     sn.cap.assign(s.sp.size(), 0);
     sn.slots.assign(s.sp.size(), 0);
@@ -181,6 +196,10 @@ int snapshot_take(State& s, State::Snap& sn) {
             }
             QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][10], cap * 4));
             QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][10], sp.perm, cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+            if (sp.trn[sp.cur]) {
+                QP_CUDA_CHECK(s, cudaMalloc(&sn.arrays[i][11], cap * 4));
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.arrays[i][11], sp.trn[sp.cur], cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+            }
         }
         if (!sn.cell_start[i]) QP_CUDA_CHECK(s, cudaMalloc(&sn.cell_start[i], (nc + 1) * 4));
         QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.cell_start[i], sp.cell_start, (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
@@ -206,6 +225,8 @@ int snapshot_restore(State& s, State::Snap& sn) {
                 QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.buf[sp.cur][a], sn.arrays[i][a], cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
             }
             QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.perm, sn.arrays[i][10], cap * 4, cudaMemcpyDeviceToDevice, s.stream));
+            if (sp.trn[sp.cur] && sn.arrays[i].size() > 11 && sn.arrays[i][11])
+                QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.trn[sp.cur], sn.arrays[i][11], cap * 4, cudaMemcpyDeviceToDevice, s.stream));
         }
         QP_CUDA_CHECK(s, cudaMemcpyAsync(sp.cell_start, sn.cell_start[i], (nc + 1) * 4, cudaMemcpyDeviceToDevice, s.stream));
         sp.n = sn.n[i];
@@ -713,6 +734,9 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
         if (s.prm.qed) {
             int r = qed_prepare(s);
             if (r != QP_OK) return r;
+            for (auto& sp : s.sp)  // particles born in this push: untracked
+                if (sp.trn[1 - sp.cur] && sp.cap > sp.n)
+                    QP_CUDA_CHECK(s, cudaMemsetAsync(sp.trn[1 - sp.cur] + sp.n, 0, (sp.cap - sp.n) * sizeof(int32_t), s.stream));
             for (size_t i = 0; i < s.sp.size(); i++) launch_push_fp64_qed(s, (int)i, external_bz);
             QP_CUDA_CHECK(s, cudaGetLastError());
             for (size_t i = 0; i < s.sp.size(); i++)

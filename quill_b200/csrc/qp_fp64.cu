@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
             dst.g[s] = gm; dst.q[s] = q;
             if (dst.chi) dst.chi[s] = src.chi[p];
+            if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
             dq = q;
             de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
             dc = 1;
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
             dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
             dst.g[s] = gm; dst.q[s] = q; dst.chi[s] = chi;
+            if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
             dq = q;
             de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
             dc = 1;
@@ -401,6 +403,8 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
     a.track = 0;
     a.step = (uint32_t)s.step_index;
     a.cat = s.d_cat;
+    a.trn_src = sp.trn[sp.cur];
+    a.trn_dst = sp.trn[1 - sp.cur];
     QedArgs qa = qed_args(s);
     AppendTarget<PStore64> t0, t1;
     if (sp.kind == KIND_PHOTON) {
@@ -457,6 +461,8 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.track = s.track_erased ? 1 : 0;
     a.step = (uint32_t)s.step_index;
     a.cat = s.d_cat;
+    a.trn_src = sp.trn[sp.cur];
+    a.trn_dst = sp.trn[1 - sp.cur];
     const int nb = (int)((sp.n + 255) / 256);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;

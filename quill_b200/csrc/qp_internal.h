@@ -84,6 +84,7 @@ struct Species {
     int32_t* cell_next = nullptr;  // nc+1, traversal order after the rebin
     int32_t* count = nullptr;      // nc, rebin histogram
     int* d_counter = nullptr;      // device append counter (QED)
+    int32_t* trn[2] = {nullptr, nullptr};  // track numbers (0 = untracked), per buffer; tracking only
 };
 
 struct DiagAccum {
@@ -139,6 +140,7 @@ struct State {
     // diagnostics + J reset)
     bool timing = false;
     bool track_erased = false;  // qp_set_erased_tracking
+    bool tracking = false;      // qp_set_tracking: Species::trn allocated and carried by the pushes
     void* window_scratch = nullptr;  // one field plane, for the moving window's shift
     CatchBuf cat{};                  // catching: erased particles (counter null = off)
     CatchBuf* d_cat = nullptr;       // its device copy, passed to the push kernels

@@ -306,6 +306,8 @@ struct PushArgs {
     int track;  // sum the energy of erased particles into diag->sum_erased
     uint32_t step;
     const CatchBuf* cat;  // device copy; nullptr: catching off
+    const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
+    int32_t* trn_dst;
     unsigned int* status;
     DiagAccum* diag;
 };

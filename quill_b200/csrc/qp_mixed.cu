@@ -15,6 +15,8 @@ struct PushArgs32 {
     DiagAccum* diag;
     uint32_t step;
     const CatchBuf* cat;  // device copy; nullptr: catching off
+    const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
+    int32_t* trn_dst;
 };
 
 __device__ __forceinline__ float wrap_offset(float o, int& shift) {
@@ -89,6 +91,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
             dst.g[s] = gm; dst.q[s] = q;
             if (dst.chi) dst.chi[s] = src.chi[p];
+            if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
             dq = (double)q;
             de = KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
             dc = 1;
@@ -171,6 +174,8 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.track = s.track_erased ? 1 : 0;
     a.step = (uint32_t)s.step_index;
     a.cat = s.d_cat;
+    a.trn_src = sp.trn[sp.cur];
+    a.trn_dst = sp.trn[1 - sp.cur];
     const int nb = (int)((sp.n + 255) / 256);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
