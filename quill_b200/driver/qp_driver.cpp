@@ -120,6 +120,9 @@ struct Config {
     bool mwseed = true;            // main.cpp:2948-2950
     double t_add_mw = 0;           // main.cpp:2665-2679, 1/omega (0: last output time)
     bool catching = false;         // main.cpp:3531-3534
+    int n_tracks = 0;              // main.cpp:3408-3413
+    std::string particles_to_track = "epgi";
+    double tr_start = 0, xtr1 = 0, ytr1 = 0, ztr1 = 0, xtr2 = 0, ytr2 = 0, ztr2 = 0;  // main.cpp:3419-3480
     double deps_ph = 0;            // MeV, photon spectrum bin (main.cpp:3337-3359)
     int neps_ph = 0;               // photon spectrum bins (main.cpp:3363-3370)
     int enthp_p = 0, enthp_ph = 0, enthp_i = 0;  // main.cpp:3374-3385
@@ -263,6 +266,21 @@ Config parse(const std::vector<Var>& v) {
     c.enthp_ph = (int)find(v, "enthp_ph").value; if (c.enthp_ph == 0) c.enthp_ph = c.enthp;
     c.enthp_i = (int)find(v, "enthp_i").value; if (c.enthp_i == 0) c.enthp_i = c.enthp;
     c.catching = find(v, "catching").units == "on";
+    c.n_tracks = (int)find(v, "n_tracks").value;
+    c.particles_to_track = find(v, "particles_to_track").units;
+    if (c.particles_to_track.empty()) c.particles_to_track = "epgi";
+    if (c.particles_to_track == "none") c.particles_to_track = "";
+    if (find(v, "tr_init").units == "volume") throw std::runtime_error("tr_init = volume is not part of this build");
+    {
+        const Var& ts = find(v, "tr_start");
+        double tv = ts.value;
+        if (ts.units == "um") tv = tv * 1e-4 / c.lambda;
+        else if (ts.units == "mm") tv = tv / 10 / c.lambda;
+        else if (ts.units == "cm") tv = tv / c.lambda;
+        c.tr_start = tv * 2 * PI;
+    }
+    c.xtr1 = length(find(v, "xtr1"), c.lambda); c.ytr1 = length(find(v, "ytr1"), c.lambda); c.ztr1 = length(find(v, "ztr1"), c.lambda);
+    c.xtr2 = length(find(v, "xtr2"), c.lambda); c.ytr2 = length(find(v, "ytr2"), c.lambda); c.ztr2 = length(find(v, "ztr2"), c.lambda);
     if (find(v, "dump_photons").units == "on") throw std::runtime_error("dump_photons is not part of this build");
     auto mev = [&](const char* n) { const Var& w = find(v, n); return w.units == "mc^2" ? w.value * 0.511 : w.value; };
     c.deps_ph = mev("deps_ph");
@@ -552,6 +570,7 @@ int main() {
     double e_del = 0, p_del = 0, ph_del = 0;
     std::vector<double> i_del(icmr.size(), 0.0);
     int i_particle = 0, i_particle_p = 0, i_particle_ph = 0, i_particle_i = 0;
+    if (r == QP_OK && c.n_tracks > 0) r = qp_set_tracking(h, 1);
     std::ofstream fED;
     if (r == QP_OK && c.catching) {
         int64_t total = 0, np = 0;
@@ -669,6 +688,79 @@ int main() {
         if (sp_pos >= 0) put(sp_pos, Pm);
         return rr;
     };
+    // start_tracking (main.cpp:1516-1612, the line mode): the first particle
+    // of each requested kind in every distinct cell along the line from
+    // (xtr1, ytr1, ztr1) to (xtr2, ytr2, ztr2) gets the next track number
+    const int nm = 4;  // nx_ich / 2 (main.cpp:2232-2233)
+    bool tracking = false;
+    auto start_tracking = [&]() -> int {
+        if (c.xtr1 < 0 || c.xtr2 < 0 || c.ytr1 < 0 || c.ytr2 < 0 || c.ztr1 < 0 || c.ztr2 < 0 || c.xtr1 >= c.xlength ||
+            c.xtr2 >= c.xlength || c.ytr1 >= c.ylength || c.ytr2 >= c.ylength || c.ztr1 >= c.zlength ||
+            c.ztr2 >= c.zlength) {
+            std::cout << "Error - tracks outside of compulational domain" << std::endl;
+            return QP_OK;
+        }
+        std::vector<int64_t> cells;
+        int x1 = -1, y1 = 0, z1 = 0;
+        for (int i = 0; i < c.n_tracks; i++) {
+            const int x2 = (int)((c.xtr1 + (c.xtr2 - c.xtr1) * i / c.n_tracks) / c.dx);
+            const int y2 = (int)((c.ytr1 + (c.ytr2 - c.ytr1) * i / c.n_tracks) / c.dy);
+            const int z2 = (int)((c.ztr1 + (c.ztr2 - c.ztr1) * i / c.n_tracks) / c.dz);
+            if (x2 != x1 || y2 != y1 || z2 != z1) {
+                x1 = x2; y1 = y2; z1 = z2;
+                cells.push_back(((int64_t)x2 * g.ny + y2) * g.nz + z2);
+            }
+        }
+        // kinds in the reference's order per cell: e, p, g, then every ion population
+        std::vector<int> kinds;
+        if (c.particles_to_track.find('e') != std::string::npos) kinds.push_back(sp_e);
+        if (c.particles_to_track.find('p') != std::string::npos && sp_pos >= 0) kinds.push_back(sp_pos);
+        if (c.particles_to_track.find('g') != std::string::npos && sp_ph >= 0) kinds.push_back(sp_ph);
+        if (c.particles_to_track.find('i') != std::string::npos)
+            for (int f : sp_ion) if (f >= 0) kinds.push_back(f);
+        std::vector<std::vector<int64_t>> first(kinds.size(), std::vector<int64_t>(cells.size()));
+        for (size_t k = 0; k < kinds.size(); k++) {
+            const int rr = qp_first_in_cells(h, kinds[k], (int64_t)cells.size(), cells.data(), first[k].data());
+            if (rr != QP_OK) return rr;
+        }
+        std::vector<std::vector<int64_t>> pos(kinds.size()), num(kinds.size());
+        int64_t trn = 1;
+        for (size_t cc = 0; cc < cells.size(); cc++)
+            for (size_t k = 0; k < kinds.size(); k++)
+                if (first[k][cc] >= 0) { pos[k].push_back(first[k][cc]); num[k].push_back(trn++); }
+        for (size_t k = 0; k < kinds.size(); k++) {
+            const int rr = qp_set_track_numbers(h, kinds[k], (int64_t)pos[k].size(), pos[k].data(), num[k].data());
+            if (rr != QP_OK) return rr;
+        }
+        tracking = true;
+        return QP_OK;
+    };
+    // fout_tracks (fout.cpp:706-734): one file per tracked particle, 9 values per step
+    auto fout_tracks = [&](double a) -> int {
+        for (int s2 = 0; s2 < n; s2++) {
+            int64_t m = 0;
+            int rr = qp_get_tracked(h, s2, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    nullptr, nullptr, &m);
+            if (rr != QP_OK) return rr;
+            if (m == 0) continue;
+            std::vector<int64_t> tn(m);
+            std::vector<double> t9[9];
+            for (auto& v2 : t9) v2.resize(m);
+            rr = qp_get_tracked(h, s2, m, tn.data(), t9[0].data(), t9[1].data(), t9[2].data(), t9[3].data(),
+                                t9[4].data(), t9[5].data(), t9[6].data(), t9[7].data(), t9[8].data(), &m);
+            if (rr != QP_OK) return rr;
+            char cm[32];
+            snprintf(cm, sizeof cm, "%g", p.cmr[s2]);
+            for (int64_t t = 0; t < m; t++) {
+                if (!(t9[0][t] >= nm && t9[0][t] < g.nx - nm)) continue;
+                std::ofstream T(c.data_folder + "/track_" + cm + "_" + std::to_string(tn[t]), std::ios::app);
+                T << t9[7][t] << '\n' << t9[0][t] * c.dx / 2 / PI + a << '\n' << t9[1][t] * c.dy / 2 / PI << '\n'
+                  << t9[2][t] * c.dz / 2 / PI << '\n' << t9[3][t] << '\n' << t9[4][t] << '\n' << t9[5][t] << '\n'
+                  << t9[6][t] << '\n' << t9[8][t] << '\n';
+            }
+        }
+        return QP_OK;
+    };
     for (int l = 0; l <= sch.it.back(); l++) {
         qp_diag d;
         if (merge_now && qp_pmerging(h, c.pmerging == "ti" ? QP_MERGE_TI : QP_MERGE_NL, ppd_sp.data()) != QP_OK) {
@@ -685,6 +777,11 @@ int main() {
         fE << d.energy_f << '\t' << d.energy_e << '\t' << d.energy_p << '\t' << d.energy_ph;  // write_energy
         for (int m = 0; m < d.n_ion; m++) fE << '\t' << d.ienergy[m];
         fE << std::endl;
+        if (c.n_tracks > 0 && tracking && fout_tracks(nmw * c.dx / 2 / PI) != QP_OK) {
+            std::cerr << "qp_driver: tracks at step " << l << ": " << qp_last_error(h) << std::endl;
+            qp_destroy(h);
+            return 1;
+        }
         // check_moving_window, mode on (main.cpp:1953-1959, 2333-2336)
         const bool mw_now = c.mwindow && (l + 1) * c.dt * c.mwspeed > nmw * c.dx;
         if (mw_now) {
@@ -822,6 +919,12 @@ int main() {
                 }
             }
             out_i++;
+        }
+        if (c.n_tracks > 0 && !c.particles_to_track.empty() && l == (int)(c.tr_start / c.dt) &&
+            start_tracking() != QP_OK) {
+            std::cerr << "qp_driver: start_tracking: " << qp_last_error(h) << std::endl;
+            qp_destroy(h);
+            return 1;
         }
         if (mw_now && add_window_particles(l) != QP_OK) {
             std::cerr << "qp_driver: window plasma after step " << l << ": " << qp_last_error(h) << std::endl;

@@ -172,3 +172,30 @@ def test_driver_catching(tmp_path):
         n = np.array([log["nx"], log["ny"], log["nz"]])
         assert np.all(((cells <= 0) | (cells >= n - 2)).any(axis=1))
     assert total > 0
+
+
+@pytest.mark.gpu
+def test_driver_tracks(tmp_path):
+    """n_tracks electrons along a line through the film are tracked from
+    tr_start on (start_tracking, main.cpp:1516-1612); each gets a file
+    track_-1_<n> with 9 values per step while it stays in [nm, nx - nm)
+    (fout_tracks, fout.cpp:706-734)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200 import build
+    build.build()
+    folder = str(tmp_path / "results")
+    conf = CONF + [("n_tracks", "4", "#"), ("particles_to_track", "#", "e"), ("tr_start", "0", "lambda"),
+                   ("xtr1", "1.1", "lambda"), ("ytr1", "0.75", "lambda"), ("ztr1", "0.75", "lambda"),
+                   ("xtr2", "1.4", "lambda"), ("ytr2", "0.75", "lambda"), ("ztr2", "0.75", "lambda")]
+    r = subprocess.run([DRIVER], input=stream(conf, folder), text=True, capture_output=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    files = sorted(f for f in os.listdir(folder) if f.startswith("track_-1_"))
+    assert [f for f in files] == [f"track_-1_{i}" for i in range(1, 5)]
+    for f in files:
+        rec = np.array(open(os.path.join(folder, f)).read().split(), dtype=float).reshape(-1, 9)
+        assert 1 <= rec.shape[0] <= 16
+        assert np.all(rec[:, 0] < 0)                     # electrons
+        assert np.all((rec[:, 1] > 1.0) & (rec[:, 1] < 1.6))  # near the film, in lambda
+        # continuous trajectories: at most half a cell per step in x
+        assert np.all(np.abs(np.diff(rec[:, 1])) <= 0.5 * 0.0625 + 1e-12)
