@@ -242,6 +242,39 @@ int qp_set_track_numbers(qp_handle* h, int species, int64_t n, const int64_t* po
 int qp_get_tracked(qp_handle* h, int species, int64_t cap, int64_t* trn, double* x, double* y, double* z,
                    double* ux, double* uy, double* uz, double* g, double* q, double* chi, int64_t* n_out);
 
+/* x-slabs, for a decomposition into overlapping x-slab regions (the
+ * reference's n_sr > 1 layout and synchronize_regions, main.cpp:1286-1514).
+ *
+ * The diagnostics of qp_step count only the cells with i in [i_lo, i_hi)
+ * (compute_N / compute_energy's n1 and n2, main.cpp:2325-2327); the
+ * default is the whole region. */
+int qp_set_diag_range(qp_handle* h, int i_lo, int i_hi);
+
+/* Copy the 12 field planes (E B J Bbar) of the slab i in [i0, i0 + width)
+ * out / in: 12 blocks of width*ny*nz doubles, k fastest (send_field_slice /
+ * receive_field_slice, main.cpp:1286-1302).  Host or device memory. */
+int qp_get_field_slab(qp_handle* h, int i0, int width, double* out12);
+int qp_set_field_slab(qp_handle* h, int i0, int width, const double* in12);
+
+/* The particles of one species in the slab, in traversal order (cell
+ * lists in order, pack_particle_slice, main.cpp:1330-1394): positions in
+ * cell units of this region, host or device arrays.  All arrays NULL: count
+ * only. */
+int qp_get_particle_slab(qp_handle* h, int species, int i0, int width, int64_t cap, double* x, double* y, double* z,
+                         double* ux, double* uy, double* uz, double* g, double* q, double* chi, int64_t* n_out);
+
+/* Replace the particles of one species in the slab by the n given
+ * (unpack_particle_slice, main.cpp:1360-1423): the slab's cell lists become
+ * exactly these, in the given order inside each cell; a particle's cell
+ * follows from its position.  Host or device arrays. */
+int qp_replace_particle_slab(qp_handle* h, int species, int i0, int width, int64_t n, const double* x,
+                             const double* y, const double* z, const double* ux, const double* uy, const double* uz,
+                             const double* g, const double* q, const double* chi);
+
+/* Quasiparticles per x-layer, all species: counts[nx] (the particle term
+ * of spatial_region::calculate_layer_weights, balancing.cpp:25-40). */
+int qp_layer_counts(qp_handle* h, int64_t* counts);
+
 /* Particle merging modes (the reference's `pmerging` parameter, main.cpp:3397). */
 enum { QP_MERGE_TI = 1, QP_MERGE_NL = 2 };
 

@@ -98,7 +98,19 @@ def _load(kind: str, flavour: str):
         "get_rand": fn("get_rand", _D, C.c_void_p),
         "pmerging": fn("pmerging", None, C.c_void_p, C.c_int, _DP),
         "moving_window": fn("moving_window", None, C.c_void_p),
+        "set_diag_range": fn("set_diag_range", None, C.c_void_p, C.c_int, C.c_int),
+        "get_field_slab": fn("get_field_slab", None, C.c_void_p, C.c_int, C.c_int, _DP),
+        "set_field_slab": fn("set_field_slab", None, C.c_void_p, C.c_int, C.c_int, _DP),
+        "get_particle_slab": fn("get_particle_slab", C.c_long, C.c_void_p, C.c_int, C.c_int, C.c_long, _DP, _LP),
+        "replace_particle_slab": fn("replace_particle_slab", None, C.c_void_p, C.c_int, C.c_int, C.c_long,
+                                    _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP),
+        "layer_counts": fn("layer_counts", None, C.c_void_p, _LP),
     }
+    if kind == "ref":
+        _IP = C.POINTER(C.c_int)
+        api["optimal_partition"] = fn("optimal_partition", None, _DP, C.c_int, C.c_int, C.c_int, _IP)
+        api["normalize_partition"] = fn("normalize_partition", None, _IP, _IP, C.c_int, C.c_int, _IP)
+        api["partition_imbalance"] = fn("partition_imbalance", _D, _DP, C.c_int, _IP, C.c_int, C.c_int)
     _LIBS[key] = api
     return api
 
@@ -246,6 +258,68 @@ class Region:
         v = np.asarray(ppd, dtype=np.float64).reshape(-1)
         p[:min(v.size, p.size)] = v[:p.size]
         self.api["pmerging"](self.h, 1 if mode == "ti" else 2, _dp(p))
+
+
+    # --- x-slabs (the n_sr > 1 exchange, main.cpp:1286-1514) ---------------
+    # The CPU checkers keep all species in one list per cell, so a slab is
+    # exchanged for all species at once (species=None).
+    species_ids = (None,)
+
+    def set_diag_range(self, i_lo: int, i_hi: int):
+        self.api["set_diag_range"](self.h, int(i_lo), int(i_hi))
+
+    def get_field_slab(self, i0: int, width: int) -> np.ndarray:
+        out = np.zeros((12, width) + self.shape[1:])
+        self.api["get_field_slab"](self.h, i0, width, _dp(out))
+        return out
+
+    def set_field_slab(self, i0: int, planes12: np.ndarray):
+        a = np.ascontiguousarray(planes12, dtype=np.float64)
+        self.api["set_field_slab"](self.h, i0, a.size // (12 * self.shape[1] * self.shape[2]), _dp(a))
+
+    def get_particle_slab(self, species, i0: int, width: int) -> dict:
+        n = self.api["get_particle_slab"](self.h, i0, width, 0, None, None)
+        cap = max(n, 1)
+        out = np.zeros((10, cap))
+        self.api["get_particle_slab"](self.h, i0, width, cap, _dp(out), None)
+        return {k: out[i, :n].copy() for i, k in enumerate(PARTICLE_KEYS)}
+
+    def replace_particle_slab(self, species, i0: int, width: int, parts: dict):
+        n = len(parts["x"])
+        arrs = [np.ascontiguousarray(parts[k] if parts.get(k) is not None else np.zeros(n), dtype=np.float64)
+                for k in PARTICLE_KEYS]
+        self.api["replace_particle_slab"](self.h, i0, width, n, *[_dp(a) for a in arrs])
+
+    def layer_counts(self) -> np.ndarray:
+        out = np.zeros(self.shape[0], dtype=np.int64)
+        self.api["layer_counts"](self.h, out.ctypes.data_as(_LP))
+        return out
+
+
+def ref_optimal_partition(weights, regions: int, overlap: int) -> list:
+    """The reference's calculate_optimal_partition (balancing.cpp:54-115)."""
+    api = _load("ref", "parity")
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    out = (C.c_int * regions)()
+    api["optimal_partition"](_dp(w), w.size, regions, overlap, out)
+    return list(out)
+
+
+def ref_normalize_partition(old, new, overlap: int) -> list:
+    """The reference's normalize_new_partition (balancing.cpp:136-175)."""
+    api = _load("ref", "parity")
+    n = len(old)
+    a, b, out = (C.c_int * n)(*old), (C.c_int * n)(*new), (C.c_int * n)()
+    api["normalize_partition"](a, b, n, overlap, out)
+    return list(out)
+
+
+def ref_partition_imbalance(weights, partition, overlap: int) -> float:
+    """The reference's calculate_partition_imbalance (balancing.cpp:132-134)."""
+    api = _load("ref", "parity")
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    p = (C.c_int * len(partition))(*partition)
+    return api["partition_imbalance"](_dp(w), w.size, p, len(partition), overlap)
 
 
 def push(pusher, cmr, state, e, b, dt, kind="port", flavour="parity"):

@@ -46,8 +46,9 @@ struct qor_region {
     /* solver coefficients */
     double fp_ax, fp_ay, fp_az, fp_bx, fp_by, fp_bz;   /* five-point, maxwell.cpp:24-33 */
     double nd_ax, nd_bx, nd_ay, nd_by, nd_az, nd_bz;   /* NDFX, maxwell.cpp:238-249 */
-    /* diagnostics */
+    /* diagnostics: cells with i in [dlo, dhi) (compute_N's n1, n2) */
     double diag[10 + 32];
+    int dlo, dhi;
 };
 
 #define IDX(r, i, j, k) ((((long)(i)) * (r)->ny + (j)) * (r)->nz + (k))
@@ -80,6 +81,7 @@ qor_region* qor_create(int nx, int ny, int nz, double dx, double dy, double dz, 
     qor_region* r = (qor_region*)calloc(1, sizeof(qor_region));
     r->nx = nx; r->ny = ny; r->nz = nz;
     r->nc = (long)nx * ny * nz;
+    r->dlo = 0; r->dhi = nx;
     r->dx = dx; r->dy = dy; r->dz = dz; r->dt = dt;
     /* maxwell.cpp:6-8 */
     r->dtdx = dt / dx; r->dtdy = dt / dy; r->dtdz = dt / dz;
@@ -728,7 +730,7 @@ void qor_padvance(qor_region* r, double external_bz) {
     free(tmp); free(fill); free(dst); free(tot); free(arr); free(newc);
 }
 
-/* fout.cpp:41-138 with n1 = n2 = 0 (one region) */
+/* fout.cpp:41-138: cells with i in [n1, nx - n2) = [dlo, dhi) */
 void qor_compute_diag(qor_region* r, double* d) {
     const double dx = r->dx, dy = r->dy, dz = r->dz, lam = r->lam;
     const double aN = dx * dy * dz * 1.11485e13 * lam / (8 * PI_ * PI_ * PI_);
@@ -738,8 +740,10 @@ void qor_compute_diag(qor_region* r, double* d) {
     int nqe = 0, nqp = 0, nqg = 0;
     int nqi[16] = {0};
     double ie[16] = {0};
+    const long ynz = (long)r->ny * r->nz;
     long p = 0;
-    for (long c = 0; c < r->nc; c++) {
+    while (p < r->n && r->cell[p] < r->dlo * ynz) p++;
+    for (long c = r->dlo * ynz; c < r->dhi * ynz; c++) {
         ef += EX(r)[c] * EX(r)[c] + EY(r)[c] * EY(r)[c] + EZ(r)[c] * EZ(r)[c] + BX(r)[c] * BX(r)[c] + BY(r)[c] * BY(r)[c] + BZ(r)[c] * BZ(r)[c];
         for (; p < r->n && r->cell[p] == c; p++) {
             double cm = r->cmr[p], q = r->q[p], g = r->g[p];
@@ -971,4 +975,67 @@ double qor_mathcal_W(qor_region* r, const double* e, const double* b) {
         return es * es / (4 * PI_) * xi * xi / PI_ * exp(-PI_ * es / xi);
     }
     return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* x-slabs of a region (main.cpp:1286-1423)                                   */
+/* ------------------------------------------------------------------------ */
+void qor_set_diag_range(qor_region* r, int lo, int hi) { r->dlo = lo; r->dhi = hi; }
+
+/* send_field_slice / receive_field_slice: ce, cb, cj, cbe of the cells with
+ * i in [i0, i0 + w); 12 blocks of w*ny*nz */
+void qor_get_field_slab(qor_region* r, int i0, int w, double* out12) {
+    const long m = (long)w * r->ny * r->nz, off = (long)i0 * r->ny * r->nz;
+    for (int a = 0; a < 12; a++) memcpy(out12 + a * m, r->f[a] + off, sizeof(double) * (size_t)m);
+}
+
+void qor_set_field_slab(qor_region* r, int i0, int w, const double* in12) {
+    const long m = (long)w * r->ny * r->nz, off = (long)i0 * r->ny * r->nz;
+    for (int a = 0; a < 12; a++) memcpy(r->f[a] + off, in12 + a * m, sizeof(double) * (size_t)m);
+}
+
+/* traversal range [*a, *b) of the slab's cells */
+static void slab_range(qor_region* r, int i0, int w, long* a, long* b) {
+    const long c0 = (long)i0 * r->ny * r->nz, c1 = (long)(i0 + w) * r->ny * r->nz;
+    long p = 0;
+    while (p < r->n && r->cell[p] < c0) p++;
+    *a = p;
+    while (p < r->n && r->cell[p] < c1) p++;
+    *b = p;
+}
+
+/* pack_particle_slice (main.cpp:1330-1394): the slab's cell lists in order;
+ * out10 as qor_get_particles.  Returns the count. */
+long qor_get_particle_slab(qor_region* r, int i0, int w, long cap, double* out10, long* cell) {
+    long a, b;
+    slab_range(r, i0, w, &a, &b);
+    const double* arrs[10] = {r->x, r->y, r->z, r->ux, r->uy, r->uz, r->g, r->q, r->cmr, r->chi};
+    const long m = b - a < cap ? b - a : cap;
+    if (out10)
+        for (int k = 0; k < 10; k++) memcpy(out10 + k * cap, arrs[k] + a, sizeof(double) * (size_t)m);
+    if (cell) memcpy(cell, r->cell + a, sizeof(long) * (size_t)m);
+    return b - a;
+}
+
+/* unpack_particle_slice (main.cpp:1360-1423): the slab's lists are erased
+ * and rebuilt from the given particles in the given order (cells from the
+ * positions). */
+void qor_replace_particle_slab(qor_region* r, int i0, int w, long n, const double* x, const double* y,
+                               const double* z, const double* ux, const double* uy, const double* uz,
+                               const double* g, const double* q, const double* cmr, const double* chi) {
+    long a, b;
+    slab_range(r, i0, w, &a, &b);
+    double* arrs[10] = {r->x, r->y, r->z, r->ux, r->uy, r->uz, r->g, r->q, r->cmr, r->chi};
+    const long tail = r->n - b;
+    for (int k = 0; k < 10; k++) memmove(arrs[k] + a, arrs[k] + b, sizeof(double) * (size_t)tail);
+    memmove(r->cell + a, r->cell + b, sizeof(long) * (size_t)tail);
+    r->n -= b - a;
+    if (n > 0) qor_add_particles(r, n, x, y, z, ux, uy, uz, g, q, cmr, chi);
+}
+
+/* particles per x-layer (calculate_layer_weights, balancing.cpp:25-40) */
+void qor_layer_counts(qor_region* r, long* counts) {
+    const long ynz = (long)r->ny * r->nz;
+    for (int i = 0; i < r->nx; i++) counts[i] = 0;
+    for (long p = 0; p < r->n; p++) counts[r->cell[p] / ynz]++;
 }

@@ -46,6 +46,16 @@ double qor_get_rand(qor_region* r);
 void qor_moving_window(qor_region* r);
 /* particle merging, mode 1 "ti", 2 "nl"; ppd[3 + n_ion] */
 void qor_pmerging(qor_region* r, int mode, const double* ppd);
+/* x-slabs: diagnostics over i in [lo, hi); field planes and cell lists of
+ * the cells with i in [i0, i0 + w) */
+void qor_set_diag_range(qor_region* r, int lo, int hi);
+void qor_get_field_slab(qor_region* r, int i0, int w, double* out12);
+void qor_set_field_slab(qor_region* r, int i0, int w, const double* in12);
+long qor_get_particle_slab(qor_region* r, int i0, int w, long cap, double* out10, long* cell);
+void qor_replace_particle_slab(qor_region* r, int i0, int w, long n, const double* x, const double* y,
+                               const double* z, const double* ux, const double* uy, const double* uz,
+                               const double* g, const double* q, const double* cmr, const double* chi);
+void qor_layer_counts(qor_region* r, long* counts);
 
 #ifdef __cplusplus
 }

@@ -23,6 +23,7 @@
 #include "main.h"
 #include "pusher.h"
 #include "containers.h"
+#include "balancing.h"
 
 bool catching_enabled = false;
 bool dump_photons = false;
@@ -42,6 +43,7 @@ struct RefRegion {
     double lam;
     int qed;
     std::vector<double> icmr;
+    int n1 = 0, n2 = 0;  // compute_N / compute_energy range [n1, nx - n2)
 };
 
 inline long lin(const RefRegion* r, int i, int j, int k) {
@@ -221,8 +223,8 @@ void qref_step(void* h, int nsteps, double external_bz, double* diag) {
     for (int l = 0; l < nsteps; l++) {
         r->sr.birth_from_vacuum(8 * PI_ * PI_ / (dx * dy * dz) * 2.818e-13 / lambda);
         r->sr.padvance(external_bz);
-        r->sr.compute_N(0, 0, dx * dy * dz * 1.11485e13 * lambda / (8 * PI_ * PI_ * PI_));
-        r->sr.compute_energy(0, 0, 0.5 * dx * dy * dz * 3.691e4 * lambda / 1e7,
+        r->sr.compute_N(r->n1, r->n2, dx * dy * dz * 1.11485e13 * lambda / (8 * PI_ * PI_ * PI_));
+        r->sr.compute_energy(r->n1, r->n2, 0.5 * dx * dy * dz * 3.691e4 * lambda / 1e7,
                              8.2e-14 * dx * dy * dz * 1.11485e13 * lambda / (8 * PI_ * PI_ * PI_));
         r->sr.fadvance();
         if (diag) fill_diag(r, diag + (long)l * qref_diag_len(h));
@@ -243,8 +245,8 @@ void qref_compute_diag(void* h, double* diag) {
     RefRegion* r = (RefRegion*)h;
     const double dx = r->dx, dy = r->dy, dz = r->dz;
     lambda = r->lam;
-    r->sr.compute_N(0, 0, dx * dy * dz * 1.11485e13 * lambda / (8 * PI_ * PI_ * PI_));
-    r->sr.compute_energy(0, 0, 0.5 * dx * dy * dz * 3.691e4 * lambda / 1e7,
+    r->sr.compute_N(r->n1, r->n2, dx * dy * dz * 1.11485e13 * lambda / (8 * PI_ * PI_ * PI_));
+    r->sr.compute_energy(r->n1, r->n2, 0.5 * dx * dy * dz * 3.691e4 * lambda / 1e7,
                          8.2e-14 * dx * dy * dz * 1.11485e13 * lambda / (8 * PI_ * PI_ * PI_));
     fill_diag(r, diag);
 }
@@ -329,6 +331,113 @@ void qref_pmerging(void* h, int mode, const double* ppd) {
     RefRegion* r = (RefRegion*)h;
     std::vector<double> p(ppd, ppd + 3 + r->icmr.size());
     r->sr.pmerging(p.data(), mode == 1 ? "ti" : "nl");
+}
+
+// --- x-slabs (the n_sr > 1 exchange of src/main.cpp:1286-1514) -------------
+
+void qref_set_diag_range(void* h, int lo, int hi) {
+    RefRegion* r = (RefRegion*)h;
+    r->n1 = lo;
+    r->n2 = r->nx - hi;
+}
+
+// ce cb cj cbe of the cells with i in [i0, i0 + w): 12 blocks of w*ny*nz
+void qref_get_field_slab(void* h, int i0, int w, double* out) {
+    RefRegion* r = (RefRegion*)h;
+    const long m = (long)w * r->ny * r->nz;
+    for (int i = i0; i < i0 + w; i++)
+        for (int j = 0; j < r->ny; j++)
+            for (int k = 0; k < r->nz; k++) {
+                const long c = lin(r, i - i0, j, k);
+                const celle& e = r->sr.ce[i][j][k];
+                const cellb& b = r->sr.cb[i][j][k];
+                const cellj& jj = r->sr.cj[i][j][k];
+                const cellbe& be = r->sr.cbe[i][j][k];
+                const double v[12] = {e.ex, e.ey, e.ez, b.bx, b.by, b.bz, jj.jx, jj.jy, jj.jz, be.bex, be.bey, be.bez};
+                for (int a = 0; a < 12; a++) out[a * m + c] = v[a];
+            }
+}
+
+void qref_set_field_slab(void* h, int i0, int w, const double* in) {
+    RefRegion* r = (RefRegion*)h;
+    const long m = (long)w * r->ny * r->nz;
+    for (int i = i0; i < i0 + w; i++)
+        for (int j = 0; j < r->ny; j++)
+            for (int k = 0; k < r->nz; k++) {
+                const long c = lin(r, i - i0, j, k);
+                celle& e = r->sr.ce[i][j][k];
+                cellb& b = r->sr.cb[i][j][k];
+                cellj& jj = r->sr.cj[i][j][k];
+                cellbe& be = r->sr.cbe[i][j][k];
+                e.ex = in[c]; e.ey = in[m + c]; e.ez = in[2 * m + c];
+                b.bx = in[3 * m + c]; b.by = in[4 * m + c]; b.bz = in[5 * m + c];
+                jj.jx = in[6 * m + c]; jj.jy = in[7 * m + c]; jj.jz = in[8 * m + c];
+                be.bex = in[9 * m + c]; be.bey = in[10 * m + c]; be.bez = in[11 * m + c];
+            }
+}
+
+// The slab's cell lists, each from its head (the order pack_cell sends).
+long qref_get_particle_slab(void* h, int i0, int w, long cap, double* out, long* cell) {
+    RefRegion* r = (RefRegion*)h;
+    long n = 0;
+    for (int i = i0; i < i0 + w; i++)
+        for (int j = 0; j < r->ny; j++)
+            for (int k = 0; k < r->nz; k++)
+                for (particle* p = r->sr.cp[i][j][k].pl.head; p; p = p->next) {
+                    if (out && n < cap) {
+#ifndef QUILL_NOQED
+                        const double chi = p->chi;
+#else
+                        const double chi = 0.0;
+#endif
+                        const double v[10] = {p->x, p->y, p->z, p->ux, p->uy, p->uz, p->g, p->q, p->cmr, chi};
+                        for (int a = 0; a < 10; a++) out[a * cap + n] = v[a];
+                    }
+                    if (cell && n < cap) cell[n] = lin(r, i, j, k);
+                    n++;
+                }
+    return n;
+}
+
+// The slab's lists are erased (spatial_region::erase) and rebuilt with the
+// given particles, in the given order inside each cell (as unpack_cell
+// leaves them); a particle's cell follows from its position.
+void qref_replace_particle_slab(void* h, int i0, int w, long n, const double* x, const double* y, const double* z,
+                                const double* ux, const double* uy, const double* uz, const double* g,
+                                const double* q, const double* cmr, const double* chi) {
+    RefRegion* r = (RefRegion*)h;
+    for (int i = i0; i < i0 + w; i++)
+        for (int j = 0; j < r->ny; j++)
+            for (int k = 0; k < r->nz; k++) r->sr.erase(r->sr.cp[i][j][k].pl);
+    qref_add_particles(h, n, x, y, z, ux, uy, uz, g, q, cmr, chi);
+}
+
+// particles per x-layer: spatial_region::calculate_layer_weights with
+// particle weight 1, minus the ny*nz it starts each layer from
+void qref_layer_counts(void* h, long* counts) {
+    RefRegion* r = (RefRegion*)h;
+    std::vector<double> wts = r->sr.calculate_layer_weights(1.0);
+    for (int i = 0; i < r->nx; i++) counts[i] = (long)(wts[i] - (double)r->ny * r->nz);
+}
+
+// calculate_optimal_partition / normalize_new_partition /
+// calculate_partition_imbalance (balancing.cpp:54-175)
+void qref_optimal_partition(const double* weights, int n, int regions, int overlap, int* out) {
+    std::vector<double> wv(weights, weights + n);
+    std::vector<int> p = calculate_optimal_partition(wv, regions, overlap);
+    for (int i = 0; i < regions; i++) out[i] = p[i];
+}
+
+void qref_normalize_partition(const int* old_p, const int* new_p, int regions, int overlap, int* out) {
+    std::vector<int> a(old_p, old_p + regions), b(new_p, new_p + regions);
+    std::vector<int> p = normalize_new_partition(a, b, overlap);
+    for (int i = 0; i < regions; i++) out[i] = p[i];
+}
+
+double qref_partition_imbalance(const double* weights, int n, const int* part, int regions, int overlap) {
+    std::vector<double> wv(weights, weights + n);
+    std::vector<int> p(part, part + regions);
+    return calculate_partition_imbalance(wv, p, overlap);
 }
 
 }  // extern "C"

@@ -112,6 +112,12 @@ def load_library(path: str | None = None):
         "qp_moving_window": (C.c_int, [VP]),
         "qp_set_catching": (C.c_int, [VP, C.c_int, I64]),
         "qp_set_tracking": (C.c_int, [VP, C.c_int]),
+        "qp_set_diag_range": (C.c_int, [VP, C.c_int, C.c_int]),
+        "qp_get_field_slab": (C.c_int, [VP, C.c_int, C.c_int, DP]),
+        "qp_set_field_slab": (C.c_int, [VP, C.c_int, C.c_int, DP]),
+        "qp_get_particle_slab": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, I64] + [DP] * 9 + [I64P]),
+        "qp_replace_particle_slab": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, I64] + [DP] * 9),
+        "qp_layer_counts": (C.c_int, [VP, I64P]),
         "qp_first_in_cells": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
         "qp_set_track_numbers": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
         "qp_get_tracked": (C.c_int, [VP, C.c_int, I64, I64P] + [DP] * 9 + [I64P]),
@@ -127,7 +133,15 @@ def load_library(path: str | None = None):
 
 
 def _dp(a):
-    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+    """double* of a numpy array, or of a torch tensor (host or device: the
+    entry points that take it copy with cudaMemcpyDefault)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        if str(a.dtype) != "torch.float64" or not a.is_contiguous():
+            raise ValueError("tensor arguments must be contiguous float64")
+        return C.cast(C.c_void_p(a.data_ptr()), C.POINTER(C.c_double))
+    return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
 PARTICLE_KEYS = ("x", "y", "z", "ux", "uy", "uz", "g", "q", "chi")
@@ -256,6 +270,66 @@ class Region:
 
     def set_stream(self, stream_ptr: int):
         self._check(self.lib.qp_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_diag_range(self, i_lo: int, i_hi: int):
+        self._check(self.lib.qp_set_diag_range(self.h, int(i_lo), int(i_hi)))
+
+    def layer_counts(self) -> np.ndarray:
+        """Quasiparticles per x-layer, all species."""
+        out = np.zeros(self.shape[0], dtype=np.int64)
+        self._check(self.lib.qp_layer_counts(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        return out
+
+    # one slab exchange per species
+    @property
+    def species_ids(self):
+        return tuple(range(self.n_species))
+
+    def get_field_slab(self, i0: int, width: int, out=None):
+        """E B J Bbar of the cells with i in [i0, i0 + width): (12, width,
+        ny, nz) float64, into `out` (numpy or torch, host or device) if given."""
+        if out is None:
+            out = np.zeros((12, width, self.shape[1], self.shape[2]))
+        self._check(self.lib.qp_get_field_slab(self.h, i0, width, _dp(out)))
+        return out
+
+    def set_field_slab(self, i0: int, planes12):
+        a = planes12 if hasattr(planes12, "data_ptr") else np.ascontiguousarray(planes12, dtype=np.float64)
+        width = a.numel() // (12 * self.shape[1] * self.shape[2]) if hasattr(a, "numel") else \
+            a.size // (12 * self.shape[1] * self.shape[2])
+        self._check(self.lib.qp_set_field_slab(self.h, i0, width, _dp(a)))
+
+    def get_particle_slab(self, species: int, i0: int, width: int, device=None) -> dict:
+        """The species' particles in the slab, in traversal order: numpy
+        arrays, or torch float64 tensors on `device` if given."""
+        n = C.c_int64()
+        self._check(self.lib.qp_get_particle_slab(self.h, species, i0, width, 0, *([None] * 9), C.byref(n)))
+        m = n.value
+        if device is not None:
+            import torch
+            buf = torch.empty((len(PARTICLE_KEYS), max(m, 1)), dtype=torch.float64, device=device)
+        else:
+            buf = np.zeros((len(PARTICLE_KEYS), max(m, 1)))
+        if m:
+            rows = [buf[i] for i in range(len(PARTICLE_KEYS))]
+            self._check(self.lib.qp_get_particle_slab(self.h, species, i0, width, m, *[_dp(r) for r in rows],
+                                                      C.byref(n)))
+        return {k: buf[i, :m] for i, k in enumerate(PARTICLE_KEYS)}
+
+    def replace_particle_slab(self, species: int, i0: int, width: int, parts: dict):
+        """Replace the species' particles in the slab by `parts` (numpy or
+        torch arrays; in the given order inside each cell)."""
+        n = len(parts["x"])
+        arrs = []
+        for k in PARTICLE_KEYS:
+            a = parts.get(k)
+            if a is None:
+                arrs.append(None)
+            elif hasattr(a, "data_ptr"):
+                arrs.append(a.contiguous())
+            else:
+                arrs.append(np.ascontiguousarray(a, dtype=np.float64))
+        self._check(self.lib.qp_replace_particle_slab(self.h, species, i0, width, n, *[_dp(a) for a in arrs]))
 
     def set_tracking(self, enable: bool = True):
         self._check(self.lib.qp_set_tracking(self.h, int(bool(enable))))

@@ -39,6 +39,7 @@ SOURCES = [
     ("qp_window.cu", []),
     ("qp_catch.cu", []),
     ("qp_track.cu", []),
+    ("qp_slab.cu", []),
     ("qp_api.cu", []),
 ]
 HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh", "qp_dual.cuh"]

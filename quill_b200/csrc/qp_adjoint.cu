@@ -390,6 +390,7 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
         return QP_ERR_CONFIG;
     }
     if (!s.boundaries_done) { s.err = "qp_init_boundaries has not run"; return QP_ERR_STATE; }
+    if (s.diag_lo != 0 || s.diag_hi != s.grid.nx) { s.err = "the adjoint needs the full diagnostic range"; return QP_ERR_STATE; }
     if (nsteps < 1 || every < 1) { s.err = "nsteps and the checkpoint interval must be positive"; return QP_ERR_ARG; }
     const Grid g = s.grid;
     const size_t nc = (size_t)g.nc;
@@ -445,6 +446,7 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
     pa.cat = nullptr;
     pa.trn_src = nullptr;
     pa.trn_dst = nullptr;
+    pa.dlo = 0; pa.dhi = s.grid.nx;
     const int nbc = nblk(nc, 256);
     double* lE = lE6;
     double* lB = lE6 + 3 * nc;

@@ -324,6 +324,8 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.grid.nynz = p.ny * p.nz;
     s.grid.nc = p.nx * p.ny * p.nz;
     s.grid.div_nz.init((uint32_t)p.nz);
+    s.diag_lo = 0;
+    s.diag_hi = p.nx;
     s.grid.div_nynz.init((uint32_t)(p.ny * p.nz));
     s.field_elem = s.fp64 ? 8 : 4;
     if (const char* mb = getenv("QP_PUSH_MINBLOCKS")) s.push_minblocks = atoi(mb) == 2 ? 2 : (atoi(mb) == 4 ? 4 : 3);

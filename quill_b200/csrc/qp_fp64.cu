@@ -21,6 +21,7 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
     int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+    bool nc_owned = true;
     bool live = false, active = false;
     double pos[3] = {0.0, 0.0, 0.0}, d[3] = {0.0, 0.0, 0.0};
     double ux = 0.0, uy = 0.0, uz = 0.0, gm = 1.0, q = 0.0;
@@ -57,7 +58,10 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
             if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
         newcell[s] = nc;
-        if (nc < 0 && a.cat)
+        // an erasure in the exchange area of an x-slab is not one of the whole box (delete_particle,
+        // low-level.cpp:247-259): only erasures inside [dlo, dhi) are caught and counted
+        if (nc < 0 && !((int)pos[0] >= a.dlo && (int)pos[0] < a.dhi)) nc_owned = false;
+        if (nc < 0 && a.cat && nc_owned)
             catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, pos[0], pos[1], pos[2], ux, uy, uz, gm, q,
                            src.chi ? src.chi[p] : 0.0);
         if (nc >= 0) {
@@ -66,15 +70,18 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
             dst.g[s] = gm; dst.q[s] = q;
             if (dst.chi) dst.chi[s] = src.chi[p];
             if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
-            dq = q;
-            de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
-            dc = 1;
+            const int ii = (int)pos[0];
+            if (ii >= a.dlo && ii < a.dhi) {
+                dq = q;
+                de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
+                dc = 1;
+            }
         }
     }
     warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
     if (a.track) {  // uniform: energy of the particles erased in this push
-        const double er = (s < a.n && nc < 0) ? (KIND == KIND_PHOTON ? gm * q : (gm - 1) * q) : 0.0;
+        const double er = (s < a.n && nc < 0 && nc_owned) ? (KIND == KIND_PHOTON ? gm * q : (gm - 1) * q) : 0.0;
         block_sum(&a.diag->sum_erased[a.sp], er);
     }
 }
@@ -82,7 +89,8 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
 // Particle born during a push: appended to the target species' output
 // buffer with its final cell, erased (not stored) if the cell is not inside
 // (place(p), plist.cpp:22-39).  Counted in the target's diagnostics.
-__device__ __forceinline__ void append64(const AppendTarget<PStore64>& t, const Grid& g, const double pos[3],
+__device__ __forceinline__ void append64(const AppendTarget<PStore64>& t, const Grid& g, int dlo, int dhi,
+                                         const double pos[3],
                                          const double u[3], double gm, double q, double chi, bool photon,
                                          unsigned int* status, DiagAccum* diag) {
     const int i = (int)pos[0], j = (int)pos[1], k = (int)pos[2];
@@ -97,6 +105,7 @@ __device__ __forceinline__ void append64(const AppendTarget<PStore64>& t, const 
     t.dst.g[slot] = gm; t.dst.q[slot] = q;
     if (t.dst.chi) t.dst.chi[slot] = chi;
     t.newcell[slot] = cidx(g, i, j, k);
+    if (i < dlo || i >= dhi) return;
     atomicAdd(&diag->sum_q[t.sp], q);
     atomicAdd(&diag->sum_e[t.sp], photon ? gm * q : (gm - 1) * q);
     atomicAdd(&diag->cnt[t.sp], 1ull);
@@ -129,7 +138,7 @@ __device__ __forceinline__ void born_lepton64(const Fields<double>& f, const Gri
     d[0] = d[0] / a.dx; d[1] = d[1] / a.dy; d[2] = d[2] / a.dz;
     double pos[3] = {pos0[0], pos0[1], pos0[2]};
     jdeposition(f, g, pos, d, q, 0, 0, 0, a.status);
-    append64(t, g, pos, u, gm, q, chi, false, a.status, a.diag);
+    append64(t, g, a.dlo, a.dhi, pos, u, gm, q, chi, false, a.status, a.diag);
 }
 
 // advance.cpp:90-387 with QED on.  Photons: chi, pair creation with
@@ -211,7 +220,7 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
                     ph[0] += a3 * uph[0] / a.dx;
                     ph[1] += a3 * uph[1] / a.dy;
                     ph[2] += a3 * uph[2] / a.dz;
-                    append64(t0, g, ph, uph, gph, fabs(q), r * chi, true, a.status, a.diag);
+                    append64(t0, g, a.dlo, a.dhi, ph, uph, gph, fabs(q), r * chi, true, a.status, a.diag);
                     // recoil (advance.cpp:308-322)
                     chi = (1 - r) * chi;
                     gm = (1 - r) * g_prev;
@@ -242,7 +251,7 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
         }
         newcell[s] = nc;
-        if (nc < 0 && a.cat)
+        if (nc < 0 && a.cat && (int)pos[0] >= a.dlo && (int)pos[0] < a.dhi)
             catch_particle(*a.cat, a.sp, a.step, kill_layer(g, i0, j0, k0) ? 0 : 1, s, pos[0], pos[1], pos[2], ux, uy,
                            uz, gm, q, chi);
         if (nc >= 0) {
@@ -250,9 +259,12 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
             dst.g[s] = gm; dst.q[s] = q; dst.chi[s] = chi;
             if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
-            dq = q;
-            de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
-            dc = 1;
+            const int ii = (int)pos[0];
+            if (ii >= a.dlo && ii < a.dhi) {
+                dq = q;
+                de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
+                dc = 1;
+            }
         }
     }
     block_diag(a.diag, a.sp, dq, de, dc);
@@ -405,6 +417,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
     a.cat = s.d_cat;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
+    a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     QedArgs qa = qed_args(s);
     AppendTarget<PStore64> t0, t1;
     if (sp.kind == KIND_PHOTON) {
@@ -463,6 +476,7 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.cat = s.d_cat;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
+    a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     const int nb = (int)((sp.n + 255) / 256);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
@@ -482,7 +496,10 @@ void launch_push_fp64(State& s, int si, double external_bz) {
 
 void launch_field_energy_fp64(State& s) {
     Fields<double> f = fields64(s);
-    k_field_energy<double><<<148 * 4, 256, 0, s.stream>>>(f, s.grid.nc, s.d_diag);
+    const size_t off = (size_t)s.diag_lo * s.grid.nynz;
+    Fields<double> fo = f;
+    fo.ex += off; fo.ey += off; fo.ez += off; fo.bx += off; fo.by += off; fo.bz += off;
+    k_field_energy<double><<<148 * 4, 256, 0, s.stream>>>(fo, (s.diag_hi - s.diag_lo) * s.grid.nynz, s.d_diag);
     s.launches++;
 }
 

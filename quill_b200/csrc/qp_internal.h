@@ -141,6 +141,7 @@ struct State {
     bool timing = false;
     bool track_erased = false;  // qp_set_erased_tracking
     bool tracking = false;      // qp_set_tracking: Species::trn allocated and carried by the pushes
+    int diag_lo = 0, diag_hi = 0;  // qp_set_diag_range: cells i in [diag_lo, diag_hi) counted (create: [0, nx))
     void* window_scratch = nullptr;  // one field plane, for the moving window's shift
     CatchBuf cat{};                  // catching: erased particles (counter null = off)
     CatchBuf* d_cat = nullptr;       // its device copy, passed to the push kernels

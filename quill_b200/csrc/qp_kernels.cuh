@@ -308,6 +308,7 @@ struct PushArgs {
     const CatchBuf* cat;  // device copy; nullptr: catching off
     const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
     int32_t* trn_dst;
+    int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)
     unsigned int* status;
     DiagAccum* diag;
 };

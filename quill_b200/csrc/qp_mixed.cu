@@ -17,6 +17,7 @@ struct PushArgs32 {
     const CatchBuf* cat;  // device copy; nullptr: catching off
     const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
     int32_t* trn_dst;
+    int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)
 };
 
 __device__ __forceinline__ float wrap_offset(float o, int& shift) {
@@ -40,6 +41,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
     int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+    bool nc_owned = true;
     bool live = false, active = false;
     float o[3] = {0.f, 0.f, 0.f}, d[3] = {0.f, 0.f, 0.f};
     float ux = 0.f, uy = 0.f, uz = 0.f, gm = 1.f, q = 0.f;
@@ -82,7 +84,10 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
             if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
         newcell[s] = nc;
-        if (nc < 0 && a.cat)
+        // an erasure in the exchange area of an x-slab is not one of the whole box (delete_particle,
+        // low-level.cpp:247-259): only erasures inside [dlo, dhi) are caught and counted
+        if (nc < 0 && !(i1 >= a.dlo && i1 < a.dhi)) nc_owned = false;
+        if (nc < 0 && a.cat && nc_owned)
             catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, (double)i1 + (double)o[0], (double)j1 + (double)o[1],
                            (double)k1 + (double)o[2], ux, uy, uz, gm, q, src.chi ? (double)src.chi[p] : 0.0);
         if (nc >= 0) {
@@ -92,15 +97,17 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
             dst.g[s] = gm; dst.q[s] = q;
             if (dst.chi) dst.chi[s] = src.chi[p];
             if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
-            dq = (double)q;
-            de = KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
-            dc = 1;
+            if (i1 >= a.dlo && i1 < a.dhi) {
+                dq = (double)q;
+                de = KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
+                dc = 1;
+            }
         }
     }
     warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
     if (a.track) {  // uniform: energy of the particles erased in this push
-        const double er = (s < a.n && nc < 0)
+        const double er = (s < a.n && nc < 0 && nc_owned)
                               ? (KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q)
                               : 0.0;
         block_sum(&a.diag->sum_erased[a.sp], er);
@@ -176,6 +183,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.cat = s.d_cat;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
+    a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     const int nb = (int)((sp.n + 255) / 256);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
@@ -193,7 +201,10 @@ void launch_push_mixed(State& s, int si, double external_bz) {
 
 void launch_field_energy_mixed(State& s) {
     Fields<float> f = fields32(s);
-    k_field_energy<float><<<148 * 4, 256, 0, s.stream>>>(f, s.grid.nc, s.d_diag);
+    const size_t off = (size_t)s.diag_lo * s.grid.nynz;
+    Fields<float> fo = f;
+    fo.ex += off; fo.ey += off; fo.ez += off; fo.bx += off; fo.by += off; fo.bz += off;
+    k_field_energy<float><<<148 * 4, 256, 0, s.stream>>>(fo, (s.diag_hi - s.diag_lo) * s.grid.nynz, s.d_diag);
     s.launches++;
 }
 

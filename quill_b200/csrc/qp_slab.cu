@@ -1,0 +1,237 @@
+// Slabs of a region along x, for a decomposition into x-slab regions that
+// overlap (the reference's n_sr > 1 layout, main.cpp:1286-1514): the
+// neighbours' owned cells overwrite a region's halo cells after every step,
+// fields (ce, cb, cj, cbe) and particle lists alike, and the diagnostics of
+// each region count its owned cells only (compute_N / compute_energy with
+// n1, n2 = nm at inner faces, main.cpp:2325-2327).
+//
+// An x-slab [i0, i0 + w) is contiguous in every field plane (k fastest) and
+// in the traversal order of every species ([cell_start[i0 ny nz],
+// cell_start[(i0 + w) ny nz])).
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "qp_internal.h"
+
+namespace qp {
+
+namespace {
+
+// Particles at traversal positions [a, a + m): state in doubles, absolute
+// cell-unit positions (x y z ux uy uz g q chi), into out9 (9 planes of m).
+template <bool FP64>
+__global__ void k_slab_gather(Grid g, const int32_t* __restrict__ perm, int a, int m, void* const* arrays,
+                              double* __restrict__ out9) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const int p = perm[a + t];
+    double v[9];
+    if (FP64) {
+        for (int c = 0; c < 8; c++) v[c] = ((const double*)arrays[c])[p];
+        v[8] = arrays[8] ? ((const double*)arrays[8])[p] : 0.0;
+    } else {
+        const int cell = ((const int32_t*)arrays[0])[p];
+        const int i = cell / g.nynz, j = (cell / g.nz) % g.ny, k = cell % g.nz;
+        v[0] = i + (double)((const float*)arrays[1])[p];
+        v[1] = j + (double)((const float*)arrays[2])[p];
+        v[2] = k + (double)((const float*)arrays[3])[p];
+        for (int c = 3; c < 8; c++) v[c] = (double)((const float*)arrays[c + 1])[p];
+        v[8] = arrays[9] ? (double)((const float*)arrays[9])[p] : 0.0;
+    }
+    for (int c = 0; c < 9; c++) out9[(size_t)c * m + t] = v[c];
+}
+
+// Drop the traversal range [a, b): the permutation closes the gap, cells of
+// the slab [c0, c1) become empty and later cells move back by b - a.
+__global__ void k_slab_drop_perm(const int32_t* __restrict__ perm, int a, int b, int n, int32_t* __restrict__ out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    if (s < a) out[s] = perm[s];
+    else if (s >= b) out[s - (b - a)] = perm[s];
+}
+
+__global__ void k_slab_drop_starts(int nc, int c0, int c1, int a, int b, const int32_t* __restrict__ cs,
+                                   int32_t* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > nc) return;
+    out[c] = c <= c0 ? cs[c] : (c < c1 ? a : cs[c] - (b - a));
+}
+
+}  // namespace
+
+}  // namespace qp
+
+#define QP_SLAB_ENTRY(h, s)                                                           \
+    if (!(h)) return QP_ERR_ARG;                                                      \
+    qp::State& s = *qp::state_of(h);                                                  \
+    {                                                                                 \
+        const cudaError_t e0 = cudaSetDevice(s.prm.device);                           \
+        if (e0 != cudaSuccess) { s.err = cudaGetErrorString(e0); return QP_ERR_CUDA; } \
+    }
+
+static bool slab_ok(qp::State& s, int i0, int width) {
+    if (i0 < 0 || width < 0 || i0 + width > s.grid.nx) {
+        s.err = "slab outside the region";
+        return false;
+    }
+    return true;
+}
+
+extern "C" int qp_set_diag_range(qp_handle* h, int i_lo, int i_hi) {
+    QP_SLAB_ENTRY(h, s);
+    if (i_lo < 0 || i_hi > s.grid.nx || i_lo > i_hi) { s.err = "diagnostic range outside the region"; return QP_ERR_ARG; }
+    s.diag_lo = i_lo;
+    s.diag_hi = i_hi;
+    return QP_OK;
+}
+
+// 12 planes of the slab <-> 12 consecutive blocks of m doubles (device).
+template <typename T>
+__global__ void k_field_slab_out(const T* __restrict__ fields, size_t nc, size_t off, size_t m, double* __restrict__ out) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 12 * m) return;
+    const size_t a = t / m, c = t - a * m;
+    out[t] = (double)fields[a * nc + off + c];
+}
+
+template <typename T>
+__global__ void k_field_slab_in(const double* __restrict__ in, size_t nc, size_t off, size_t m, T* __restrict__ fields) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 12 * m) return;
+    const size_t a = t / m, c = t - a * m;
+    fields[a * nc + off + c] = (T)in[t];
+}
+
+// Host or device buffers (the copies are cudaMemcpyDefault).
+extern "C" int qp_get_field_slab(qp_handle* h, int i0, int width, double* out12) {
+    QP_SLAB_ENTRY(h, s);
+    if (!slab_ok(s, i0, width) || !out12) return QP_ERR_ARG;
+    const size_t nc = (size_t)s.grid.nc, m = (size_t)width * s.grid.nynz, off = (size_t)i0 * s.grid.nynz;
+    if (m == 0) return QP_OK;
+    double* d = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&d, 12 * m * sizeof(double)));
+    const unsigned nb = (unsigned)((12 * m + 255) / 256);
+    if (s.fp64) k_field_slab_out<double><<<nb, 256, 0, s.stream>>>((const double*)s.fields, nc, off, m, d);
+    else k_field_slab_out<float><<<nb, 256, 0, s.stream>>>((const float*)s.fields, nc, off, m, d);
+    s.launches++;
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) cudaMemcpyAsync(out12, d, 12 * m * sizeof(double), cudaMemcpyDefault, s.stream);
+    const cudaError_t e2 = cudaStreamSynchronize(s.stream);
+    cudaFree(d);
+    if (e != cudaSuccess || e2 != cudaSuccess) { s.err = cudaGetErrorString(e != cudaSuccess ? e : e2); return QP_ERR_CUDA; }
+    return QP_OK;
+}
+
+extern "C" int qp_set_field_slab(qp_handle* h, int i0, int width, const double* in12) {
+    QP_SLAB_ENTRY(h, s);
+    if (!slab_ok(s, i0, width) || !in12) return QP_ERR_ARG;
+    const size_t nc = (size_t)s.grid.nc, m = (size_t)width * s.grid.nynz, off = (size_t)i0 * s.grid.nynz;
+    if (m == 0) return QP_OK;
+    double* d = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&d, 12 * m * sizeof(double)));
+    cudaError_t e = cudaMemcpyAsync(d, in12, 12 * m * sizeof(double), cudaMemcpyDefault, s.stream);
+    const unsigned nb = (unsigned)((12 * m + 255) / 256);
+    if (e == cudaSuccess) {
+        if (s.fp64) k_field_slab_in<double><<<nb, 256, 0, s.stream>>>(d, nc, off, m, (double*)s.fields);
+        else k_field_slab_in<float><<<nb, 256, 0, s.stream>>>(d, nc, off, m, (float*)s.fields);
+        s.launches++;
+        e = cudaGetLastError();
+    }
+    const cudaError_t e2 = cudaStreamSynchronize(s.stream);
+    cudaFree(d);
+    if (e != cudaSuccess || e2 != cudaSuccess) { s.err = cudaGetErrorString(e != cudaSuccess ? e : e2); return QP_ERR_CUDA; }
+    return QP_OK;
+}
+
+// Quasiparticles per x-layer, all species (the particle part of
+// spatial_region::calculate_layer_weights, balancing.cpp:25-40).
+extern "C" int qp_layer_counts(qp_handle* h, int64_t* counts) {
+    QP_SLAB_ENTRY(h, s);
+    if (!counts) return QP_ERR_ARG;
+    const int nx = s.grid.nx, ynz = s.grid.nynz;
+    for (int i = 0; i < nx; i++) counts[i] = 0;
+    std::vector<int32_t> cs(nx + 1);
+    for (auto& sp : s.sp) {
+        if (sp.n == 0) continue;
+        QP_CUDA_CHECK(s, cudaMemcpy2DAsync(cs.data(), sizeof(int32_t), sp.cell_start, (size_t)ynz * sizeof(int32_t),
+                                           sizeof(int32_t), nx + 1, cudaMemcpyDeviceToHost, s.stream));
+        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        for (int i = 0; i < nx; i++) counts[i] += cs[i + 1] - cs[i];
+    }
+    return QP_OK;
+}
+
+// traversal range of the slab's cells
+static int slab_range(qp::State& s, qp::Species& sp, int i0, int width, int32_t& a, int32_t& b) {
+    const size_t c0 = (size_t)i0 * s.grid.nynz, c1 = (size_t)(i0 + width) * s.grid.nynz;
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(&a, sp.cell_start + c0, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream));
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(&b, sp.cell_start + c1, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream));
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    return QP_OK;
+}
+
+extern "C" int qp_get_particle_slab(qp_handle* h, int species, int i0, int width, int64_t cap, double* x, double* y,
+                                    double* z, double* ux, double* uy, double* uz, double* g, double* q, double* chi,
+                                    int64_t* n_out) {
+    QP_SLAB_ENTRY(h, s);
+    if (!n_out || species < 0 || species >= (int)s.sp.size() || !slab_ok(s, i0, width)) return QP_ERR_ARG;
+    qp::Species& sp = s.sp[species];
+    *n_out = 0;
+    if (sp.n == 0 || width == 0) return QP_OK;
+    int32_t a = 0, b = 0;
+    int r = slab_range(s, sp, i0, width, a, b);
+    if (r != QP_OK) return r;
+    const int m = b - a;
+    *n_out = m;
+    double* out[9] = {x, y, z, ux, uy, uz, g, q, chi};
+    bool any = false;
+    for (double* p : out) any = any || p;
+    if (!any || m == 0) return QP_OK;
+    if (cap < m) { s.err = "output arrays shorter than the slab's particles"; return QP_ERR_ARG; }
+    double* d9 = nullptr;
+    void** darr = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&d9, (size_t)9 * m * sizeof(double)));
+    QP_CUDA_CHECK(s, cudaMalloc(&darr, 10 * sizeof(void*)));
+    QP_CUDA_CHECK(s, cudaMemcpy(darr, sp.buf[sp.cur], 10 * sizeof(void*), cudaMemcpyHostToDevice));
+    if (s.fp64)
+        qp::k_slab_gather<true><<<(m + 255) / 256, 256, 0, s.stream>>>(s.grid, sp.perm, a, m, darr, d9);
+    else
+        qp::k_slab_gather<false><<<(m + 255) / 256, 256, 0, s.stream>>>(s.grid, sp.perm, a, m, darr, d9);
+    s.launches++;
+    QP_CUDA_CHECK(s, cudaGetLastError());
+    for (int c = 0; c < 9; c++)
+        if (out[c]) QP_CUDA_CHECK(s, cudaMemcpyAsync(out[c], d9 + (size_t)c * m, m * sizeof(double), cudaMemcpyDefault, s.stream));
+    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+    cudaFree(d9);
+    cudaFree(darr);
+    return QP_OK;
+}
+
+extern "C" int qp_replace_particle_slab(qp_handle* h, int species, int i0, int width, int64_t n, const double* x,
+                                        const double* y, const double* z, const double* ux, const double* uy,
+                                        const double* uz, const double* g, const double* q, const double* chi) {
+    QP_SLAB_ENTRY(h, s);
+    if (species < 0 || species >= (int)s.sp.size() || !slab_ok(s, i0, width) || n < 0) return QP_ERR_ARG;
+    qp::Species& sp = s.sp[species];
+    if (sp.n > 0 && width > 0) {
+        int32_t a = 0, b = 0;
+        int r = slab_range(s, sp, i0, width, a, b);
+        if (r != QP_OK) return r;
+        if (b > a) {
+            const int nn = (int)sp.n;
+            const int c0 = i0 * s.grid.nynz, c1 = (i0 + width) * s.grid.nynz;
+            qp::k_slab_drop_perm<<<(nn + 255) / 256, 256, 0, s.stream>>>(sp.perm, a, b, nn, sp.newcell);
+            qp::k_slab_drop_starts<<<(s.grid.nc + 1 + 255) / 256, 256, 0, s.stream>>>(s.grid.nc, c0, c1, a, b,
+                                                                                      sp.cell_start, sp.cell_next);
+            s.launches += 2;
+            QP_CUDA_CHECK(s, cudaGetLastError());
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            std::swap(sp.perm, sp.newcell);
+            std::swap(sp.cell_start, sp.cell_next);
+            sp.n = nn - (b - a);
+        }
+    }
+    if (n == 0) return QP_OK;
+    return qp_load_particles(h, species, n, x, y, z, ux, uy, uz, g, q, chi);
+}
