@@ -42,7 +42,8 @@ SOURCES = [
     ("qp_slab.cu", []),
     ("qp_api.cu", []),
 ]
-HEADERS = ["qp_internal.h", "qp_physics.cuh", "qp_fields.cuh", "qp_kernels.cuh", "qp_dual.cuh"]
+# every header of csrc/ is a dependency of every translation unit
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -308,7 +308,6 @@ int qp_create(const qp_params* prm, qp_handle** out) {
             has_ph |= p.cmr[i] == 0;
         }
         if (!(has_e && has_p && has_ph)) return bad("QED needs species with cmr -1, +1 and 0");
-        if (p.precision != QP_PREC_FP64) return bad("QED runs in FP64 precision");
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -644,7 +643,8 @@ static int qed_prepare(State& s) {
     if ((r = ensure_capacity(s, p, std::max(s.sp[p].slots, s.sp[p].n + nph) + 1024)) != QP_OK) return r;
     for (auto& sp : s.sp)
         if (sp.d_counter) QP_CUDA_CHECK(s, cudaMemsetAsync(sp.d_counter, 0, sizeof(int), s.stream));
-    launch_vacuum_fp64(s);
+    if (s.fp64) launch_vacuum_fp64(s);
+    else launch_vacuum_mixed(s);
     int kv[2] = {0, 0};
     QP_CUDA_CHECK(s, cudaMemcpyAsync(&kv[0], s.sp[e].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     QP_CUDA_CHECK(s, cudaMemcpyAsync(&kv[1], s.sp[p].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
@@ -660,13 +660,17 @@ static int qed_prepare(State& s) {
         std::vector<int64_t> order(k);
         for (int64_t t = 0; t < k; t++) order[t] = t;
         std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cells[a] < cells[b]; });
-        std::vector<double> tmp(k), srt(k);
-        for (int a = 0; a < 9; a++) {
+        // every array of the store (8-byte elements in FP64, 4-byte cell
+        // and offsets in mixed precision) in cell order
+        const int na = n_arrays(s);
+        const size_t el = arr_elem(s, 0);
+        std::vector<char> tmp(k * el), srt(k * el);
+        for (int a = 0; a < na; a++) {
             if (!sp.buf[sp.cur][a]) continue;
-            double* d = (double*)sp.buf[sp.cur][a] + slot0;
-            QP_CUDA_CHECK(s, cudaMemcpy(tmp.data(), d, k * 8, cudaMemcpyDeviceToHost));
-            for (int64_t t = 0; t < k; t++) srt[t] = tmp[order[t]];
-            QP_CUDA_CHECK(s, cudaMemcpy(d, srt.data(), k * 8, cudaMemcpyHostToDevice));
+            char* d = (char*)sp.buf[sp.cur][a] + slot0 * el;
+            QP_CUDA_CHECK(s, cudaMemcpy(tmp.data(), d, k * el, cudaMemcpyDeviceToHost));
+            for (int64_t t = 0; t < k; t++) memcpy(&srt[t * el], &tmp[order[t] * el], el);
+            QP_CUDA_CHECK(s, cudaMemcpy(d, srt.data(), k * el, cudaMemcpyHostToDevice));
         }
         std::vector<int32_t> sc(k);
         for (int64_t t = 0; t < k; t++) sc[t] = cells[order[t]];
@@ -677,6 +681,11 @@ static int qed_prepare(State& s) {
         cudaFree(dc);
         if (r != QP_OK) return r;
     }
+    // room for a photon from every lepton, the vacuum pairs included
+    nlep = 0;
+    for (auto& sp : s.sp)
+        if (sp.kind == KIND_LEPTON) nlep += sp.n;
+    if ((r = ensure_capacity(s, ph, std::max(s.sp[ph].slots, nph + nlep) + 1)) != QP_OK) return r;
     for (auto& sp : s.sp)
         if (sp.d_counter) QP_CUDA_CHECK(s, cudaMemsetAsync(sp.d_counter, 0, sizeof(int), s.stream));
     return QP_OK;
@@ -739,7 +748,10 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
             for (auto& sp : s.sp)  // particles born in this push: untracked
                 if (sp.trn[1 - sp.cur] && sp.cap > sp.n)
                     QP_CUDA_CHECK(s, cudaMemsetAsync(sp.trn[1 - sp.cur] + sp.n, 0, (sp.cap - sp.n) * sizeof(int32_t), s.stream));
-            for (size_t i = 0; i < s.sp.size(); i++) launch_push_fp64_qed(s, (int)i, external_bz);
+            for (size_t i = 0; i < s.sp.size(); i++) {
+                if (s.fp64) launch_push_fp64_qed(s, (int)i, external_bz);
+                else launch_push_mixed_qed(s, (int)i, external_bz);
+            }
             QP_CUDA_CHECK(s, cudaGetLastError());
             for (size_t i = 0; i < s.sp.size(); i++)
                 QP_CUDA_CHECK(s, cudaMemcpyAsync(&born[i], s.sp[i].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));

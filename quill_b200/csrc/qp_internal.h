@@ -187,6 +187,8 @@ void launch_field_energy_fp64(State& s);
 void launch_fields_mixed(State& s, int phase);
 void launch_init_boundaries_mixed(State& s);
 void launch_push_mixed(State& s, int species, double external_bz);
+int launch_push_mixed_qed(State& s, int species, double external_bz);
+int launch_vacuum_mixed(State& s);
 void launch_field_energy_mixed(State& s);
 
 // ---- rebin and scans (qp_rebin.cu) ----

@@ -55,6 +55,14 @@ enum RngTag : uint32_t { RNG_PUSH = 0x51u, RNG_VACUUM = 0x56u };
 // Rates, mc.cpp:26-116.  e_s is the Sauter field in m c omega / e.
 // ----------------------------------------------------------------------------
 
+// The radicand of chi is >= 0 in exact arithmetic (|u| <= g); for a photon
+// moving along E its two terms cancel, and FP32 rounding (with approximate
+// division and square root) can leave it slightly negative, which would make
+// chi, then every rate, NaN.  The FP32 path clamps it; the FP64 path keeps
+// the reference's arithmetic as it is.
+__device__ __forceinline__ double chi_radicand(double a2) { return a2; }
+__device__ __forceinline__ float chi_radicand(float a2) { return fmaxf(a2, 0.f); }
+
 // chi = sqrt(|g E + u x B|^2 - (u.E)^2) / e_s  (mc.cpp:26-38)
 template <typename T>
 __device__ __forceinline__ T qed_chi(const T e[3], const T b[3], const T u[3], T g, T e_s) {
@@ -66,7 +74,7 @@ __device__ __forceinline__ T qed_chi(const T e[3], const T b[3], const T u[3], T
     a2 += a1 * a1;
     a1 = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
     a2 -= a1 * a1;
-    return sqrt(a2) / e_s;
+    return sqrt(chi_radicand(a2)) / e_s;
 }
 
 // Photon emission spectrum (mc.cpp:40-74) with the Airy-function fits

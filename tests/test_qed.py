@@ -97,19 +97,31 @@ def _ref_stats(seed):
     return _stats_from(sel(-1.0), sel(1.0), sel(0.0))
 
 
+_REF_CACHE = {}
+
+
+def _ref_stats_cached(seed):
+    if seed not in _REF_CACHE:
+        _REF_CACHE[seed] = _ref_stats(seed)
+    return _REF_CACHE[seed]
+
+
 @pytest.mark.gpu
-def test_qed_step_statistics_vs_reference():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_qed_step_statistics_vs_reference(precision):
+    """Emission, recoil and pair creation; the mixed path evaluates the
+    rates in FP32 against the same per-step rejection."""
     if not gpu_available():
         pytest.skip("no CUDA device")
     if KIND != "ref":
         pytest.skip("whole-step QED statistics need the compiled reference")
     from quill_b200.api import Region
-    ref = [_ref_stats(1 + s) for s in range(16)]
+    ref = [_ref_stats_cached(1 + s) for s in range(16)]
     gpu = []
     for seed in range(16):
         fields, e, ph = _emission_case(0)
         g = Region(N, N, N, DX, DX, DX, DT, species_cmr=(-1.0, 1.0, 0.0), solver="fdtd", pusher="boris",
-                   qed=True, seed=1000 + seed)
+                   qed=True, seed=1000 + seed, precision=precision)
         g.set_fields(*[fields[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
         g.init_boundaries()
         g.add_particles(0, _sort(e))
@@ -124,3 +136,54 @@ def test_qed_step_statistics_vs_reference():
         sig = np.sqrt(r.var(ddof=1) / r.size + v.var(ddof=1) / v.size)
         assert abs(v.mean() - r.mean()) <= 3 * sig + 1e-12 * abs(r.mean()), (key, v.mean(), r.mean(), sig)
         assert r.mean() > 0
+
+
+# Schwinger pairs from a uniform Ex of 0.073 e_s: about 1e-2 pairs per
+# interior cell and step, so a 16^3 box makes about 17 per step
+E_VAC = 0.073 * 1e-4 / 2.4263086e-10
+
+
+def _vacuum_counts_ref(seed, steps=2):
+    reg = O.Region(N, N, N, DX, DX, DX, DT, solver=0, pusher=1, qed=True, seed=seed, kind=KIND)
+    z = np.zeros((N, N, N))
+    reg.set_fields(np.full((N, N, N), E_VAC), z, z, z, z, z)
+    reg.init_boundaries()
+    out = []
+    for _ in range(steps):
+        reg.step(1)
+        p = reg.get_particles()
+        out.append(((p["cmr"] == -1).sum(), (p["cmr"] == 1).sum()))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_vacuum_pairs_vs_reference(precision):
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    if KIND != "ref":
+        pytest.skip("vacuum pair statistics need the compiled reference")
+    from quill_b200.api import Region
+    ref = np.array([_vacuum_counts_ref(1 + s) for s in range(16)], dtype=float)
+    gpu = []
+    z = np.zeros((N, N, N))
+    for seed in range(16):
+        g = Region(N, N, N, DX, DX, DX, DT, species_cmr=(-1.0, 1.0, 0.0), solver="fdtd", pusher="boris",
+                   qed=True, seed=500 + seed, precision=precision)
+        g.set_fields(np.full((N, N, N), E_VAC), z, z, z, z, z)
+        g.init_boundaries()
+        rows = []
+        for _ in range(2):
+            g.step(1)
+            rows.append((g.count(0), g.count(1)))
+        gpu.append(rows)
+        g.close()
+    gpu = np.array(gpu, dtype=float)
+    assert ref[:, 0, 0].mean() > 3
+    # step 1: the pairs themselves; step 2 adds the cascade they start (the
+    # field accelerates them to chi ~ 1e2 within a step)
+    for step in range(2):
+        for sp in range(2):
+            r, v = ref[:, step, sp], gpu[:, step, sp]
+            sig = np.sqrt(r.var(ddof=1) / r.size + v.var(ddof=1) / v.size)
+            assert abs(v.mean() - r.mean()) <= 3 * sig, (step, sp, v.mean(), r.mean(), sig)
