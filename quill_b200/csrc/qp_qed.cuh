@@ -61,7 +61,7 @@ enum RngTag : uint32_t { RNG_PUSH = 0x51u, RNG_VACUUM = 0x56u };
 // chi, then every rate, NaN.  The FP32 path clamps it; the FP64 path keeps
 // the reference's arithmetic as it is.
 __device__ __forceinline__ double chi_radicand(double a2) { return a2; }
-__device__ __forceinline__ float chi_radicand(float a2) { return fmaxf(a2, 0.f); }
+__device__ __forceinline__ float chi_radicand(float a2) { return a2 > 0.f ? a2 : 0.f; }
 
 // chi = sqrt(|g E + u x B|^2 - (u.E)^2) / e_s  (mc.cpp:26-38)
 template <typename T>
