@@ -40,55 +40,74 @@ __global__ void __launch_bounds__(256) k_rebin_count(const int32_t* __restrict__
     warp_count_runs(count, t < total ? __ldg(newcell + t) : -1);
 }
 
+// Positions per warp of the scatter: REBIN_CHUNKS chunks of 32, whose loads
+// and claims are issued together (the kernel waits on memory and atomics).
+constexpr int REBIN_CHUNKS = 2;
+
 __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict__ newcell, int total,
                                                        const int32_t* __restrict__ cs,
                                                        const int32_t* __restrict__ start,
                                                        int32_t* __restrict__ cursor, int32_t* __restrict__ perm,
                                                        unsigned int* status) {
     const unsigned full = 0xffffffffu;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const int wb = t - lane;  // first position of this warp
-    const int key = t < total ? __ldg(newcell + t) : -1;
-    int e = 0, end = 0;
-    bool stay = false;
-    if (key >= 0) {
+    const int w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * REBIN_CHUNKS;
+    int key[REBIN_CHUNKS], e[REBIN_CHUNKS], end[REBIN_CHUNKS], b[REBIN_CHUNKS];
+#pragma unroll
+    for (int h = 0; h < REBIN_CHUNKS; h++) {
+        const int t = w0 + 32 * h + lane;
+        key[h] = t < total ? __ldg(newcell + t) : -1;
+    }
+#pragma unroll
+    for (int h = 0; h < REBIN_CHUNKS; h++) {
         // independent loads, issued together: the old range of the new cell
         // and the end of its new range (used if the particle stayed)
-        const int b = __ldg(cs + key);
-        e = __ldg(cs + key + 1);
-        end = __ldg(start + key + 1);
-        stay = t >= b && t < e;
+        b[h] = 0; e[h] = 0; end[h] = 0;
+        if (key[h] >= 0) {
+            b[h] = __ldg(cs + key[h]);
+            e[h] = __ldg(cs + key[h] + 1);
+            end[h] = __ldg(start + key[h] + 1);
+        }
     }
-    // stayers: slot counted from the end of the new range
-    const unsigned smask = __ballot_sync(full, stay);
-    if (stay) {
-        const int hi = min(e - wb, 32);
-        const unsigned below_hi = hi >= 32 ? full : ((1u << hi) - 1u);
-        const unsigned above_me = lane == 31 ? 0u : ~((2u << lane) - 1u);
-        int after = __popc(smask & below_hi & above_me);
-        for (int u = wb + 32; u < e; u++) after += __ldg(newcell + u) == key;
-        const int pos = end - 1 - after;
-        if (pos >= 0 && pos < total) perm[pos] = t;
-        else atomicOr(status, (unsigned int)ST_BOUNDS);  // counts inconsistent with the cells
+    int base[REBIN_CHUNKS], hl[REBIN_CHUNKS], akey[REBIN_CHUNKS];
+#pragma unroll
+    for (int h = 0; h < REBIN_CHUNKS; h++) {
+        const int wb = w0 + 32 * h;  // first position of this chunk
+        const int t = wb + lane;
+        const bool stay = key[h] >= 0 && t >= b[h] && t < e[h];
+        // stayers: slot counted from the end of the new range
+        const unsigned smask = __ballot_sync(full, stay);
+        if (stay) {
+            const int hi = min(e[h] - wb, 32);
+            const unsigned below_hi = hi >= 32 ? full : ((1u << hi) - 1u);
+            const unsigned above_me = lane == 31 ? 0u : ~((2u << lane) - 1u);
+            int after = __popc(smask & below_hi & above_me);
+            for (int u = wb + 32; u < e[h]; u++) after += __ldg(newcell + u) == key[h];
+            const int pos = end[h] - 1 - after;
+            if (pos >= 0 && pos < total) perm[pos] = t;
+            else atomicOr(status, (unsigned int)ST_BOUNDS);  // counts inconsistent with the cells
+        }
+        // arrivals and born: claimed from the front, one atomic per run
+        akey[h] = (key[h] >= 0 && !stay) ? key[h] : -1;
+        const int ukey = akey[h] >= 0 ? akey[h] : -1 - lane;
+        const int prev = __shfl_up_sync(full, ukey, 1);
+        const bool head = lane == 0 || prev != ukey;
+        const unsigned heads = __ballot_sync(full, head);
+        const unsigned upto = lane == 31 ? full : ((2u << lane) - 1u);
+        hl[h] = 31 - __clz(heads & upto);                 // first lane of this lane's run
+        const unsigned above = heads & ~upto;
+        const int next = above ? __ffs(above) - 1 : 32;   // first lane of the next run
+        base[h] = 0;
+        if (head && akey[h] >= 0) base[h] = atomicAdd(cursor + akey[h], next - lane);
     }
-    // arrivals and born: claimed from the front, one atomic per run
-    const int akey = (key >= 0 && !stay) ? key : -1;
-    const int ukey = akey >= 0 ? akey : -1 - lane;
-    const int prev = __shfl_up_sync(full, ukey, 1);
-    const bool head = lane == 0 || prev != ukey;
-    const unsigned heads = __ballot_sync(full, head);
-    const unsigned upto = lane == 31 ? full : ((2u << lane) - 1u);
-    const int hl = 31 - __clz(heads & upto);          // first lane of this lane's run
-    const unsigned above = heads & ~upto;
-    const int next = above ? __ffs(above) - 1 : 32;   // first lane of the next run
-    int base = 0;
-    if (head && akey >= 0) base = atomicAdd(cursor + akey, next - lane);
-    base = __shfl_sync(full, base, hl);
-    if (akey >= 0) {
-        const int pos = base + lane - hl;
-        if (pos >= 0 && pos < total) perm[pos] = t;
-        else atomicOr(status, (unsigned int)ST_BOUNDS);
+#pragma unroll
+    for (int h = 0; h < REBIN_CHUNKS; h++) {
+        const int bb = __shfl_sync(full, base[h], hl[h]);
+        if (akey[h] >= 0) {
+            const int pos = bb + lane - hl[h];
+            if (pos >= 0 && pos < total) perm[pos] = w0 + 32 * h + lane;
+            else atomicOr(status, (unsigned int)ST_BOUNDS);
+        }
     }
 }
 
@@ -101,25 +120,56 @@ __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* _
                                                      int32_t* __restrict__ perm, int32_t* __restrict__ long_list,
                                                      int* __restrict__ n_long, unsigned int* status) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    const int b = __ldg(start + c), f = __ldg(cursor + c) - b;
-    if (f < 2) return;
-    if (b < 0 || b + f > total) {  // counts inconsistent with the cells
-        atomicOr(status, (unsigned int)ST_BOUNDS);
-        return;
+    int b = 0, f = 0;
+    if (c < ncell) {
+        b = __ldg(start + c);
+        f = __ldg(cursor + c) - b;
+        if (f >= 2 && (b < 0 || b + f > total)) {  // counts inconsistent with the cells
+            atomicOr(status, (unsigned int)ST_BOUNDS);
+            f = 0;
+        }
+        if (f > REBIN_LONG_SEG) {
+            long_list[atomicAdd(n_long, 1)] = c;
+            f = 0;
+        }
     }
-    if (f > REBIN_LONG_SEG) {
-        long_list[atomicAdd(n_long, 1)] = c;
-        return;
-    }
-    if (f == 2) {
-        const int x0 = perm[b], x1 = perm[b + 1];
-        if (front_key(x0, n_old) > front_key(x1, n_old)) {
-            perm[b] = x1;
-            perm[b + 1] = x0;
+    // the sorting network is chosen for the longest part in the warp (most
+    // parts are 0 or 1 long, a few 2, rarely more than 4)
+    const int fmax = __reduce_max_sync(0xffffffffu, f);
+    if (fmax < 2) return;
+    if (fmax == 2) {
+        if (f == 2) {
+            const int x0 = perm[b], x1 = perm[b + 1];
+            if (front_key(x0, n_old) > front_key(x1, n_old)) {
+                perm[b] = x1;
+                perm[b + 1] = x0;
+            }
         }
         return;
     }
+    if (fmax <= 4) {
+        if (f < 2) return;
+        int x[4];
+        long long k[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            x[u] = u < f ? perm[b + u] : 0;
+            k[u] = u < f ? front_key(x[u], n_old) : 0x7fffffffffffffffll;
+        }
+        // optimal 4-input network: (0,1) (2,3) (0,2) (1,3) (1,2)
+        auto cx = [&](int i, int j) {
+            if (k[i] > k[j]) {
+                const long long tk = k[i]; k[i] = k[j]; k[j] = tk;
+                const int tx = x[i]; x[i] = x[j]; x[j] = tx;
+            }
+        };
+        cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (u < f) perm[b + u] = x[u];
+        return;
+    }
+    if (f < 2) return;
     if (f <= 8) {
         // in registers: all loads issued together, odd-even transposition sort
         int x[8];
@@ -289,8 +339,9 @@ int64_t rebin(State& s, int si, int64_t born, bool counted) {
     // cell_next = exclusive scan of the counts; count becomes the claim cursor
     exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc, sp.count);
     if (total > 0) {
-        k_rebin_scatter<<<(total + 255) / 256, 256, 0, s.stream>>>(sp.newcell, total, sp.cell_start, sp.cell_next,
-                                                                   sp.count, sp.perm, s.d_status);
+        const int per_block = 256 * REBIN_CHUNKS;
+        k_rebin_scatter<<<(total + per_block - 1) / per_block, 256, 0, s.stream>>>(
+            sp.newcell, total, sp.cell_start, sp.cell_next, sp.count, sp.perm, s.d_status);
         s.launches++;
     }
     int* n_long = (int*)s.long_list;  // entry 0: count; cells from entry 1
