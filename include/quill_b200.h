@@ -271,6 +271,11 @@ int qp_replace_particle_slab(qp_handle* h, int species, int i0, int width, int64
                              const double* y, const double* z, const double* ux, const double* uy, const double* uz,
                              const double* g, const double* q, const double* chi);
 
+/* max over the cells with i in [i0, i1) of Ex^2+Ey^2+Ez^2+Bx^2+By^2+Bz^2
+ * (spatial_region::get_max_w, low-level.cpp:512-532), for the moving
+ * window's AUTO mode (check_moving_window, main.cpp:1961-1975). */
+int qp_max_w(qp_handle* h, int i0, int i1, double* out);
+
 /* Quasiparticles per x-layer, all species: counts[nx] (the particle term
  * of spatial_region::calculate_layer_weights, balancing.cpp:25-40). */
 int qp_layer_counts(qp_handle* h, int64_t* counts);

@@ -118,6 +118,7 @@ def load_library(path: str | None = None):
         "qp_get_particle_slab": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, I64] + [DP] * 9 + [I64P]),
         "qp_replace_particle_slab": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, I64] + [DP] * 9),
         "qp_layer_counts": (C.c_int, [VP, I64P]),
+        "qp_max_w": (C.c_int, [VP, C.c_int, C.c_int, DP]),
         "qp_first_in_cells": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
         "qp_set_track_numbers": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
         "qp_get_tracked": (C.c_int, [VP, C.c_int, I64, I64P] + [DP] * 9 + [I64P]),
@@ -279,6 +280,12 @@ class Region:
         out = np.zeros(self.shape[0], dtype=np.int64)
         self._check(self.lib.qp_layer_counts(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))))
         return out
+
+    def max_w(self, i0: int = 0, i1: int | None = None) -> float:
+        """max of E^2 + B^2 over the cells with i in [i0, i1)."""
+        v = C.c_double()
+        self._check(self.lib.qp_max_w(self.h, i0, self.shape[0] if i1 is None else i1, C.byref(v)))
+        return v.value
 
     # one slab exchange per species
     @property

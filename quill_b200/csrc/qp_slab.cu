@@ -9,10 +9,17 @@
 // in the traversal order of every species ([cell_start[i0 ny nz],
 // cell_start[(i0 + w) ny nz])).
 #include <algorithm>
+#include <cstring>
 #include <string>
 #include <vector>
 
 #include "qp_internal.h"
+
+static double __longlong_as_double_host(unsigned long long v) {
+    double d;
+    memcpy(&d, &v, sizeof d);
+    return d;
+}
 
 namespace qp {
 
@@ -141,6 +148,57 @@ extern "C" int qp_set_field_slab(qp_handle* h, int i0, int width, const double* 
     const cudaError_t e2 = cudaStreamSynchronize(s.stream);
     cudaFree(d);
     if (e != cudaSuccess || e2 != cudaSuccess) { s.err = cudaGetErrorString(e != cudaSuccess ? e : e2); return QP_ERR_CUDA; }
+    return QP_OK;
+}
+
+// max of E^2 + B^2 over the cells with i in [i0, i1) (get_max_w,
+// low-level.cpp:512-532).  w >= 0, so the bit patterns of the doubles order
+// like the values and an unsigned 64-bit atomicMax takes the maximum.
+template <typename T>
+__global__ void k_max_w(qp::Fields<T> f, size_t off, size_t m, unsigned long long* out) {
+    double w = 0.0;
+    for (size_t x = off + (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < off + m; x += (size_t)gridDim.x * blockDim.x) {
+        const double ex = f.ex[x], ey = f.ey[x], ez = f.ez[x], bx = f.bx[x], by = f.by[x], bz = f.bz[x];
+        const double v = ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
+        if (v > w) w = v;
+    }
+    for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_down_sync(0xffffffffu, w, o));
+    if ((threadIdx.x & 31) == 0 && w > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(w));
+}
+
+extern "C" int qp_max_w(qp_handle* h, int i0, int i1, double* out) {
+    QP_SLAB_ENTRY(h, s);
+    if (!out) return QP_ERR_ARG;
+    i0 = std::max(i0, 0);
+    i1 = std::min(i1, s.grid.nx);
+    *out = 0.0;
+    if (i1 <= i0) return QP_OK;
+    const size_t off = (size_t)i0 * s.grid.nynz, m = (size_t)(i1 - i0) * s.grid.nynz;
+    unsigned long long* d = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&d, sizeof(unsigned long long)));
+    QP_CUDA_CHECK(s, cudaMemsetAsync(d, 0, sizeof(unsigned long long), s.stream));
+    const size_t nc = (size_t)s.grid.nc;
+    if (s.fp64) {
+        const double* b = (const double*)s.fields;
+        qp::Fields<double> f{};
+        f.ex = const_cast<double*>(b); f.ey = f.ex + nc; f.ez = f.ey + nc;
+        f.bx = f.ez + nc; f.by = f.bx + nc; f.bz = f.by + nc;
+        k_max_w<double><<<148 * 4, 256, 0, s.stream>>>(f, off, m, d);
+    } else {
+        const float* b = (const float*)s.fields;
+        qp::Fields<float> f{};
+        f.ex = const_cast<float*>(b); f.ey = f.ex + nc; f.ez = f.ey + nc;
+        f.bx = f.ez + nc; f.by = f.bx + nc; f.bz = f.by + nc;
+        k_max_w<float><<<148 * 4, 256, 0, s.stream>>>(f, off, m, d);
+    }
+    s.launches++;
+    unsigned long long v = 0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&v, d, sizeof(v), cudaMemcpyDeviceToHost, s.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+    cudaFree(d);
+    if (e != cudaSuccess) { s.err = cudaGetErrorString(e); return QP_ERR_CUDA; }
+    *out = __longlong_as_double_host(v);
     return QP_OK;
 }
 

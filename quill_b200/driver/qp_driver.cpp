@@ -20,10 +20,11 @@
 // y0film y1film z0film z1film nfilm mcr Tfilm vxfilm xnpic_film ynpic_film
 // znpic_film xnpic ynpic znpic ions data_folder output_mode
 // e_components_for_output b_components_for_output particles_for_output enthp
-// pmerging crpc mwindow (off | on) mwspeed mwseed t_add_mw and two
-// additions: precision (fp64 | mixed) and seed.  Not supported (the driver
-// stops with a message): mwindow = auto, mwseed_ions, neutral flows, density
-// profile arrays.
+// pmerging crpc mwindow (off | on | auto) mwtolerance mwspeed mwseed
+// mwseed_ions mw_mcr t_add_mw ne_profile_x_coords ne_profile_x_values
+// ne_profile_r_coords ne_profile_r_values nfilm_y0 nfilm_y1 gradwidth_y
+// nelflow vlflow mcrlflow Tlflow nerflow vrflow mcrrflow Trflow and two
+// additions: precision (fp64 | mixed) and seed.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -50,6 +51,7 @@ struct Var {
     std::string name;
     double value = 0;
     std::string units;
+    std::vector<double> arr;  // "[a;b;c]" values (input_array)
 };
 
 // One record: name, value (or '#'), units or text (or '#'), '$'.
@@ -63,7 +65,18 @@ std::vector<Var> read_stream(std::istream& in) {
         if (end != "$") throw std::runtime_error("malformed record for " + name);
         Var v;
         v.name = name;
-        v.value = (val == "#" || val.empty() || val[0] == '[') ? 0.0 : std::stod(val);
+        if (!val.empty() && val[0] == '[') {
+            // an array: numbers separated by ';' up to ']' (atof, low-level.cpp:387-411)
+            std::string cur;
+            for (size_t i = 1; i < val.size() && val[i] != ']'; i++) {
+                if (val[i] == ';') { v.arr.push_back(std::atof(cur.c_str())); cur.clear(); }
+                else cur += val[i];
+            }
+            if (!cur.empty()) v.arr.push_back(std::atof(cur.c_str()));
+        } else {
+            // the reference reads a single value with stof (low-level.cpp:414): float precision
+            v.value = (val == "#" || val.empty()) ? 0.0 : (double)std::stof(val);
+        }
         v.units = units == "#" ? "" : units;
         vars.push_back(v);
     }
@@ -94,7 +107,13 @@ double length(const Var& v, double lambda_cm) {
 // ------------------------------------------------------------ parameters ---
 struct Film {
     double x0 = 0, width = 0, grad = 0, y0 = 0, y1 = 0, z0 = 0, z1 = 0, ne = 0, mcr = 1, T = 0, vx = 0;
+    double ne_y0 = 0, ne_y1 = 0, grad_y = 0;  // cm^-3 at y0film / y1film, 1/k
     int xn = 0, yn = 0, zn = 0;
+};
+
+// a neutral flow entering through a face (main.cpp:1837-1880); n in n_cr
+struct Flow {
+    double n = 0, v = 0, mcr = 0, T = 0;
 };
 
 struct Config {
@@ -115,7 +134,13 @@ struct Config {
     int precision = QP_PREC_FP64;
     uint64_t seed = 0;
     std::string polarization = "linear";
-    bool mwindow = false;          // main.cpp:2932-2938 (on only)
+    bool mwindow = false;          // main.cpp:2932-2938
+    bool mw_auto = false;          // mwindow = auto (main.cpp:1961-1975)
+    double mwtolerance = 1e-6;     // main.cpp:2939-2943
+    bool mwseed_ions = false;      // main.cpp:2951-2954
+    double mw_mcr = 1;             // main.cpp:2955-2958
+    std::vector<double> prof_x, prof_xv, prof_r, prof_rv;  // ne_profile_* (main.cpp:3496-3523), coords in 1/k
+    Flow lflow, rflow;             // nelflow ... Trflow (main.cpp:3232-3249)
     double mwspeed = 1;            // main.cpp:2944-2947
     bool mwseed = true;            // main.cpp:2948-2950
     double t_add_mw = 0;           // main.cpp:2665-2679, 1/omega (0: last output time)
@@ -208,12 +233,18 @@ Config parse(const std::vector<Var>& v) {
     const std::string q = find(v, "qed").units;
     c.qed = !(q == "off");
     const std::string mw = find(v, "mwindow").units;
-    if (mw == "auto" || (mw != "off" && mw != "on" && !mw.empty()))
-        throw std::runtime_error("mwindow must be off or on (auto is not part of this build)");
-    if (mw.empty() || mw == "on") {  // the reference's default is on
+    if (mw != "off" && mw != "on" && mw != "auto" && !mw.empty())
+        throw std::runtime_error("mwindow must be off, on or auto");
+    c.mwtolerance = find(v, "mwtolerance").value;
+    if (c.mwtolerance == 0.0) c.mwtolerance = 1e-6;
+    c.mw_mcr = find(v, "mw_mcr").value;
+    if (c.mw_mcr == 0) c.mw_mcr = 1;
+    c.mwseed_ions = find(v, "mwseed_ions").units == "on";
+    if (mw.empty() || mw == "on" || mw == "auto") {  // the reference's default is on
         c.mwindow = true;
+        c.mw_auto = mw == "auto";
         c.mwspeed = find(v, "mwspeed").value;
-        if (c.mwspeed == 0) c.mwspeed = 1;
+        if (c.mwspeed == 0 && !c.mw_auto) c.mwspeed = 1;
         c.mwseed = find(v, "mwseed").units != "off";
         const Var& ta = find(v, "t_add_mw");
         double tv = ta.value;
@@ -221,13 +252,30 @@ Config parse(const std::vector<Var>& v) {
         else if (ta.units == "mm") tv = tv / (10 * c.lambda);
         else if (ta.units == "cm") tv = tv / c.lambda;
         c.t_add_mw = tv * 2 * PI;
-        if (find(v, "mwseed_ions").units == "on")
-            throw std::runtime_error("mwseed_ions is not part of this build");
-        if (find(v, "nelflow").value != 0 || find(v, "nerflow").value != 0)
-            throw std::runtime_error("neutral flows are not part of this build");
-        if (!find(v, "ne_profile_x_coords").units.empty() || !find(v, "ne_profile_r_coords").units.empty())
-            throw std::runtime_error("density profile arrays are not part of this build");
     }
+    // density profiles of the window's new plasma (main.cpp:3496-3523):
+    // coordinates in lambda unless given in um
+    auto coords = [&](const char* n) {
+        const Var& a = find(v, n);
+        std::vector<double> out = a.arr;
+        for (double& x : out) x = a.units == "um" ? x * 1e-4 / c.lambda * 2 * PI : x * 2 * PI;
+        return out;
+    };
+    c.prof_x = coords("ne_profile_x_coords");
+    c.prof_xv = find(v, "ne_profile_x_values").arr;
+    c.prof_r = coords("ne_profile_r_coords");
+    c.prof_rv = find(v, "ne_profile_r_values").arr;
+    if (c.prof_x.size() != c.prof_xv.size() || c.prof_r.size() != c.prof_rv.size())
+        throw std::runtime_error("density profile coordinates and values differ in length");
+    if (!std::is_sorted(c.prof_x.begin(), c.prof_x.end()) || !std::is_sorted(c.prof_r.begin(), c.prof_r.end()))
+        throw std::runtime_error("density profile coordinates are not sorted");
+    // neutral flows (main.cpp:3232-3249); they switch the moving window off
+    const double ncr = 1.11485e+13 / c.lambda / c.lambda;
+    c.lflow = {find(v, "nelflow").value * c.ne / ncr, find(v, "vlflow").value, find(v, "mcrlflow").value,
+               find(v, "Tlflow").value};
+    c.rflow = {find(v, "nerflow").value * c.ne / ncr, find(v, "vrflow").value, find(v, "mcrrflow").value,
+               find(v, "Trflow").value};
+    if (c.lflow.n != 0 || c.rflow.n != 0) c.mwindow = c.mw_auto = false;
     // films (main.cpp:3055-3229)
     c.xnpic = (int)find(v, "xnpic").value; if (c.xnpic <= 0) c.xnpic = 1;
     c.ynpic = (int)find(v, "ynpic").value; if (c.ynpic <= 0) c.ynpic = 1;
@@ -245,8 +293,15 @@ Config parse(const std::vector<Var>& v) {
         f.y1 = find(v, "y1film", s).value == 0 ? c.ylength : fl("y1film");
         f.z0 = fl("z0film");
         f.z1 = find(v, "z1film", s).value == 0 ? c.zlength : fl("z1film");
-        const Var& n = find(v, "nfilm", s);
-        f.ne = n.units == "ncr" ? n.value * 1.11485e+13 / c.lambda / c.lambda : (n.units == "ne" ? n.value * c.ne : n.value);
+        auto dens = [&](const char* nm) {
+            const Var& n = find(v, nm, s);
+            return n.units == "ncr" ? n.value * 1.11485e+13 / c.lambda / c.lambda : (n.units == "ne" ? n.value * c.ne : n.value);
+        };
+        f.ne = dens("nfilm");
+        f.ne_y0 = dens("nfilm_y0");
+        f.ne_y1 = dens("nfilm_y1");
+        if (f.ne != 0) f.ne_y0 = f.ne_y1 = f.ne;  // init_films, main.cpp:1253-1257
+        f.grad_y = fl("gradwidth_y");
         f.mcr = find(v, "mcr", s).value == 0 ? 1 : find(v, "mcr", s).value;
         f.T = find(v, "Tfilm", s).value;
         f.vx = find(v, "vxfilm", s).value;
@@ -370,9 +425,9 @@ struct Parts {
 // an exponential by rejection, isotropic direction, boost by the drift);
 // a zero drift leaves the direction unrotated (the reference divides by it).
 void fill_cell(Parts& P, double cmr, int ci, int cj, int ck, int xn, int yn, int zn, double n, double ux0, double T,
-               std::mt19937_64& rng) {
+               std::mt19937_64& rng, double dsplmt = 0) {
     std::uniform_real_distribution<double> U(0.0, 1.0);
-    const double x0 = 0.5 / xn, y0 = 0.5 / yn, z0 = 0.5 / zn;
+    const double x0 = 0.5 / xn + dsplmt, y0 = 0.5 / yn, z0 = 0.5 / zn;
     double q0 = 1 / double(xn * yn * zn) * n;
     if (cmr < 0) q0 = -q0;
     for (int ip = 0; ip < xn; ip++)
@@ -403,12 +458,13 @@ void fill_cell(Parts& P, double cmr, int ci, int cj, int ck, int xn, int yn, int
             }
 }
 
-// film (init.cpp:537-646) without transverse profile or y-gradient.
-// shift: how far the window has moved (x0 of the film in window coordinates
-// is x0 - shift); append: fill only the layer nx-3 the window just exposed,
-// if the film covers it (append_for_moving_window, init.cpp:559-570)
+// film (init.cpp:537-646).  shift: how far the window has moved (x0 of the
+// film in window coordinates is x0 - shift); append: fill only the layer
+// nx-3 the window just exposed, if the film covers it
+// (append_for_moving_window, init.cpp:559-570); profiled: the transverse
+// envelope the reference applies when neutral flows are on.
 void film(const Config& c, const Grid3& g, const Film& f, Parts& e, Parts* ion, double ion_cmr, Parts* pos,
-          std::mt19937_64& rng, double shift = 0, bool append = false) {
+          std::mt19937_64& rng, double shift = 0, bool append = false, bool profiled = false) {
     int i0 = (int)((f.x0 - shift) / c.dx), i1 = (int)((f.x0 + f.width - shift) / c.dx);
     if (append) {
         i0 = g.nx - 3;
@@ -418,12 +474,28 @@ void film(const Config& c, const Grid3& g, const Film& f, Parts& e, Parts* ion, 
         i0 = std::max(0, std::min(i0, g.nx));
         i1 = std::max(0, std::min(i1, g.nx));
     }
-    const double n_norm = f.ne / (1.11485e+13 / c.lambda / c.lambda);
+    const double ne_y0 = f.ne_y0 / (1.11485e+13 / c.lambda / c.lambda);
+    const double ne_y1 = f.ne_y1 / (1.11485e+13 / c.lambda / c.lambda);
     const double ux0 = f.vx / std::sqrt(1 - f.vx * f.vx);
+    const int jy0 = (int)(f.y0 / c.dy), jy1 = (int)(f.y1 / c.dy);
+    const double film_ylen = double(jy1 - jy0 - 3);
     for (int i = i0; i < i1; i++)
-        for (int j = (int)(f.y0 / c.dy) + 1; j < (int)(f.y1 / c.dy) - 1; j++)
+        for (int j = jy0 + 1; j < jy1 - 1; j++) {
+            const double nes_j = ne_y1 * (j - jy0 - 1) / film_ylen + ne_y0 * (jy1 - 2 - j) / film_ylen;
+            double nes_run = nes_j;  // the reference scales nes in place along k (init.cpp:583-600)
             for (int k = (int)(f.z0 / c.dz) + 1; k < (int)(f.z1 / c.dz) - 1; k++) {
-                double nes = n_norm;
+                if (profiled) {
+                    double tmp = (j * c.dy - g.ny * c.dy / 2) / (g.ny * c.dy / 2);
+                    tmp = std::cos(0.5 * PI * tmp * tmp * tmp * tmp * tmp);
+                    double tr_env = tmp * tmp;
+                    tmp = (k * c.dz - g.nz * c.dz / 2) / (g.nz * c.dz / 2);
+                    tmp = std::cos(0.5 * PI * tmp * tmp * tmp * tmp * tmp);
+                    tr_env *= tmp * tmp;
+                    nes_run *= tr_env;
+                }
+                if (f.grad_y >= 0 && j - jy0 - 1 < f.grad_y / c.dy) nes_run *= (j - jy0 - 1) / (f.grad_y / c.dy);
+                if (f.grad_y >= 0 && jy1 - 2 - j < f.grad_y / c.dy) nes_run *= (jy1 - 2 - j) / (f.grad_y / c.dy);
+                double nes = nes_run;
                 const double fx0 = f.x0 - shift;
                 if (f.grad >= 0) {
                     if (!(i >= (int)((fx0 + f.grad) / c.dx))) nes = nes * (i * c.dx - fx0) / f.grad;
@@ -435,6 +507,17 @@ void film(const Config& c, const Grid3& g, const Film& f, Parts& e, Parts* ion, 
                 if (ion) fill_cell(*ion, ion_cmr, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T * ion_cmr, rng);
                 if (pos) fill_cell(*pos, 1, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T, rng);
             }
+        }
+}
+
+// lin_interpolation (low-level.cpp:492-510): 1 without a profile
+double lin_interp(double x, const std::vector<double>& xs, const std::vector<double>& vs) {
+    if (xs.empty()) return 1.0;
+    if (x < xs[0]) return vs[0];
+    if (x > xs.back()) return vs.back();
+    const size_t i = std::lower_bound(xs.begin(), xs.end(), x) - xs.begin();
+    if (i == 0) return vs[0];
+    return vs[i - 1] + (vs[i] - vs[i - 1]) * (x - xs[i - 1]) / (xs[i] - xs[i - 1]);
 }
 
 // ------------------------------------------------------------- schedule ----
@@ -512,14 +595,32 @@ int main() {
     int n = 0;
     const int sp_e = n; p.cmr[n++] = -1;
     int sp_pos = -1, sp_ph = -1;
-    std::vector<int> sp_ion(c.films.size(), -1);
+    // ion populations (main.cpp:3250-3325): the distinct mcr of the films
+    // (last film first), then of the flows, then of the window's ions; one
+    // species each
+    std::vector<double> mcrs;
+    auto add_mcr = [&](double m) {
+        if (std::find(mcrs.begin(), mcrs.end(), m) == mcrs.end()) mcrs.push_back(m);
+    };
+    if (c.ions == "on" || c.ions == "positrons") {
+        for (size_t f = c.films.size(); f-- > 0;) add_mcr(c.films[f].mcr);
+        if (c.lflow.n != 0) add_mcr(c.lflow.mcr);
+        if (c.rflow.n != 0) add_mcr(c.rflow.mcr);
+        if (c.mwindow && !c.mw_auto && c.mwseed_ions) add_mcr(c.mw_mcr);
+    }
     std::vector<double> icmr;
+    std::vector<int> sp_pop;
+    for (double m : mcrs) {
+        icmr.push_back(1 / (PROTON_MASS * m));
+        sp_pop.push_back(n);
+        p.cmr[n++] = icmr.back();
+    }
+    auto ion_species = [&](double mcr) {
+        return (int)(std::find(mcrs.begin(), mcrs.end(), mcr) - mcrs.begin());
+    };
+    std::vector<int> sp_ion(c.films.size(), -1);
     if (c.ions == "on")
-        for (size_t f = 0; f < c.films.size(); f++) {
-            sp_ion[f] = n;
-            icmr.push_back(1 / (PROTON_MASS * c.films[f].mcr));
-            p.cmr[n++] = icmr.back();
-        }
+        for (size_t f = 0; f < c.films.size(); f++) sp_ion[f] = sp_pop[ion_species(c.films[f].mcr)];
     if (c.ions == "positrons" || c.qed) { sp_pos = n; p.cmr[n++] = 1; }
     if (c.qed) { sp_ph = n; p.cmr[n++] = 0; }
     p.n_species = n;
@@ -542,19 +643,22 @@ int main() {
     // films, loaded species by species (cell order is sorted inside the library)
     std::mt19937_64 rng(c.seed * 0x9E3779B97F4A7C15ull + 1);
     Parts E;
-    std::vector<Parts> I(c.films.size());
+    std::vector<Parts> I(mcrs.size());
     Parts Pz;
-    for (size_t f = 0; f < c.films.size(); f++)
-        film(c, g, c.films[f], E, sp_ion[f] >= 0 ? &I[f] : nullptr, sp_ion[f] >= 0 ? icmr[f] : 0,
-             c.ions == "positrons" ? &Pz : nullptr, rng);
+    const bool profiled = c.lflow.n != 0 || c.rflow.n != 0;
+    for (size_t f = c.films.size(); f-- > 0;) {
+        const int pi = sp_ion[f] >= 0 ? ion_species(c.films[f].mcr) : -1;
+        film(c, g, c.films[f], E, pi >= 0 ? &I[pi] : nullptr, pi >= 0 ? icmr[pi] : 0,
+             c.ions == "positrons" ? &Pz : nullptr, rng, 0, false, profiled);
+    }
     auto load = [&](int s, Parts& P) {
         if (r != QP_OK || P.x.empty()) return;
         r = qp_load_particles(h, s, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
                               P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
     };
     load(sp_e, E);
-    for (size_t f = 0; f < c.films.size(); f++)
-        if (sp_ion[f] >= 0) load(sp_ion[f], I[f]);
+    if (c.ions == "on")
+        for (size_t k = 0; k < mcrs.size(); k++) load(sp_pop[k], I[k]);
     if (sp_pos >= 0) load(sp_pos, Pz);
     if (r != QP_OK) {
         std::cerr << "qp_driver: " << qp_last_error(h) << std::endl;
@@ -644,8 +748,7 @@ int main() {
             ppd_sp[sp_e] = ppd[0];
             if (sp_pos >= 0) ppd_sp[sp_pos] = ppd[1];
             if (sp_ph >= 0) ppd_sp[sp_ph] = ppd[2];
-            for (size_t f = 0; f < sp_ion.size(); f++)
-                if (sp_ion[f] >= 0) ppd_sp[sp_ion[f]] = ppd[3 + (int)(std::find(icmr.begin(), icmr.end(), p.cmr[sp_ion[f]]) - icmr.begin())];
+            for (size_t k = 0; k < sp_pop.size(); k++) ppd_sp[sp_pop[k]] = ppd[3 + k];
         }
     };
 
@@ -666,16 +769,27 @@ int main() {
     auto add_window_particles = [&](int l) -> int {
         if (!((l + 1) * c.dt < t_add_mw)) return QP_OK;
         Parts Em, Pm;
-        std::vector<Parts> Im(c.films.size());
-        if (c.mwseed && c.ne > 0) {
-            const double n = c.ne / (1.11485e+13 / c.lambda / c.lambda);  // 1 / k0^2 (main.cpp:2602)
+        std::vector<Parts> Im(mcrs.size());
+        // mwseed / mwseed_ions: density ne times the x profile at the window's
+        // offset and the radial profile of each (j, k) line (main.cpp:1756-1821)
+        const double n = c.ne / (1.11485e+13 / c.lambda / c.lambda) *  // 1 / k0^2 (main.cpp:2602)
+                         lin_interp((nmw - 1) * c.dx, c.prof_x, c.prof_xv);
+        auto seed_layer = [&](Parts& P, double cmr) {
             for (int j = 0; j < (int)(c.ylength / c.dy); j++)
-                for (int k = 0; k < (int)(c.zlength / c.dz); k++)
-                    fill_cell(Em, -1, g.nx - 3, j, k, c.xnpic, c.ynpic, c.znpic, n, 0, 0, rng);
-        }
-        for (size_t f = 0; f < c.films.size(); f++)
-            film(c, g, c.films[f], Em, sp_ion[f] >= 0 ? &Im[f] : nullptr, sp_ion[f] >= 0 ? icmr[f] : 0,
+                for (int k = 0; k < (int)(c.zlength / c.dz); k++) {
+                    const double yr = j * c.dy - c.ylength / 2.0, zr = k * c.dz - c.zlength / 2.0;
+                    const double mod = lin_interp(std::sqrt(zr * zr + yr * yr), c.prof_r, c.prof_rv);
+                    if (mod != 0.0) fill_cell(P, cmr, g.nx - 3, j, k, c.xnpic, c.ynpic, c.znpic, n * mod, 0, 0, rng);
+                }
+        };
+        if (c.mwseed) seed_layer(Em, -1);
+        const int mw_pop = c.mwseed_ions ? ion_species(c.mw_mcr) : -1;
+        if (mw_pop >= 0 && mw_pop < (int)mcrs.size()) seed_layer(Im[mw_pop], icmr[mw_pop]);
+        for (size_t f = c.films.size(); f-- > 0;) {
+            const int pi = sp_ion[f] >= 0 ? ion_species(c.films[f].mcr) : -1;
+            film(c, g, c.films[f], Em, pi >= 0 ? &Im[pi] : nullptr, pi >= 0 ? icmr[pi] : 0,
                  c.ions == "positrons" ? &Pm : nullptr, rng, nmw * c.dx, true);
+        }
         int rr = QP_OK;
         auto put = [&](int sp, Parts& P) {
             if (rr == QP_OK && !P.x.empty())
@@ -683,8 +797,7 @@ int main() {
                                        P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
         };
         put(sp_e, Em);
-        for (size_t f = 0; f < c.films.size(); f++)
-            if (sp_ion[f] >= 0) put(sp_ion[f], Im[f]);
+        for (size_t k = 0; k < mcrs.size(); k++) put(sp_pop[k], Im[k]);
         if (sp_pos >= 0) put(sp_pos, Pm);
         return rr;
     };
@@ -717,7 +830,7 @@ int main() {
         if (c.particles_to_track.find('p') != std::string::npos && sp_pos >= 0) kinds.push_back(sp_pos);
         if (c.particles_to_track.find('g') != std::string::npos && sp_ph >= 0) kinds.push_back(sp_ph);
         if (c.particles_to_track.find('i') != std::string::npos)
-            for (int f : sp_ion) if (f >= 0) kinds.push_back(f);
+            for (int s2 : sp_pop) kinds.push_back(s2);
         std::vector<std::vector<int64_t>> first(kinds.size(), std::vector<int64_t>(cells.size()));
         for (size_t k = 0; k < kinds.size(); k++) {
             const int rr = qp_first_in_cells(h, kinds[k], (int64_t)cells.size(), cells.data(), first[k].data());
@@ -761,6 +874,60 @@ int main() {
         }
         return QP_OK;
     };
+    // add_neutral_flow_particles (main.cpp:1837-1880): when the flow has
+    // advanced one cell, a layer of plasma with a transverse envelope enters
+    // at i = 2..3 (from the left) or nx-4..nx-3 (from the right); the entry
+    // offset follows the reference's xrflow for both faces
+    double xlflow = 1, xrflow = 1;
+    auto add_flow = [&](int dir, const Flow& fl) -> int {
+        double& xflow = dir > 0 ? xlflow : xrflow;
+        int rr = QP_OK;
+        if (xflow >= 1) {
+            xflow -= 1;
+            const double nn = fl.n / c.xnpic;
+            const double u = dir * fl.v / std::sqrt(1 - fl.v * fl.v);
+            Parts Ef, If;
+            const int pi = c.ions == "on" ? ion_species(fl.mcr) : -1;
+            for (int j = 0; j < (int)(c.ylength / c.dy); j++)
+                for (int k = 0; k < (int)(c.zlength / c.dz); k++)
+                    for (int ii = 0; ii < c.xnpic; ii++) {
+                        double x0 = xrflow - float(ii) / c.xnpic;
+                        int ci;
+                        if (x0 >= 0) ci = dir > 0 ? 3 : g.nx - 4;
+                        else { ci = dir > 0 ? 2 : g.nx - 3; x0 += 1; }
+                        double tmp = (j * c.dy - c.ylength / 2) / (c.ylength / 2);
+                        tmp = std::cos(0.5 * PI * tmp * tmp * tmp * tmp * tmp);
+                        double tr_env = tmp * tmp;
+                        tmp = (k * c.dz - c.zlength / 2) / (c.zlength / 2);
+                        tmp = std::cos(0.5 * PI * tmp * tmp * tmp * tmp * tmp);
+                        tr_env *= tmp * tmp;
+                        const double ds = (dir > 0 ? x0 : 1 - x0) - 0.5;
+                        fill_cell(Ef, -1, ci, j, k, 1, c.ynpic, c.znpic, nn * tr_env, u, fl.T, rng, ds);
+                        if (pi >= 0)
+                            fill_cell(If, icmr[pi], ci, j, k, 1, c.ynpic, c.znpic, nn * tr_env, u,
+                                      fl.T / (PROTON_MASS * fl.mcr), rng, ds);
+                    }
+            // place(): only particles inside the region stay (plist.cpp:22-39)
+            auto keep_inside = [&](Parts& P) {
+                Parts Q;
+                for (size_t t = 0; t < P.x.size(); t++) {
+                    const int i = (int)P.x[t], j = (int)P.y[t], k = (int)P.z[t];
+                    if (i > 0 && i < g.nx - 2 && j > 0 && j < g.ny - 2 && k > 0 && k < g.nz - 2)
+                        Q.add(P.x[t], P.y[t], P.z[t], P.ux[t], P.uy[t], P.uz[t], P.g[t], P.q[t]);
+                }
+                return Q;
+            };
+            Parts Eq = keep_inside(Ef), Iq = keep_inside(If);
+            if (!Eq.x.empty())
+                rr = qp_load_particles(h, sp_e, (int64_t)Eq.x.size(), Eq.x.data(), Eq.y.data(), Eq.z.data(),
+                                       Eq.ux.data(), Eq.uy.data(), Eq.uz.data(), Eq.g.data(), Eq.q.data(), nullptr);
+            if (rr == QP_OK && pi >= 0 && !Iq.x.empty())
+                rr = qp_load_particles(h, sp_pop[pi], (int64_t)Iq.x.size(), Iq.x.data(), Iq.y.data(), Iq.z.data(),
+                                       Iq.ux.data(), Iq.uy.data(), Iq.uz.data(), Iq.g.data(), Iq.q.data(), nullptr);
+        }
+        xflow += c.dt * fl.v / c.dx;
+        return rr;
+    };
     for (int l = 0; l <= sch.it.back(); l++) {
         qp_diag d;
         if (merge_now && qp_pmerging(h, c.pmerging == "ti" ? QP_MERGE_TI : QP_MERGE_NL, ppd_sp.data()) != QP_OK) {
@@ -782,8 +949,22 @@ int main() {
             qp_destroy(h);
             return 1;
         }
-        // check_moving_window, mode on (main.cpp:1953-1959, 2333-2336)
-        const bool mw_now = c.mwindow && (l + 1) * c.dt * c.mwspeed > nmw * c.dx;
+        // check_moving_window (main.cpp:1953-1978, 2333-2336): mode on moves
+        // with mwspeed; mode auto moves when the front slice's max E^2 + B^2
+        // exceeds mwtolerance times the box's
+        bool mw_now = false;
+        if (c.mwindow && !c.mw_auto) {
+            mw_now = (l + 1) * c.dt * c.mwspeed > nmw * c.dx;
+        } else if (c.mw_auto) {
+            double max_w = 0, front = 0;
+            if (qp_max_w(h, 0, g.nx, &max_w) != QP_OK || qp_max_w(h, g.nx - nm - 2, g.nx - nm, &front) != QP_OK) {
+                std::cerr << "qp_driver: max_w after step " << l << ": " << qp_last_error(h) << std::endl;
+                qp_destroy(h);
+                return 1;
+            }
+            const double ratio = max_w > 0 ? front / max_w : 0.0;
+            mw_now = ratio > c.mwtolerance;
+        }
         if (mw_now) {
             if (qp_moving_window(h) != QP_OK) {
                 std::cerr << "qp_driver: moving window after step " << l << ": " << qp_last_error(h) << std::endl;
@@ -812,8 +993,7 @@ int main() {
             e_del += d.energy_erased_sp[sp_e];
             if (sp_pos >= 0) p_del += d.energy_erased_sp[sp_pos];
             if (sp_ph >= 0) ph_del += d.energy_erased_sp[sp_ph];
-            for (size_t f = 0; f < sp_ion.size(); f++)
-                if (sp_ion[f] >= 0) i_del[f] += d.energy_erased_sp[sp_ion[f]];
+            for (size_t k = 0; k < sp_pop.size(); k++) i_del[k] += d.energy_erased_sp[sp_pop[k]];
             fED << e_del << '\t' << p_del << '\t' << ph_del;
             for (double v2 : i_del) fED << '\t' << v2;
             fED << std::endl;
@@ -904,9 +1084,9 @@ int main() {
                         if (ie > -1 && ie < c.neps_ph) spec[ie] += k.q;
                         if (++i_particle_ph > c.enthp_ph) { i_particle_ph = 0; put(Dph, k); }
                     } else {
-                        for (size_t f = 0; f < sp_ion.size(); f++)
-                            if (k.sp == sp_ion[f]) {
-                                if (++i_particle_i > c.enthp_i) { i_particle_i = 0; put(Di[f], k); }
+                        for (size_t m = 0; m < sp_pop.size(); m++)
+                            if (k.sp == sp_pop[m]) {
+                                if (++i_particle_i > c.enthp_i) { i_particle_i = 0; put(Di[m], k); }
                                 break;
                             }
                     }
@@ -928,6 +1108,11 @@ int main() {
         }
         if (mw_now && add_window_particles(l) != QP_OK) {
             std::cerr << "qp_driver: window plasma after step " << l << ": " << qp_last_error(h) << std::endl;
+            qp_destroy(h);
+            return 1;
+        }
+        if ((c.lflow.n != 0 && add_flow(1, c.lflow) != QP_OK) || (c.rflow.n != 0 && add_flow(-1, c.rflow) != QP_OK)) {
+            std::cerr << "qp_driver: neutral flow after step " << l << ": " << qp_last_error(h) << std::endl;
             qp_destroy(h);
             return 1;
         }

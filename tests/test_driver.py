@@ -83,14 +83,93 @@ def test_driver_runs_conf_stream_and_writes_reference_formats(tmp_path):
     assert np.abs(ey0).max() > 1 and not np.allclose(ey0, ey1)
 
 
-def test_driver_rejects_automatic_window(tmp_path):
-    """mwindow = auto (main.cpp:1961-1977) is not part of this build: the
-    driver refuses before touching a device."""
+def _run_driver(conf, folder, timeout=300):
     from quill_b200 import build
     build.build()
-    conf = [c for c in CONF if c[0] != "mwindow"] + [("mwindow", "#", "auto")]
+    r = subprocess.run([DRIVER], input=stream(conf, folder), text=True, capture_output=True, timeout=timeout)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+def _rows(path):
+    return np.array([[float(v) for v in ln.split("\t")] for ln in open(path).read().strip().splitlines()])
+
+
+def test_driver_record_stream_reads_arrays_and_float_values(tmp_path):
+    """The record reader takes values with float precision, as var::read's
+    stof does, and arrays "[a;b;c]" (low-level.cpp:376-451): unsorted
+    profile coordinates are rejected before a device is touched."""
+    from quill_b200 import build
+    build.build()
+    conf = CONF + [("ne_profile_r_coords", "[1;0.5]", "lambda"), ("ne_profile_r_values", "[1;0]", "#")]
     r = subprocess.run([DRIVER], input=stream(conf, str(tmp_path / "r")), text=True, capture_output=True, timeout=60)
-    assert r.returncode != 0 and "mwindow" in r.stderr
+    assert r.returncode != 0 and "not sorted" in r.stderr
+    conf = CONF + [("ne_profile_r_coords", "[0;0.5;1]", "lambda"), ("ne_profile_r_values", "[1;0]", "#")]
+    r = subprocess.run([DRIVER], input=stream(conf, str(tmp_path / "r2")), text=True, capture_output=True, timeout=60)
+    assert r.returncode != 0 and "differ in length" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_automatic_window(tmp_path):
+    """mwindow = auto (main.cpp:1961-1975): the window stands until the
+    laser's max E^2 + B^2 in the front slice [nx-6, nx-4) exceeds mwtolerance
+    times the box's, then moves one cell per step while it does."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    folder = str(tmp_path / "results")
+    conf = [c for c in CONF if c[0] not in ("mwindow", "t_end", "output_period")] + [
+        ("mwindow", "#", "auto"), ("mwtolerance", "1e-4", "#"), ("t_end", "1.25", "lambda"),
+        ("output_period", "1.25", "lambda")]
+    _run_driver(conf, folder)
+    mw = np.loadtxt(os.path.join(folder, "mwcoordinate"))
+    assert mw.size == 41 and np.all(np.diff(mw) >= 0)
+    assert mw[0] == 0 and mw[-1] > 0             # stood first, then moved
+    steps = np.diff(mw) / 0.0625
+    assert np.all((np.abs(steps) < 1e-9) | (np.abs(steps - 1) < 1e-9))   # zero or one cell per step
+
+
+@pytest.mark.gpu
+def test_driver_neutral_flow(tmp_path):
+    """A neutral flow from the left (add_neutral_flow_particles,
+    main.cpp:1837-1880): a layer of plasma enters at i = 2..3 each time the
+    flow has advanced a cell, i.e. every dx / (v dt) = 4 steps at v = 0.5;
+    the moving window is switched off."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    # a cold film and no laser: only the flow changes the electron charge
+    base = [c for c in CONF if c[0] not in ("mwindow", "a0", "Tfilm")] + [("a0", "0", "#")]
+    flow = base + [("nelflow", "1", "#"), ("vlflow", "0.5", "#"), ("Tlflow", "0", "#"), ("mcrlflow", "1", "#")]
+    b = str(tmp_path / "flow")
+    _run_driver(flow, b)
+    assert "mwindow\noff\n" in open(os.path.join(b, "log")).read()
+    assert not os.path.exists(os.path.join(b, "mwcoordinate"))
+    ne = _rows(os.path.join(b, "N"))[:, 0]
+    inc = np.diff(ne)
+    jumps = np.nonzero(inc > 1e-6 * ne[0])[0] + 1
+    assert len(jumps) >= 4 and jumps[0] == 1 and np.all(np.isin(np.diff(jumps), (4, 5)))
+    quiet = np.setdiff1d(np.arange(1, ne.size), jumps)
+    assert np.all(np.abs(inc[quiet - 1]) <= 1e-9 * ne[0])
+    # every entering layer carries the same charge
+    np.testing.assert_allclose(inc[jumps - 1], inc[jumps[0] - 1], rtol=1e-9)
+
+
+@pytest.mark.gpu
+def test_driver_film_density_across_y(tmp_path):
+    """nfilm_y0 / nfilm_y1 (film, init.cpp:579-583): the film density grows
+    linearly from y0film to y1film; the electron density at t = 0 shows it."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    folder = str(tmp_path / "results")
+    conf = [c for c in CONF if c[0] not in ("nfilm", "mwindow", "a0", "Tfilm")] + [
+        ("mwindow", "#", "off"), ("nfilm_y0", "0.05", "ncr"), ("nfilm_y1", "0.2", "ncr"), ("a0", "0", "#")]
+    _run_driver(conf, folder)
+    log = read_log(os.path.join(folder, "log"))
+    nx, ny, nz = log["nx"], log["ny"], log["nz"]
+    rho = np.loadtxt(os.path.join(folder, "rho0"))
+    xy = np.abs(rho[:nx * (ny + nz)].reshape(nx, ny + nz)[:, :ny])   # per i: the xy line, then the xz line
+    col = xy[20, 2:ny - 3]                  # inside the film (x = 1.25 lambda), across y
+    assert np.all(np.diff(col) > 0)
+    assert col[-1] / col[0] > 3
 
 
 @pytest.mark.gpu
