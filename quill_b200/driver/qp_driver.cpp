@@ -16,6 +16,9 @@
 //
 // Supported parameters: dx dy dz dt lambda ne xlength ylength zlength t_end
 // output_period a0 a0y a0z polarization xsigma ysigma zsigma x0 y0 z0 phase
+// f_envelope (cos | sscos | pearl | tophat | uniformB) phi_rotate r0 theta
+// xtarget ytarget ztarget lp_reflection f_reflection beam beam_particles Nb
+// epsb xb rb x0b y0b phib
 // b_sign phi external_bz solver pusher qed film x0film filmwidth gradwidth
 // y0film y1film z0film z1film nfilm mcr Tfilm vxfilm xnpic_film ynpic_film
 // znpic_film xnpic ynpic znpic ions data_folder output_mode
@@ -120,6 +123,13 @@ struct Config {
     double dx, dy, dz, dt, lambda, ne = 0, xlength, ylength, zlength;
     std::vector<double> t_end, output_period;
     double a0y = 0, a0z = 0, xsigma = 0, ysigma = 0, zsigma = 0, x0 = 0, y00 = 0, z00 = 0, phase = 0, phi = 0;
+    int sscos = 0;                 // f_envelope: cos 0, sscos 1, pearl 2, tophat 3 (main.cpp:2811-2825)
+    bool uniform_b = false;        // f_envelope = uniformB (init.cpp:387-400)
+    double phi_rotate = 0, xtarget = 0, ytarget = 0, ztarget = 0;  // main.cpp:2835-2899
+    std::string lp_reflection = "off", f_reflection = "off";        // main.cpp:3402-3407
+    bool beam = false;             // main.cpp:2988-3053
+    std::string beam_particles = "e";
+    double Nb = 0, epsb = 0, xb = 0, rb = 0, x0b = 0, y0b = 0, phib = 0;
     bool b_sign = true;
     double external_bz = 0;
     int solver = QP_SOLVER_NDFX, pusher = QP_PUSHER_VAY;
@@ -218,8 +228,49 @@ Config parse(const std::vector<Var>& v) {
     c.b_sign = find(v, "b_sign").value != -1;
     const Var& phi = find(v, "phi");
     c.phi = phi.units == "deg" ? phi.value * PI / 180 : phi.value;
-    const Var& env = find(v, "f_envelope");
-    if (!env.units.empty() && env.units != "cos") throw std::runtime_error("only the cos laser envelope is supported");
+    const std::string env = find(v, "f_envelope").units;
+    if (env.empty() || env == "cos") c.sscos = 0;
+    else if (env == "sscos") c.sscos = 1;
+    else if (env == "pearl") c.sscos = 2;
+    else if (env == "tophat") c.sscos = 3;
+    else if (env == "uniformB") c.uniform_b = true;
+    else throw std::runtime_error("f_envelope " + env + " is not part of this build (cos, sscos, pearl, tophat, uniformB)");
+    const Var& phr = find(v, "phi_rotate");
+    c.phi_rotate = phr.units == "pi" ? phr.value * PI : phr.value;
+    // the pulse position as (r0, theta) (main.cpp:2850-2867)
+    const Var& r0v = find(v, "r0");
+    if (r0v.units != "off" && r0v.value != 0) {
+        const double r0 = length(r0v, c.lambda);
+        const Var& th = find(v, "theta");
+        const double theta = th.units == "deg" ? th.value * PI / 180 : th.value;
+        c.x0 = -r0 * std::cos(theta) + 0.00001;
+        c.y00 = -r0 * std::sin(theta);
+    }
+    auto target = [&](const char* n) {
+        const Var& x = find(v, n);
+        if (x.units == "off" || x.value == 0) return 0.0;
+        return x.units == "um" ? x.value * 1e-4 / c.lambda * 2 * PI : x.value * 2 * PI;
+    };
+    c.xtarget = target("xtarget");
+    c.ytarget = target("ytarget");
+    c.ztarget = target("ztarget");
+    c.lp_reflection = find(v, "lp_reflection").units;
+    if (c.lp_reflection.empty()) c.lp_reflection = "off";
+    c.f_reflection = find(v, "f_reflection").units;
+    if (c.f_reflection.empty()) c.f_reflection = "off";
+    // particle beam (main.cpp:2988-3053, init_beam main.cpp:1230-1239)
+    c.beam = find(v, "beam").units == "on";
+    c.beam_particles = find(v, "beam_particles").units;
+    if (c.beam_particles.empty()) c.beam_particles = "e";
+    c.Nb = find(v, "Nb").value;
+    const Var& eb = find(v, "epsb");
+    c.epsb = eb.units == "mc^2" ? eb.value * 0.511 : eb.value;  // MeV
+    c.xb = length(find(v, "xb"), c.lambda);
+    c.rb = length(find(v, "rb"), c.lambda);
+    c.x0b = length(find(v, "x0b"), c.lambda);
+    c.y0b = length(find(v, "y0b"), c.lambda);
+    const Var& pb = find(v, "phib");
+    c.phib = pb.units == "deg" ? pb.value * PI / 180 : pb.value;
     c.external_bz = find(v, "external_bz").value;
     // solver / pusher / qed (main.cpp:3542-3584); defaults NDFX, Vay, QED on
     const std::string sv = find(v, "solver").units, pu = find(v, "pusher").units;
@@ -365,9 +416,18 @@ struct Grid3 {
 // box centre; E and B of the envelope-modulated wave are rotated into the box.
 void laser_cos(const Config& c, const Grid3& g, std::vector<double>* F, double a0y, double a0z, double xc,
                double x1, double y0, double z0, double phi) {
-    const double xs = c.xsigma * 2 * std::sqrt(2 * PI) / 3;
-    const double ys = c.ysigma * 2 * std::sqrt(2 * PI) / 3;
-    const double zs = c.zsigma * 2 * std::sqrt(2 * PI) / 3;
+    double xs = 0, ys = 0, zs = 0;
+    if (c.sscos == 0) {
+        xs = c.xsigma * 2 * std::sqrt(2 * PI) / 3;
+        ys = c.ysigma * 2 * std::sqrt(2 * PI) / 3;
+        zs = c.zsigma * 2 * std::sqrt(2 * PI) / 3;
+    } else if (c.sscos == 1) {
+        xs = 0.822 * c.xsigma; ys = 0.822 * c.ysigma; zs = 0.822 * c.zsigma;
+    } else if (c.sscos == 2) {
+        xs = c.xsigma * 2 * std::sqrt(2 * PI) / 3; ys = 1e2 * c.ysigma; zs = 1e2 * c.ysigma;
+    } else {
+        xs = c.xsigma * 2 * std::sqrt(2 * PI) / 3; ys = 0.822 * c.ysigma; zs = 0.822 * c.zsigma;
+    }
     const double y12 = 0.5 * g.ny * c.dy, z12 = 0.5 * g.nz * c.dz;
     double r0x = std::sqrt(x1 * x1 + y0 * y0 + z0 * z0);
     double r0y = -y0 / r0x, r0z = -z0 / r0x;
@@ -385,22 +445,54 @@ void laser_cos(const Config& c, const Grid3& g, std::vector<double>* F, double a
     for (int i = 0; i < g.nx; i++)
         for (int j = 0; j < g.ny; j++)
             for (int k = 0; k < g.nz; k++) {
-                const double X = i * c.dx - xc, Y = j * c.dy - y12 - y0, Z = k * c.dz - z12 - z0;
+                const double X = i * c.dx - xc - c.xtarget, Y = j * c.dy - y12 - y0 - c.ytarget,
+                             Z = k * c.dz - z12 - z0 - c.ztarget;
                 const double x = r0x * X + r0y * Y + r0z * Z;
                 const double y = y0x * X + y0y * Y + y0z * Z;
                 const double z = z0x * X + z0y * Y + z0z * Z;
                 if (!(x < xs && x > -xs && y < ys && y > -ys && z < zs && z > -zs)) continue;
                 const double xi = x + c.phase;
-                const double cosx = std::cos(PI * x / 2 / xs), cosy = std::cos(PI * y / 2 / ys), cosz = std::cos(PI * z / 2 / zs);
-                const double sinx = std::sin(PI * x / 2 / xs), siny = std::sin(PI * y / 2 / ys), sinz = std::sin(PI * z / 2 / zs);
-                const double tr = cosy * cosy * cosz * cosz;
-                const double ey = a0y * tr * (std::cos(xi) * cosx * cosx - PI / xs * std::sin(xi) * cosx * sinx);
-                const double ez = a0z * tr * (std::sin(xi) * cosx * cosx + PI / xs * std::cos(xi) * cosx * sinx);
-                double bz = ey, by = -ez;
-                const double ex = a0y * std::sin(xi) * cosx * cosx * cosz * cosz * PI / ys * cosy * siny -
-                                  a0z * std::cos(xi) * cosx * cosx * cosy * cosy * PI / zs * cosz * sinz;
-                double bx = a0z * std::cos(xi) * cosx * cosx * PI / ys * cosz * cosz * cosy * siny +
-                            a0y * std::sin(xi) * cosx * cosx * cosy * cosy * PI / zs * cosz * sinz;
+                double ex = 0, ey = 0, ez = 0, bx = 0, by = 0, bz = 0;
+                if (c.sscos == 0) {
+                    const double cosx = std::cos(PI * x / 2 / xs), cosy = std::cos(PI * y / 2 / ys), cosz = std::cos(PI * z / 2 / zs);
+                    const double sinx = std::sin(PI * x / 2 / xs), siny = std::sin(PI * y / 2 / ys), sinz = std::sin(PI * z / 2 / zs);
+                    const double tr = cosy * cosy * cosz * cosz;
+                    ey = a0y * tr * (std::cos(xi) * cosx * cosx - PI / xs * std::sin(xi) * cosx * sinx);
+                    ez = a0z * tr * (std::sin(xi) * cosx * cosx + PI / xs * std::cos(xi) * cosx * sinx);
+                    bz = ey; by = -ez;
+                    ex = a0y * std::sin(xi) * cosx * cosx * cosz * cosz * PI / ys * cosy * siny -
+                         a0z * std::cos(xi) * cosx * cosx * cosy * cosy * PI / zs * cosz * sinz;
+                    bx = a0z * std::cos(xi) * cosx * cosx * PI / ys * cosz * cosz * cosy * siny +
+                         a0y * std::sin(xi) * cosx * cosx * cosy * cosy * PI / zs * cosz * sinz;
+                } else if (c.sscos == 1) {  // super-cosine envelope (init.cpp:122-134)
+                    const double x4 = xs * xs * xs * xs, y4 = ys * ys * ys * ys, z4 = zs * zs * zs * zs;
+                    const double cosx = std::cos(PI * x * x * x * x / 2 / x4), cosy = std::cos(PI * y * y * y * y / 2 / y4),
+                                 cosz = std::cos(PI * z * z * z * z / 2 / z4);
+                    const double sinx = std::sin(PI * x * x * x * x / 2 / x4), siny = std::sin(PI * y * y * y * y / 2 / y4),
+                                 sinz = std::sin(PI * z * z * z * z / 2 / z4);
+                    const double tr = cosy * cosy * cosz * cosz;
+                    ey = a0y * tr * (std::cos(xi) * cosx * cosx - 4 * PI * x * x * x / x4 * std::sin(xi) * cosx * sinx);
+                    ez = a0z * tr * (std::sin(xi) * cosx * cosx + 4 * PI * x * x * x / x4 * std::cos(xi) * cosx * sinx);
+                    bz = ey; by = -ez;
+                    ex = a0y * std::sin(xi) * 4 * PI * y * y * y / y4 * cosx * cosx * cosz * cosz * cosy * siny -
+                         a0z * std::cos(xi) * 4 * PI * z * z * z / z4 * cosx * cosx * cosy * cosy * cosz * sinz;
+                    bx = a0z * std::cos(xi) * 4 * PI * y * y * y / y4 * cosx * cosx * cosz * cosz * cosy * siny +
+                         a0y * std::sin(xi) * 4 * PI * z * z * z / z4 * cosx * cosx * cosy * cosy * cosz * sinz;
+                } else if (c.sscos == 2) {  // pearl: (sin r / r) transverse (init.cpp:135-150)
+                    const double cosx = std::cos(PI * x / 2 / xs), sinx = std::sin(PI * x / 2 / xs);
+                    const double r = std::sqrt(y * y + z * z);
+                    const double sr = r != 0 ? std::sin(PI * r / c.ysigma) / (PI * r / c.ysigma) : 1.0;
+                    ey = a0y * sr * (std::cos(xi) * cosx * cosx - PI / xs * std::sin(xi) * cosx * sinx);
+                    ez = a0z * sr * (std::sin(xi) * cosx * cosx + PI / xs * std::cos(xi) * cosx * sinx);
+                    bz = ey; by = -ez;
+                } else {  // tophat: super-cosine transverse (init.cpp:151-166)
+                    const double cosx = std::cos(PI * x / 2 / xs), sinx = std::sin(PI * x / 2 / xs);
+                    const double r = std::sqrt(y * y + z * z);
+                    const double cy = r <= ys ? std::cos(PI * r * r * r * r / 2 / (ys * ys * ys * ys)) : 0.0;
+                    ey = a0y * cy * cy * (std::cos(xi) * cosx * cosx - PI / xs * std::sin(xi) * cosx * sinx);
+                    ez = a0z * cy * cy * (std::sin(xi) * cosx * cosx + PI / xs * std::cos(xi) * cosx * sinx);
+                    bz = ey; by = -ez;
+                }
                 if (!c.b_sign) { bx = -bx; by = -by; bz = -bz; }
                 const long a = g.at(i, j, k);
                 F[0][a] += ex * r0x + ey * y0x + ez * z0x;
@@ -425,7 +517,7 @@ struct Parts {
 // an exponential by rejection, isotropic direction, boost by the drift);
 // a zero drift leaves the direction unrotated (the reference divides by it).
 void fill_cell(Parts& P, double cmr, int ci, int cj, int ck, int xn, int yn, int zn, double n, double ux0, double T,
-               std::mt19937_64& rng, double dsplmt = 0) {
+               std::mt19937_64& rng, double dsplmt = 0, double uy0 = 0) {
     std::uniform_real_distribution<double> U(0.0, 1.0);
     const double x0 = 0.5 / xn + dsplmt, y0 = 0.5 / yn, z0 = 0.5 / zn;
     double q0 = 1 / double(xn * yn * zn) * n;
@@ -434,7 +526,7 @@ void fill_cell(Parts& P, double cmr, int ci, int cj, int ck, int xn, int yn, int
         for (int jp = 0; jp < yn; jp++)
             for (int kp = 0; kp < zn; kp++) {
                 const double X = x0 + ci + double(ip) / xn, Y = y0 + cj + double(jp) / yn, Z = z0 + ck + double(kp) / zn;
-                double ux = ux0, uy = 0, uz = 0;
+                double ux = ux0, uy = uy0, uz = 0;
                 if (T != 0 && cmr != 0) {
                     const double u0 = std::fabs(ux0), v0 = u0 / std::sqrt(1 + u0 * u0);
                     double gamma, a, b, cc, r;
@@ -508,6 +600,44 @@ void film(const Config& c, const Grid3& g, const Film& f, Parts& e, Parts* ion, 
                 if (pos) fill_cell(*pos, 1, i, j, k, f.xn, f.yn, f.zn, nes, ux0, f.T, rng);
             }
         }
+}
+
+// add_beam (init.cpp:480-535): a beam of particles of charge sign cmr with
+// a parabolic density profile (length 2 xb, radius rb) moving along phib in
+// the xy plane, and the fields of an infinitely relativistic beam; cells
+// outside [1, n-2) lose their particles (place)
+void add_beam(const Config& c, const Grid3& g, std::vector<double>* F, Parts& P, double cmr, double n0, double u0,
+              double x0b, std::mt19937_64& rng) {
+    const double xb = c.xb, rb = c.rb, y0b = c.y0b, phib = c.phib;
+    const double signum = (u0 > 0) - (u0 < 0), type = (cmr > 0) - (cmr < 0);
+    for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+            for (int k = 0; k < g.nz; k++) {
+                const double phi = std::atan2((j - g.ny / 2) * c.dy - y0b, i * c.dx - x0b);
+                const double rr = std::sqrt((i * c.dx - x0b) * (i * c.dx - x0b) +
+                                            ((j - g.ny / 2) * c.dy - y0b) * ((j - g.ny / 2) * c.dy - y0b));
+                const double x = rr * std::cos(phi - phib), y = rr * std::sin(phi - phib);
+                const double z = (k - g.nz / 2) * c.dz;
+                const double r = std::sqrt(y * y + z * z);
+                if (!(x > -xb && x < xb)) continue;
+                double f_ampl;
+                if (r < rb) {
+                    const double n = n0 * (1 - x * x / (xb * xb)) * (1 - r * r / (rb * rb));
+                    if (i > 0 && i < g.nx - 2 && j > 0 && j < g.ny - 2 && k > 0 && k < g.nz - 2)
+                        fill_cell(P, cmr, i, j, k, c.xnpic, c.ynpic, c.znpic, n, u0 * std::cos(phib), 0, rng, 0,
+                                  u0 * std::sin(phib));
+                    f_ampl = 0.5 * n0 * (1 - x * x / (xb * xb)) * (1 - r * r / (2 * rb * rb));
+                } else {
+                    f_ampl = 0.25 * n0 * (1 - x * x / (xb * xb)) * rb * rb / (r * r);
+                }
+                const long a = g.at(i, j, k);
+                F[0][a] -= type * f_ampl * y * std::sin(phib);
+                F[1][a] += type * f_ampl * y * std::cos(phib);
+                F[2][a] += type * f_ampl * z;
+                F[3][a] += type * signum * f_ampl * z * std::sin(phib);
+                F[4][a] -= type * signum * f_ampl * z * std::cos(phib);
+                F[5][a] += type * signum * f_ampl * y;
+            }
 }
 
 // lin_interpolation (low-level.cpp:492-510): 1 without a profile
@@ -621,8 +751,8 @@ int main() {
     std::vector<int> sp_ion(c.films.size(), -1);
     if (c.ions == "on")
         for (size_t f = 0; f < c.films.size(); f++) sp_ion[f] = sp_pop[ion_species(c.films[f].mcr)];
-    if (c.ions == "positrons" || c.qed) { sp_pos = n; p.cmr[n++] = 1; }
-    if (c.qed) { sp_ph = n; p.cmr[n++] = 0; }
+    if (c.ions == "positrons" || c.qed || (c.beam && c.beam_particles == "p")) { sp_pos = n; p.cmr[n++] = 1; }
+    if (c.qed || (c.beam && c.beam_particles == "ph")) { sp_ph = n; p.cmr[n++] = 0; }
     p.n_species = n;
     qp_handle* h = nullptr;
     if (qp_create(&p, &h) != QP_OK) {
@@ -634,14 +764,83 @@ int main() {
     // plus the counter-propagating pulse for phi != 0 (main.cpp:1190-1192)
     std::vector<double> F[6];
     for (auto& f : F) f.assign(g.nc(), 0.0);
-    if (c.a0y != 0 || c.a0z != 0) {
-        laser_cos(c, g, F, c.a0y, c.a0z, c.xlength / 2 + c.x0, c.x0, c.y00, c.z00, 0);
-        if (c.phi != 0) laser_cos(c, g, F, c.a0y, c.a0z, c.xlength / 2 - c.x0, -c.x0, -c.y00, -c.z00, c.phi);
+    if (c.uniform_b) {
+        // f_init_uniformB (init.cpp:387-400)
+        for (long a = 0; a < g.nc(); a++) { F[4][a] = c.a0y; F[5][a] = c.a0z; }
+    } else if (c.a0y != 0 || c.a0z != 0) {
+        // init_fields, cos branch (main.cpp:1136-1229): the pulse, its
+        // counter-propagating copy for phi != 0, or its mirror images
+        const double A = c.a0y, Z = c.a0z, x0 = c.x0, y0 = c.y00, z0 = c.z00, xl = c.xlength / 2;
+        auto split = [](const std::string& s) {
+            std::vector<std::string> p(3);
+            size_t k = 0;
+            for (char ch : s) { if (ch == '&') { if (++k == 3) break; } else p[k] += ch; }
+            return p;
+        };
+        const std::vector<std::string> lp = split(c.lp_reflection), fr = split(c.f_reflection);
+        auto sy = [&](int m) { return (1 - 2 * (fr[m] == "y")) * A; };
+        auto sz = [&](int m) { return (1 - 2 * (fr[m] == "z")) * Z; };
+        auto P = [&](double ay, double az, double xc, double x1, double yy, double zz, double ph) {
+            laser_cos(c, g, F, ay, az, xc, x1, yy, zz, ph);
+        };
+        if (c.phi_rotate != 0) {
+            P(A, Z, xl + x0, x0, y0, z0, c.phi_rotate);
+        } else {
+            P(A, Z, xl + x0, x0, y0, z0, 0);
+            if (c.phi != 0) {
+                P(A, Z, xl - x0, -x0, -y0, -z0, c.phi);
+            } else if (lp[0] == "xy") {
+                P(sy(0), sz(0), xl + x0, x0, y0, -z0, 0);
+                if (lp[1] == "xz") {
+                    P(sy(1), sz(1), xl + x0, x0, -y0, z0, 0);
+                    P(sy(1), sz(1), xl + x0, x0, -y0, -z0, 0);
+                    if (lp[2] == "yz") {
+                        // the reference takes the z sign of the second reflection here
+                        P(sy(2), sz(1), -x0 + xl, -x0, y0, z0, 0);
+                        P(sy(2), sz(1), -x0 + xl, -x0, y0, -z0, 0);
+                        P(sy(2), sz(1), -x0 + xl, -x0, -y0, z0, 0);
+                        P(sy(2), sz(1), -x0 + xl, -x0, -y0, -z0, 0);
+                    }
+                } else if (lp[1] == "yz") {
+                    P(sy(1), sz(1), -x0 + xl, -x0, y0, z0, 0);
+                    P(sy(1), sz(1), -x0 + xl, -x0, y0, -z0, 0);
+                    if (lp[2] == "xz") {
+                        P(sy(2), sz(1), -x0 + xl, -x0, -y0, z0, 0);
+                        P(sy(2), sz(1), x0 + xl, x0, -y0, z0, 0);
+                        P(sy(2), sz(1), -x0 + xl, -x0, -y0, -z0, 0);
+                        P(sy(2), sz(1), x0 + xl, x0, -y0, -z0, 0);
+                    }
+                }
+            } else if (lp[0] == "xz") {
+                P(sy(0), sz(0), xl + x0, x0, -y0, z0, 0);
+                if (lp[1] == "yz") {
+                    P(sy(1), sz(1), -x0 + xl, -x0, -y0, z0, 0);
+                    P(sy(1), sz(1), -x0 + xl, -x0, y0, z0, 0);
+                }
+            } else if (lp[0] == "yz") {
+                P(sy(0), sz(0), -x0 + xl, -x0, y0, z0, 0);
+            }
+        }
+    }
+    // init_beam (main.cpp:1230-1239), after the laser and before the films
+    std::mt19937_64 rng(c.seed * 0x9E3779B97F4A7C15ull + 1);
+    Parts B;
+    int sp_beam = -1;
+    if (c.beam) {
+        const double n0 = c.Nb * 1.061e-11 / (c.xb * c.rb * c.rb * c.lambda);
+        const double x0b = c.xlength - c.x0b;
+        if (c.beam_particles == "ph") {
+            sp_beam = sp_ph;
+            add_beam(c, g, F, B, 0, n0, c.epsb / 0.511, x0b, rng);
+        } else {
+            const double u0 = ((c.epsb > 0) - (c.epsb < 0)) * std::sqrt(c.epsb * c.epsb / (0.511 * 0.511) - 1);
+            sp_beam = c.beam_particles == "p" ? sp_pos : sp_e;
+            add_beam(c, g, F, B, c.beam_particles == "p" ? 1 : -1, n0, u0, x0b, rng);
+        }
     }
     int r = qp_load_fields(h, F[0].data(), F[1].data(), F[2].data(), F[3].data(), F[4].data(), F[5].data());
     if (r == QP_OK) r = qp_init_boundaries(h);
     // films, loaded species by species (cell order is sorted inside the library)
-    std::mt19937_64 rng(c.seed * 0x9E3779B97F4A7C15ull + 1);
     Parts E;
     std::vector<Parts> I(mcrs.size());
     Parts Pz;
@@ -656,6 +855,7 @@ int main() {
         r = qp_load_particles(h, s, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
                               P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
     };
+    if (sp_beam >= 0) load(sp_beam, B);
     load(sp_e, E);
     if (c.ions == "on")
         for (size_t k = 0; k < mcrs.size(); k++) load(sp_pop[k], I[k]);

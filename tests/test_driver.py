@@ -278,3 +278,103 @@ def test_driver_tracks(tmp_path):
         assert np.all((rec[:, 1] > 1.0) & (rec[:, 1] < 1.6))  # near the film, in lambda
         # continuous trajectories: at most half a cell per step in x
         assert np.all(np.abs(np.diff(rec[:, 1])) <= 0.5 * 0.0625 + 1e-12)
+
+
+def _slices(folder, name, t, nx, ny, nz):
+    """The xy line at k = nz/2 and the xz line at j = ny/2 per i, then the
+    yz plane (the field and density slice layout)."""
+    a = np.loadtxt(os.path.join(folder, name + t))
+    lines = a[:nx * (ny + nz)].reshape(nx, ny + nz)
+    return lines[:, :ny], lines[:, ny:], a[nx * (ny + nz):].reshape(ny, nz)
+
+
+@pytest.mark.gpu
+def test_driver_laser_envelopes_and_uniform_b(tmp_path):
+    """f_envelope = sscos / pearl / tophat (f_init_cos's sscos 1-3,
+    init.cpp:122-166) give a pulse with the requested transverse shape (pearl
+    and tophat without E_x); uniformB (init.cpp:387-400) sets B_y, B_z to a0y,
+    a0z everywhere."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    base = [c for c in CONF if c[0] not in ("mwindow", "t_end", "output_period", "film")] + [
+        ("mwindow", "#", "off"), ("t_end", "0.0625", "lambda"), ("output_period", "0.0625", "lambda")]
+    maps = {}
+    for env in ("cos", "sscos", "pearl", "tophat"):
+        f = str(tmp_path / env)
+        _run_driver(base + [("f_envelope", "#", env)], f)
+        log = read_log(os.path.join(f, "log"))
+        nx, ny, nz = log["nx"], log["ny"], log["nz"]
+        ey = _slices(f, "ey", "0", nx, ny, nz)[0]   # (x, y) at z = the centre
+        assert 1 < np.abs(ey).max() < 1.5 * 5   # a0 = 5 is the vector potential; E has its derivative terms too
+        maps[env] = ey
+    envs = list(maps)
+    for a in range(len(envs)):
+        for b in range(a + 1, len(envs)):
+            assert not np.allclose(maps[envs[a]], maps[envs[b]], rtol=1e-3, atol=1e-3), (envs[a], envs[b])
+    # across y at the pulse's peak: the top hat is flat over most of its
+    # radius, the cos pulse is not
+    c, th = np.abs(maps["cos"]), np.abs(maps["tophat"])
+    i0 = int(np.argmax(c.max(axis=1)))
+    jc = ny // 2
+    assert th[i0, jc + 3] / th[i0, jc] > c[i0, jc + 3] / c[i0, jc]
+    f = str(tmp_path / "ub")
+    ub = [c for c in base if c[0] != "b_components_for_output"] + [("b_components_for_output", "#", "xyz")]
+    _run_driver(ub + [("f_envelope", "#", "uniformB"), ("a0y", "2", "#"), ("a0z", "3", "#")], f)
+    log = read_log(os.path.join(f, "log"))
+    nx, ny, nz = log["nx"], log["ny"], log["nz"]
+    by, bz = _slices(f, "by", "0", nx, ny, nz)[0], _slices(f, "bz", "0", nx, ny, nz)[0]
+    assert np.abs(_slices(f, "ey", "0", nx, ny, nz)[0]).max() == 0
+    np.testing.assert_allclose(by[2:-2, 2:-2], 2.0, rtol=1e-12)
+    np.testing.assert_allclose(bz[2:-2, 2:-2], 3.0, rtol=1e-12)
+
+
+@pytest.mark.gpu
+def test_driver_reflected_pulses(tmp_path):
+    """lp_reflection = xy (init_fields, main.cpp:1153-1229) adds the pulse's
+    mirror image at -z0.  In vacuum the field step is linear, so the run
+    equals the sum of a run with the pulse at z0 and one with it at -z0."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    base = [c for c in CONF if c[0] not in ("mwindow", "t_end", "output_period", "film", "zsigma")] + [
+        ("mwindow", "#", "off"), ("t_end", "0.0625", "lambda"), ("output_period", "0.0625", "lambda"),
+        ("zsigma", "0.2", "lambda")]
+    f1, f2, f3 = str(tmp_path / "up"), str(tmp_path / "both"), str(tmp_path / "down")
+    _run_driver(base + [("z0", "0.1", "lambda")], f1)
+    _run_driver(base + [("z0", "0.1", "lambda"), ("lp_reflection", "#", "xy")], f2)
+    _run_driver(base + [("z0", "-0.1", "lambda")], f3)
+    log = read_log(os.path.join(f1, "log"))
+    nx, ny, nz = log["nx"], log["ny"], log["nz"]
+    for name in ("ex", "ey", "ez", "bz"):
+        a, b, c = (np.loadtxt(os.path.join(f, name + "0")) for f in (f1, f2, f3))
+        assert np.abs(a).max() > 0
+        # (to 1e-4 of the peak: the text files carry 6 significant digits and
+        # cells at the envelope's edge enter with rounding-level differences)
+        np.testing.assert_allclose(b, a + c, rtol=0, atol=1e-4 * np.abs(b).max(), err_msg=name)
+
+
+@pytest.mark.gpu
+def test_driver_particle_beam(tmp_path):
+    """beam = on (init_beam / add_beam, main.cpp:1230-1239, init.cpp:480-535):
+    electrons with the parabolic profile moving along phib, and the beam's
+    own fields; the beam is the only charge of the run."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    f = str(tmp_path / "beam")
+    conf = [c for c in CONF if c[0] not in ("mwindow", "film", "a0", "t_end", "output_period")] + [
+        ("mwindow", "#", "off"), ("a0", "0", "#"), ("t_end", "0.0625", "lambda"), ("output_period", "0.0625", "lambda"),
+        ("beam", "#", "on"), ("Nb", "1e9", "#"), ("epsb", "100", "MeV"), ("xb", "0.3", "lambda"),
+        ("rb", "0.3", "lambda"), ("x0b", "1", "lambda"), ("y0b", "0", "lambda"), ("phib", "0", "deg")]
+    _run_driver(conf, f)
+    n = _rows(os.path.join(f, "N"))
+    assert n[0, 0] > 0 and n[0, 1] == 0
+    log = read_log(os.path.join(f, "log"))
+    nx, ny, nz = log["nx"], log["ny"], log["nz"]
+    ey = _slices(f, "ey", "0", nx, ny, nz)[0]
+    assert np.abs(ey).max() > 0
+    ps = np.array(open(os.path.join(f, "phasespace0")).read().split(), dtype=float).reshape(-1, 9)
+    # q x y z ux uy uz g chi: every beam electron moves along +x with gamma = 100 / 0.511
+    assert ps.shape[0] > 0
+    # (after one step in the beam's own fields, which nearly cancel)
+    assert np.all(ps[:, 4] > 0)
+    assert np.abs(ps[:, 5]).max() < 1e-2 * ps[:, 4].min() and np.abs(ps[:, 6]).max() < 1e-2 * ps[:, 4].min()
+    np.testing.assert_allclose(ps[:, 7], 100 / 0.511, rtol=1e-3)
