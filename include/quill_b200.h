@@ -271,6 +271,13 @@ int qp_replace_particle_slab(qp_handle* h, int species, int i0, int width, int64
                              const double* y, const double* z, const double* ux, const double* uy, const double* uz,
                              const double* g, const double* q, const double* chi);
 
+/* The field slices the reference's output writers use (fout.cpp:180-235),
+ * for the 12 planes E B J Bbar in turn: for each i the nz/2 line along y
+ * (ny values) and the ny/2 line along z (nz values), then the plane i = ix
+ * (ny*nz values, k fastest).  out: 12 * (nx*(ny+nz) + ny*nz) doubles, host
+ * or device. */
+int qp_dump_field_slices(qp_handle* h, int ix, double* out);
+
 /* max over the cells with i in [i0, i1) of Ex^2+Ey^2+Ez^2+Bx^2+By^2+Bz^2
  * (spatial_region::get_max_w, low-level.cpp:512-532), for the moving
  * window's AUTO mode (check_moving_window, main.cpp:1961-1975). */

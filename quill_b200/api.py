@@ -119,6 +119,7 @@ def load_library(path: str | None = None):
         "qp_replace_particle_slab": (C.c_int, [VP, C.c_int, C.c_int, C.c_int, I64] + [DP] * 9),
         "qp_layer_counts": (C.c_int, [VP, I64P]),
         "qp_max_w": (C.c_int, [VP, C.c_int, C.c_int, DP]),
+        "qp_dump_field_slices": (C.c_int, [VP, C.c_int, DP]),
         "qp_first_in_cells": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
         "qp_set_track_numbers": (C.c_int, [VP, C.c_int, I64, I64P, I64P]),
         "qp_get_tracked": (C.c_int, [VP, C.c_int, I64, I64P] + [DP] * 9 + [I64P]),
@@ -279,6 +280,13 @@ class Region:
         """Quasiparticles per x-layer, all species."""
         out = np.zeros(self.shape[0], dtype=np.int64)
         self._check(self.lib.qp_layer_counts(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        return out
+
+    def field_slices(self, ix: int) -> np.ndarray:
+        """(12, nx*(ny+nz) + ny*nz): the output slices of each field plane."""
+        nx, ny, nz = self.shape
+        out = np.zeros((12, nx * (ny + nz) + ny * nz))
+        self._check(self.lib.qp_dump_field_slices(self.h, ix, _dp(out)))
         return out
 
     def max_w(self, i0: int = 0, i1: int | None = None) -> float:

@@ -202,6 +202,48 @@ extern "C" int qp_max_w(qp_handle* h, int i0, int i1, double* out) {
     return QP_OK;
 }
 
+// The field output slices of the reference's writers (fout.cpp:180-235):
+// per component, for each i the line along y at k = nz/2 and the line along
+// z at j = ny/2, then the plane i = ix.
+template <typename T>
+__global__ void k_field_slices(const T* __restrict__ fields, int nx, int ny, int nz, int ix, size_t per,
+                               double* __restrict__ out) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 12 * per) return;
+    const int a = (int)(t / per);
+    const size_t r = t - (size_t)a * per;
+    const size_t lines = (size_t)nx * (ny + nz);
+    long cell;
+    if (r < lines) {
+        const int i = (int)(r / (ny + nz)), u = (int)(r - (size_t)i * (ny + nz));
+        cell = u < ny ? ((long)i * ny + u) * nz + nz / 2 : ((long)i * ny + ny / 2) * nz + (u - ny);
+    } else {
+        const size_t v = r - lines;
+        const int j = (int)(v / nz), k = (int)(v - (size_t)j * nz);
+        cell = ((long)ix * ny + j) * nz + k;
+    }
+    out[t] = (double)fields[(size_t)a * nx * ny * nz + cell];
+}
+
+extern "C" int qp_dump_field_slices(qp_handle* h, int ix, double* out) {
+    QP_SLAB_ENTRY(h, s);
+    if (!out || ix < 0 || ix >= s.grid.nx) { s.err = "qp_dump_field_slices: bad argument"; return QP_ERR_ARG; }
+    const int nx = s.grid.nx, ny = s.grid.ny, nz = s.grid.nz;
+    const size_t per = (size_t)nx * (ny + nz) + (size_t)ny * nz;
+    double* d = nullptr;
+    QP_CUDA_CHECK(s, cudaMalloc(&d, 12 * per * sizeof(double)));
+    const unsigned nb = (unsigned)((12 * per + 255) / 256);
+    if (s.fp64) k_field_slices<double><<<nb, 256, 0, s.stream>>>((const double*)s.fields, nx, ny, nz, ix, per, d);
+    else k_field_slices<float><<<nb, 256, 0, s.stream>>>((const float*)s.fields, nx, ny, nz, ix, per, d);
+    s.launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 12 * per * sizeof(double), cudaMemcpyDefault, s.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s.stream);
+    cudaFree(d);
+    if (e != cudaSuccess) { s.err = cudaGetErrorString(e); return QP_ERR_CUDA; }
+    return QP_OK;
+}
+
 // Quasiparticles per x-layer, all species (the particle part of
 // spatial_region::calculate_layer_weights, balancing.cpp:25-40).
 extern "C" int qp_layer_counts(qp_handle* h, int64_t* counts) {

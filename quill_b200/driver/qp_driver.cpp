@@ -682,6 +682,17 @@ struct Schedule {
 // Field slice file (fout.cpp:180-235 and the yz plane writers): for each i
 // the xy line at k = nz/2 then the xz line at j = ny/2, then the yz plane at
 // i = ix.  Text: one value per line with the default ostream precision.
+// values in the slice file's format: text, one per line, or raw doubles
+void write_values(const std::string& path, const double* a, size_t n, bool binary) {
+    if (binary) {
+        std::ofstream f(path, std::ios::out | std::ios::binary);
+        f.write((const char*)a, n * sizeof(double));
+    } else {
+        std::ofstream f(path);
+        for (size_t i = 0; i < n; i++) f << a[i] << "\n";
+    }
+}
+
 void write_slice(const std::string& path, const double* F, const Grid3& g, int ix, bool binary) {
     std::vector<double> a;
     a.reserve((size_t)g.nx * (g.ny + g.nz) + (size_t)g.ny * g.nz);
@@ -956,7 +967,7 @@ int main() {
     Schedule sch(c.t_end, c.output_period, c.dt);
     std::ofstream fN(c.data_folder + "/N"), fE(c.data_folder + "/energy");
     size_t out_i = 0;
-    std::vector<double> all(12 * (size_t)g.nc());
+    std::vector<double> slices(12 * ((size_t)g.nx * (g.ny + g.nz) + (size_t)g.ny * g.nz));
     const int ix = (int)((c.xlength - c.xlength / 2) / c.dx);
     // moving window state (main.cpp:122, 2665-2679)
     int nmw = 1;
@@ -1201,16 +1212,18 @@ int main() {
         evaluate_merging(d);
         if (out_i < sch.it.size() && l == sch.it[out_i]) {
             const std::string sfx = Schedule::suffix(sch.t[out_i]);
-            qp_dump_fields(h, all.data());
+            // the output slices come from the device (qp_dump_field_slices)
+            const size_t per = (size_t)g.nx * (g.ny + g.nz) + (size_t)g.ny * g.nz;
+            qp_dump_field_slices(h, ix, slices.data());
             const size_t NC = (size_t)g.nc();
             const char* en[3] = {"ex", "ey", "ez"};
             const char* bn[3] = {"bx", "by", "bz"};
             for (int a = 0; a < 3; a++) {
                 const char comp = "xyz"[a];
                 if (c.e_out.find(comp) != std::string::npos)
-                    write_slice(c.data_folder + "/" + en[a] + sfx, all.data() + a * NC, g, ix, c.binary);
+                    write_values(c.data_folder + "/" + en[a] + sfx, slices.data() + a * per, per, c.binary);
                 if (c.b_out.find(comp) != std::string::npos)
-                    write_slice(c.data_folder + "/" + bn[a] + sfx, all.data() + (3 + a) * NC, g, ix, c.binary);
+                    write_values(c.data_folder + "/" + bn[a] + sfx, slices.data() + (3 + a) * per, per, c.binary);
             }
             // densities: CIC deposition of every species (rhodeposition,
             // deposition.cpp:358-429) into rho / rho_p / rho_ph

@@ -210,3 +210,26 @@ def test_moving_window_mixed():
     for a in range(6):
         assert _rel(fg[a], fc[a]) <= 1e-4, a
     assert abs(g.count(0) - c.count()) <= max(2, c.count() // 2000)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_field_slices_and_max_w(precision):
+    """qp_dump_field_slices gives the output writers' lines and plane of every
+    field plane (fout.cpp:180-235); qp_max_w the max of E^2 + B^2 over an x
+    range (get_max_w, low-level.cpp:512-532)."""
+    species = (-1.0,)
+    case, fields, parts = small_case("fdtd", "boris", species=species)
+    g, _ = _load_both(case, fields, parts, species, precision)
+    g.step(2)
+    f = g.get_fields()
+    nx, ny, nz = case.nx, case.ny, case.nz
+    ix = nx // 2 + 1
+    s = g.field_slices(ix)
+    for a in range(12):
+        want = np.concatenate([np.concatenate([f[a, i, :, nz // 2], f[a, i, ny // 2, :]]) for i in range(nx)] +
+                              [f[a, ix].reshape(-1)])
+        np.testing.assert_array_equal(s[a], want)
+    w = (f[:6] ** 2).sum(0)
+    for i0, i1 in ((0, nx), (nx - 6, nx - 4), (3, 4)):
+        np.testing.assert_allclose(g.max_w(i0, i1), w[i0:i1].max(), rtol=1e-12 if precision == "fp64" else 1e-6)
+    assert g.max_w(5, 5) == 0.0
