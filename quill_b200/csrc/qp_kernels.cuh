@@ -6,23 +6,35 @@
 
 namespace qp {
 
-// One thread per cell, (k, j, i) = (x, y, z) launch axes.
+// (k, j, i) = (x, y, z) launch axes; each thread updates the cells (i, j, k)
+// for FIELD_CELLS<T> consecutive i (two in FP32, where one cell's bytes are
+// too few to keep enough loads in flight), every cell independently.
+template <typename T>
+struct FieldCells { static constexpr int value = 1; };
+template <>
+struct FieldCells<float> { static constexpr int value = 2; };
+
 template <typename T, int SOLVER, int PHASE>
 __global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
     if (k >= g.nz || j >= g.ny) return;
-    if (PHASE == 0) {
-        if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
-        else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
-        else fp_b(f, g, c, i, j, k);
-    } else if (PHASE == 1) {
-        if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
-        else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
-        else fp_e(f, g, c, i, j, k);
-    } else {
-        bbar(f, g, i, j, k);
+    constexpr int CPT = FieldCells<T>::value;
+#pragma unroll
+    for (int u = 0; u < CPT; u++) {
+        const int i = blockIdx.z * CPT + u;
+        if (i >= g.nx) break;
+        if (PHASE == 0) {
+            if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
+            else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
+            else fp_b(f, g, c, i, j, k);
+        } else if (PHASE == 1) {
+            if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
+            else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
+            else fp_e(f, g, c, i, j, k);
+        } else {
+            bbar(f, g, i, j, k);
+        }
     }
 }
 
@@ -58,26 +70,30 @@ __device__ __forceinline__ V warp_sum(V v) {
 // diagnostic accumulators.
 __device__ __forceinline__ void block_diag(DiagAccum* acc, int sp, double dq, double de,
                                            unsigned long long dc) {
-    __shared__ double s_q[32], s_e[32];
-    __shared__ unsigned long long s_c[32];
-    dq = warp_sum(dq);
-    de = warp_sum(de);
-    dc = warp_sum(dc);
+    // the block's values through shared memory, summed by its first warp
+    // (blocks of at most 256 threads); the counts with one warp reduction
+    __shared__ double s_q[256], s_e[256];
+    __shared__ unsigned s_c[8];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) { s_q[wid] = dq; s_e[wid] = de; s_c[wid] = dc; }
+    s_q[threadIdx.x] = dq;
+    s_e[threadIdx.x] = de;
+    const unsigned c = __reduce_add_sync(0xffffffffu, (unsigned)dc);
+    if (lane == 0) s_c[wid] = c;
     __syncthreads();
     if (wid == 0) {
+        double q = 0.0, e = 0.0;
+        for (int u = lane; u < (int)blockDim.x; u += 32) {
+            q += s_q[u];
+            e += s_e[u];
+        }
+        q = warp_sum(q);
+        e = warp_sum(e);
         const int nw = (blockDim.x + 31) >> 5;
-        dq = lane < nw ? s_q[lane] : 0.0;
-        de = lane < nw ? s_e[lane] : 0.0;
-        dc = lane < nw ? s_c[lane] : 0ull;
-        dq = warp_sum(dq);
-        de = warp_sum(de);
-        dc = warp_sum(dc);
-        if (lane == 0 && dc) {
-            atomicAdd(&acc->sum_q[sp], dq);
-            atomicAdd(&acc->sum_e[sp], de);
-            atomicAdd(&acc->cnt[sp], dc);
+        const unsigned cc = __reduce_add_sync(0xffffffffu, lane < nw ? s_c[lane] : 0u);
+        if (lane == 0 && cc) {
+            atomicAdd(&acc->sum_q[sp], q);
+            atomicAdd(&acc->sum_e[sp], e);
+            atomicAdd(&acc->cnt[sp], (unsigned long long)cc);
         }
     }
 }
@@ -284,8 +300,9 @@ __device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, 
 
 // Particles per new cell for the rebin, one atomic per run of equal cells.
 __device__ __forceinline__ void warp_count_runs(int32_t* count, int cell) {
-    int n[1] = {cell >= 0 ? 1 : 0};
-    if (warp_run_sum<int, 1>(cell, n)) atomicAdd(count + cell, n[0]);
+    // lanes with the same cell, wherever they sit in the warp: one atomic each
+    const unsigned m = __match_any_sync(0xffffffffu, cell);
+    if (cell >= 0 && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(count + cell, __popc(m));
 }
 
 __device__ __forceinline__ void catch_particle(const CatchBuf& c, int sp, uint32_t step, int phase, int s,

@@ -363,7 +363,8 @@ void launch_fields_mixed(State& s, int phase) {
     Fields<float> f = fields32(s);
     Coef<float> c(solver_coef(s.prm));
     dim3 blk(32, 8, 1);
-    dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, s.grid.nx);
+    constexpr int CPT = FieldCells<float>::value;
+    dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, (s.grid.nx + CPT - 1) / CPT);
     const int sol = s.prm.solver;
 #define QP_LF(SOL, PH) k_field<float, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c)
     if (phase == 0 || phase == 2) {

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256) k_rebin_count(const int32_t* __restrict__
 
 // Positions per warp of the scatter: REBIN_CHUNKS chunks of 32, whose loads
 // and claims are issued together (the kernel waits on memory and atomics).
-constexpr int REBIN_CHUNKS = 2;
+constexpr int REBIN_CHUNKS = 4;
 
 __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict__ newcell, int total,
                                                        const int32_t* __restrict__ cs,
