@@ -77,15 +77,17 @@ class _Setup:
     momenta (traversal order), step count."""
 
     def __init__(self, shape, dx, dt, lambda_cm, particles: dict, nsteps: int, every: int,
-                 external_bz: float = 0.0, device: int = 0):
+                 external_bz: float = 0.0, device: int = 0, precision: str = "fp64"):
         self.shape = tuple(shape)
         self.dx, self.dt, self.lambda_cm = dx, dt, lambda_cm
         self.particles = particles
         self.nsteps, self.every = nsteps, every
         self.external_bz = external_bz
         self.device = device
+        self.precision = precision
 
-    def region(self, fields: np.ndarray, q: np.ndarray, precision="fp64") -> Region:
+    def region(self, fields: np.ndarray, q: np.ndarray, precision=None) -> Region:
+        precision = self.precision if precision is None else precision
         nx, ny, nz = self.shape
         r = Region(nx, ny, nz, self.dx, self.dx, self.dx, self.dt, species_cmr=(-1.0,), lambda_cm=self.lambda_cm,
                    solver="fdtd", pusher="boris", precision=precision, device=self.device)
@@ -102,7 +104,9 @@ class FinalElectronEnergy(torch.autograd.Function):
 
     fields: float64 tensor (6, nx, ny, nz), Ex Ey Ez Bx By Bz as loaded;
     q: float64 tensor (n,), electron weights in traversal order (positions
-    sorted by cell; the order inside a cell is kept)."""
+    sorted by cell; the order inside a cell is kept).  With
+    setup.precision == "mixed" the forward runs in mixed precision and the
+    gradient is the FP64 adjoint along that trajectory."""
 
     @staticmethod
     def forward(ctx, fields: torch.Tensor, q: torch.Tensor, setup: _Setup):
@@ -145,7 +149,7 @@ def hermite_functions(u: torch.Tensor, n: int) -> torch.Tensor:
 class SlabLaserProblem:
     """The tanh-slab / Gauss-Hermite-laser gradient problem on one GPU."""
 
-    def __init__(self, case: SlabLaserCase, device: int = 0):
+    def __init__(self, case: SlabLaserCase, device: int = 0, precision: str = "fp64"):
         self.case = case
         c = case
         rng = np.random.default_rng(c.seed)
@@ -162,7 +166,7 @@ class SlabLaserProblem:
         self.particles = {"x": ci + rng.random(m), "y": cj + rng.random(m), "z": ck + rng.random(m),
                           "ux": zeros, "uy": zeros.copy(), "uz": zeros.copy(), "g": np.ones(m)}
         self.setup = _Setup((c.nx, c.ny, c.nz), c.dx, c.dt, c.lambda_cm, self.particles, c.nsteps, c.every,
-                            device=device)
+                            device=device, precision=precision)
         self._x = torch.from_numpy(self.particles["x"])
         # laser geometry (cells): cos^2 half-length from the FWHM as the
         # reference's f_init_cos converts it (init.cpp:34-37)
@@ -220,8 +224,9 @@ class SlabLaserProblem:
     def loss(self, coef: torch.Tensor, slab: torch.Tensor) -> torch.Tensor:
         return FinalElectronEnergy.apply(self.fields(coef), self.weights(slab), self.setup)
 
-    def loss_value(self, coef: torch.Tensor, slab: torch.Tensor, precision: str = "fp64") -> float:
-        """Forward only (FP64 or mixed precision), no gradients."""
+    def loss_value(self, coef: torch.Tensor, slab: torch.Tensor, precision: str | None = None) -> float:
+        """Forward only (FP64 or mixed precision; the problem's by default),
+        no gradients."""
         with torch.no_grad():
             f = self.fields(coef).cpu().numpy()
             q = self.weights(slab).cpu().numpy()

@@ -19,8 +19,15 @@
 // the rebin permutation of every step are recorded, then swept in reverse.
 //
 // Built with --fmad=false: the values recomputed inside the backward kernels
-// equal the forward step's, so branch decisions (cell floors, crossing
+// equal the FP64 forward step's, so branch decisions (cell floors, crossing
 // order) match it.
+//
+// Mixed precision: the forward and its re-runs are the FP32 step; each
+// step's recorded inputs (cell + offset widened to absolute FP64 positions,
+// FP32 momenta, weights, E and Bbar) are the linearisation points of the same
+// FP64 adjoint.  The gradient is that of the FP64 step map along the FP32
+// trajectory: it agrees with the FP64 adjoint to the FP32 trajectory's
+// distance from the FP64 one.
 #include <cmath>
 #include <string>
 #include <vector>
@@ -166,6 +173,26 @@ __global__ void k_record(PStore64 src, const int32_t* __restrict__ perm, int n, 
     rec.a[3][s] = src.ux[p]; rec.a[4][s] = src.uy[p]; rec.a[5][s] = src.uz[p];
     rec.a[6][s] = src.q[p];
     if (g_out) g_out[s] = src.g[p];
+}
+
+// The same from the mixed store: absolute positions cell + offset, FP32
+// values widened to FP64.
+__global__ void k_record32(Grid g, PStore32 src, const int32_t* __restrict__ perm, int n, Lam7 rec,
+                           double* g_out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int p = perm[s];
+    const int c = src.cell[p];
+    const int i = c / g.nynz, j = (c / g.nz) % g.ny, k = c % g.nz;
+    rec.a[0][s] = i + (double)src.ox[p]; rec.a[1][s] = j + (double)src.oy[p]; rec.a[2][s] = k + (double)src.oz[p];
+    rec.a[3][s] = src.ux[p]; rec.a[4][s] = src.uy[p]; rec.a[5][s] = src.uz[p];
+    rec.a[6][s] = src.q[p];
+    if (g_out) g_out[s] = src.g[p];
+}
+
+__global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, size_t n) {
+    const size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < n) b[x] = a[x];
 }
 
 // Adjoints through the rebin: out[perm[t]] = in[t] (erased particles keep 0).
@@ -377,16 +404,45 @@ PStore64 cur_store(Species& sp) {
     return st;
 }
 
+PStore32 cur_store32(Species& sp) {
+    PStore32 st;
+    st.cell = (int32_t*)sp.buf[sp.cur][0];
+    float** ps[9] = {&st.ox, &st.oy, &st.oz, &st.ux, &st.uy, &st.uz, &st.g, &st.q, &st.chi};
+    for (int a = 0; a < 9; a++) *ps[a] = (float*)sp.buf[sp.cur][1 + a];
+    return st;
+}
+
 inline int nblk(size_t n, int b) { return (int)((n + b - 1) / b); }
+
+// The step's particle inputs in traversal order, FP64, from either store.
+void record_inputs(State& s, Species& sp, int n, Lam7 rec, double* g_out) {
+    if (n <= 0) return;
+    if (s.fp64) k_record<<<nblk(n, 256), 256, 0, s.stream>>>(cur_store(sp), sp.perm, n, rec, g_out);
+    else k_record32<<<nblk(n, 256), 256, 0, s.stream>>>(s.grid, cur_store32(sp), sp.perm, n, rec, g_out);
+}
+
+// E (planes 0..2) and Bbar (9..11) at the step's start, FP64.
+cudaError_t record_fields(State& s, double* out) {
+    const size_t nc = (size_t)s.grid.nc;
+    if (s.fp64) {
+        const double* F = (const double*)s.fields;
+        cudaError_t e = cudaMemcpyAsync(out, F, 3 * nc * 8, cudaMemcpyDeviceToDevice, s.stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out + 3 * nc, F + 9 * nc, 3 * nc * 8, cudaMemcpyDeviceToDevice, s.stream);
+        return e;
+    }
+    const float* F = (const float*)s.fields;
+    k_widen<<<nblk(3 * nc, 256), 256, 0, s.stream>>>(F, out, 3 * nc);
+    k_widen<<<nblk(3 * nc, 256), 256, 0, s.stream>>>(F + 9 * nc, out + 3 * nc, 3 * nc);
+    return cudaGetLastError();
+}
 
 }  // namespace
 
 int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz, double* grad6, double* grad_q,
                    double* loss_out) {
     const qp_params& P = s.prm;
-    if (!s.fp64 || P.solver != QP_SOLVER_FDTD || P.pusher != QP_PUSHER_BORIS || P.qed || s.sp.size() != 1 ||
-        s.sp[0].cmr != -1) {
-        s.err = "the adjoint covers FP64, FDTD, Boris, QED off and one electron species";
+    if (P.solver != QP_SOLVER_FDTD || P.pusher != QP_PUSHER_BORIS || P.qed || s.sp.size() != 1 || s.sp[0].cmr != -1) {
+        s.err = "the adjoint covers FDTD, Boris, QED off and one electron species";
         return QP_ERR_CONFIG;
     }
     if (!s.boundaries_done) { s.err = "qp_init_boundaries has not run"; return QP_ERR_STATE; }
@@ -430,7 +486,7 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
         for (int a = 0; a < 7; a++) QP_CUDA_CHECK(s, w.alloc(&rec.a[a], n));
         QP_CUDA_CHECK(s, w.alloc(&gam, n));
         if (n > 0) {
-            k_record<<<nblk(n, 256), 256, 0, s.stream>>>(cur_store(sp), sp.perm, n, rec, gam);
+            record_inputs(s, sp, n, rec, gam);
             k_loss_seed<<<nblk(n, 256), 256, 0, s.stream>>>(rec, gam, n, bE, la);
         }
         QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
@@ -459,11 +515,9 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
             StepRec& R = recs[l - l0];
             R.n = (int)sp.n;
             for (int a = 0; a < 7; a++) QP_CUDA_CHECK(s, w.alloc(&R.in.a[a], R.n));
-            if (R.n > 0) k_record<<<nblk(R.n, 256), 256, 0, s.stream>>>(cur_store(sp), sp.perm, R.n, R.in, nullptr);
+            record_inputs(s, sp, R.n, R.in, nullptr);
             QP_CUDA_CHECK(s, w.alloc(&R.fields, 6 * nc));
-            const double* F = (const double*)s.fields;
-            QP_CUDA_CHECK(s, cudaMemcpyAsync(R.fields, F, 3 * nc * 8, cudaMemcpyDeviceToDevice, s.stream));
-            QP_CUDA_CHECK(s, cudaMemcpyAsync(R.fields + 3 * nc, F + 9 * nc, 3 * nc * 8, cudaMemcpyDeviceToDevice, s.stream));
+            QP_CUDA_CHECK(s, record_fields(s, R.fields));
             if ((r = qp_step(h, 1, ext_bz, nullptr)) != QP_OK) return r;
             R.n_next = (int)sp.n;
             QP_CUDA_CHECK(s, w.alloc(&R.perm, R.n_next));

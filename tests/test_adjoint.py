@@ -264,6 +264,38 @@ def test_mixed_forward_loss_close_to_fp64():
 
 
 @gpu
+def test_mixed_adjoint_close_to_fp64_adjoint():
+    """Mixed precision: the FP64 adjoint along the FP32 trajectory agrees
+    with the FP64 adjoint to the trajectories' distance (here 1e-3 of each
+    gradient's largest entry), for the fields, the weights and the 67
+    parameters through the torch binding."""
+    _require_gpu()
+    p64 = SlabLaserProblem(_small_case())
+    p32 = SlabLaserProblem(_small_case(), precision="mixed")
+    _, slab = p64.nominal()
+    f = _random_fields(p64)
+    q = p64.weights(slab).numpy()
+    out = {}
+    for name, p in (("fp64", p64), ("mixed", p32)):
+        r = p.setup.region(f, q)
+        out[name] = r.adjoint_energy(p.setup.nsteps, p.setup.every)
+        r.close()
+    (l64, gf64, gq64), (l32, gf32, gq32) = out["fp64"], out["mixed"]
+    assert abs(l32 - l64) <= 1e-4 * abs(l64)
+    assert np.abs(gf32 - gf64).max() <= 1e-3 * np.abs(gf64).max()
+    assert np.abs(gq32 - gq64).max() <= 1e-3 * np.abs(gq64).max()
+    grads = {}
+    for name, p in (("fp64", p64), ("mixed", p32)):
+        coef, slab = p.nominal()
+        coef.requires_grad_(True)
+        slab.requires_grad_(True)
+        p.loss(coef, slab).backward()
+        grads[name] = (coef.grad.clone(), slab.grad.clone())
+    for a, b in zip(grads["mixed"], grads["fp64"]):
+        assert torch.abs(a - b).max() <= 1e-3 * torch.abs(b).max()
+
+
+@gpu
 def test_adjoint_rejects_unsupported_configurations():
     _require_gpu()
     from quill_b200.api import QPError, Region
