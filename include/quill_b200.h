@@ -211,6 +211,13 @@ int qp_moving_window(qp_handle* h);
  * born outside the region (QED) are not recorded. */
 int qp_set_catching(qp_handle* h, int enable, int64_t capacity);
 
+/* dump_photons (advance.cpp:302-306): photons emitted by leptons are
+ * deleted as they are born and recorded in the capture buffer that
+ * qp_get_caught reads (allocated with `capacity` records if catching has
+ * none), their energy counted in qp_diag.energy_erased_sp of the photon
+ * species.  Needs QED. */
+int qp_set_dump_photons(qp_handle* h, int enable, int64_t capacity);
+
 /* The recorded particles (species index, position in cell units, u, g, q,
  * chi), ordered by species, then as the reference deletes them: by step,
  * the p_boundary erasures before the moves out of the region, each in

@@ -111,6 +111,7 @@ def load_library(path: str | None = None):
         "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
         "qp_moving_window": (C.c_int, [VP]),
         "qp_set_catching": (C.c_int, [VP, C.c_int, I64]),
+        "qp_set_dump_photons": (C.c_int, [VP, C.c_int, I64]),
         "qp_set_tracking": (C.c_int, [VP, C.c_int]),
         "qp_set_diag_range": (C.c_int, [VP, C.c_int, C.c_int]),
         "qp_get_field_slab": (C.c_int, [VP, C.c_int, C.c_int, DP]),
@@ -379,6 +380,9 @@ class Region:
     def set_catching(self, enable: bool = True, capacity: int = 1 << 20):
         """Record the particles the steps erase (catching)."""
         self._check(self.lib.qp_set_catching(self.h, int(bool(enable)), int(capacity)))
+
+    def set_dump_photons(self, enable: bool = True, capacity: int = 1 << 20):
+        self._check(self.lib.qp_set_dump_photons(self.h, int(bool(enable)), int(capacity)))
 
     def get_caught(self) -> dict:
         """The recorded particles (empties the buffer): species, x y z (cell

@@ -500,6 +500,7 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
     pa.track = 0;
     pa.step = 0;
     pa.cat = nullptr;
+    pa.dcat = nullptr;
     pa.trn_src = nullptr;
     pa.trn_dst = nullptr;
     pa.dlo = 0; pa.dhi = s.grid.nx;

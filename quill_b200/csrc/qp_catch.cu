@@ -29,16 +29,11 @@ void catch_release(State& s) {
 
 }  // namespace qp
 
-extern "C" int qp_set_catching(qp_handle* h, int enable, int64_t capacity) {
-    if (!h) return QP_ERR_ARG;
-    qp::State& s = *qp::state_of(h);
-    cudaError_t e = cudaSetDevice(s.prm.device);
-    if (e != cudaSuccess) { s.err = cudaGetErrorString(e); return QP_ERR_CUDA; }
-    cudaStreamSynchronize(s.stream);
-    qp::catch_release(s);
-    if (!enable) return QP_OK;
+namespace qp {
+static int catch_alloc(State& s, int64_t capacity) {
     if (capacity <= 0 || capacity >= INT32_MAX) { s.err = "catching capacity must lie in [1, 2^31-1)"; return QP_ERR_ARG; }
-    qp::CatchBuf c{};
+    cudaError_t e = cudaSuccess;
+    CatchBuf c{};
     double** d[9] = {&c.x, &c.y, &c.z, &c.ux, &c.uy, &c.uz, &c.g, &c.q, &c.chi};
     for (double** p : d)
         if (e == cudaSuccess) e = cudaMalloc(p, (size_t)capacity * sizeof(double));
@@ -47,17 +42,60 @@ extern "C" int qp_set_catching(qp_handle* h, int enable, int64_t capacity) {
     if (e == cudaSuccess) e = cudaMalloc(&c.counter, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(c.counter, 0, sizeof(int));
     c.cap = (int)capacity;
-    qp::CatchBuf* dc = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&dc, sizeof(qp::CatchBuf));
-    if (e == cudaSuccess) e = cudaMemcpy(dc, &c, sizeof(qp::CatchBuf), cudaMemcpyHostToDevice);
+    CatchBuf* dc = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&dc, sizeof(CatchBuf));
+    if (e == cudaSuccess) e = cudaMemcpy(dc, &c, sizeof(CatchBuf), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) cudaFree(dc);
     if (e != cudaSuccess) {
-        qp::catch_free(c);
-        s.err = std::string("qp_set_catching: ") + cudaGetErrorString(e);
+        catch_free(c);
+        s.err = std::string("capture buffer: ") + cudaGetErrorString(e);
         return QP_ERR_CUDA;
     }
     s.cat = c;
     s.d_cat = dc;
+    return QP_OK;
+}
+}  // namespace qp
+
+// Erasures recorded (catching_enabled) or not.  The buffer is shared with
+// dump_photons; enabling allocates it anew with `capacity` records.
+extern "C" int qp_set_catching(qp_handle* h, int enable, int64_t capacity) {
+    if (!h) return QP_ERR_ARG;
+    qp::State& s = *qp::state_of(h);
+    cudaError_t e = cudaSetDevice(s.prm.device);
+    if (e != cudaSuccess) { s.err = cudaGetErrorString(e); return QP_ERR_CUDA; }
+    cudaStreamSynchronize(s.stream);
+    if (!enable) {
+        s.catch_erasures = false;
+        if (!s.dump_photons) qp::catch_release(s);
+        return QP_OK;
+    }
+    qp::catch_release(s);
+    const int r = qp::catch_alloc(s, capacity);
+    s.catch_erasures = r == QP_OK;
+    return r;
+}
+
+// dump_photons (advance.cpp:302-306): photons emitted by leptons are deleted
+// as they are born, into the capture buffer (allocated with `capacity`
+// records if there is none), with their energy in qp_diag's erased energy.
+extern "C" int qp_set_dump_photons(qp_handle* h, int enable, int64_t capacity) {
+    if (!h) return QP_ERR_ARG;
+    qp::State& s = *qp::state_of(h);
+    cudaError_t e = cudaSetDevice(s.prm.device);
+    if (e != cudaSuccess) { s.err = cudaGetErrorString(e); return QP_ERR_CUDA; }
+    cudaStreamSynchronize(s.stream);
+    if (!enable) {
+        s.dump_photons = false;
+        if (!s.catch_erasures) qp::catch_release(s);
+        return QP_OK;
+    }
+    if (!s.prm.qed) { s.err = "dump_photons needs QED"; return QP_ERR_STATE; }
+    if (!s.cat.counter) {
+        const int r = qp::catch_alloc(s, capacity);
+        if (r != QP_OK) return r;
+    }
+    s.dump_photons = true;
     return QP_OK;
 }
 

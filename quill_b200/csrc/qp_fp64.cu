@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
         double chi = src.chi[p];
         const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
         int nc = -1;
+        bool converted = false;  // a photon that became a pair is not an erasure
         if (!kill_layer(g, i0, j0, k0)) {
             double E[3], B[3];
             gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
@@ -186,6 +187,7 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
                     const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
                     if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
                 } else {
+                    converted = true;
                     // electron with r of the photon energy, positron with 1 - r
                     born_lepton64<PUSHER>(f, g, a, qa, pos, ui, r * g_prev, r * chi, -q, -1.0, E, B, t0);
                     born_lepton64<PUSHER>(f, g, a, qa, pos, ui, (1 - r) * gm, (1 - r) * chi, q, 1.0, E, B, t1);
@@ -220,7 +222,18 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
                     ph[0] += a3 * uph[0] / a.dx;
                     ph[1] += a3 * uph[1] / a.dy;
                     ph[2] += a3 * uph[2] / a.dz;
-                    append64(t0, g, a.dlo, a.dhi, ph, uph, gph, fabs(q), r * chi, true, a.status, a.diag);
+                    if (a.dcat) {
+                        // dump_photons: the photon is deleted as it is born (advance.cpp:302-306),
+                        // recorded with its energy unless it sits in an exchange area
+                        const int pi = (int)ph[0];
+                        if (pi >= a.dlo && pi < a.dhi) {
+                            catch_particle(*a.dcat, t0.sp, a.step, 2, s, ph[0], ph[1], ph[2], uph[0], uph[1], uph[2],
+                                           gph, fabs(q), r * chi);
+                            atomicAdd(&a.diag->sum_erased[t0.sp], gph * fabs(q));
+                        }
+                    } else {
+                        append64(t0, g, a.dlo, a.dhi, ph, uph, gph, fabs(q), r * chi, true, a.status, a.diag);
+                    }
                     // recoil (advance.cpp:308-322)
                     chi = (1 - r) * chi;
                     gm = (1 - r) * g_prev;
@@ -251,9 +264,12 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
         }
         newcell[s] = nc;
-        if (nc < 0 && a.cat && (int)pos[0] >= a.dlo && (int)pos[0] < a.dhi)
+        const bool erased = nc < 0 && !converted && (int)pos[0] >= a.dlo && (int)pos[0] < a.dhi;
+        if (erased && a.cat)
             catch_particle(*a.cat, a.sp, a.step, kill_layer(g, i0, j0, k0) ? 0 : 1, s, pos[0], pos[1], pos[2], ux, uy,
                            uz, gm, q, chi);
+        if (erased && a.track)  // erasures are few: one atomic each
+            atomicAdd(&a.diag->sum_erased[a.sp], KIND == KIND_PHOTON ? gm * q : (gm - 1) * q);
         if (nc >= 0) {
             dst.x[s] = pos[0]; dst.y[s] = pos[1]; dst.z[s] = pos[2];
             dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
@@ -412,9 +428,10 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
-    a.track = 0;
+    a.track = s.track_erased ? 1 : 0;
     a.step = (uint32_t)s.step_index;
-    a.cat = s.d_cat;
+    a.cat = s.catch_erasures ? s.d_cat : nullptr;
+    a.dcat = s.dump_photons ? s.d_cat : nullptr;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
@@ -473,7 +490,8 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.status = s.d_status; a.diag = s.d_diag;
     a.track = s.track_erased ? 1 : 0;
     a.step = (uint32_t)s.step_index;
-    a.cat = s.d_cat;
+    a.cat = s.catch_erasures ? s.d_cat : nullptr;
+    a.dcat = s.dump_photons ? s.d_cat : nullptr;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;

@@ -143,7 +143,9 @@ struct State {
     bool tracking = false;      // qp_set_tracking: Species::trn allocated and carried by the pushes
     int diag_lo = 0, diag_hi = 0;  // qp_set_diag_range: cells i in [diag_lo, diag_hi) counted (create: [0, nx))
     void* window_scratch = nullptr;  // one field plane, for the moving window's shift
-    CatchBuf cat{};                  // catching: erased particles (counter null = off)
+    CatchBuf cat{};                  // capture buffer (counter null = none)
+    bool catch_erasures = false;     // qp_set_catching: erasures go to the buffer
+    bool dump_photons = false;       // qp_set_dump_photons: emitted photons go to the buffer
     CatchBuf* d_cat = nullptr;       // its device copy, passed to the push kernels
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double phase_ms[4] = {0, 0, 0, 0};

@@ -322,7 +322,8 @@ struct PushArgs {
     int n, sp, kind;
     int track;  // sum the energy of erased particles into diag->sum_erased
     uint32_t step;
-    const CatchBuf* cat;  // device copy; nullptr: catching off
+    const CatchBuf* cat;  // device copy; nullptr: erasures are not recorded
+    const CatchBuf* dcat;  // dump_photons: emitted photons recorded here instead of kept; nullptr: kept
     const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
     int32_t* trn_dst;
     int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)

@@ -15,7 +15,8 @@ struct PushArgs32 {
     unsigned int* status;
     DiagAccum* diag;
     uint32_t step;
-    const CatchBuf* cat;  // device copy; nullptr: catching off
+    const CatchBuf* cat;  // device copy; nullptr: erasures are not recorded
+    const CatchBuf* dcat;  // dump_photons: emitted photons recorded here instead of kept; nullptr: kept
     const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
     int32_t* trn_dst;
     int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)
@@ -201,6 +202,7 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
         float chi = src.chi[p];
         const float e_s = (float)qa.e_s;
         int nc = -1, i1 = i0, j1 = j0, k1 = k0;
+        bool converted = false;  // a photon that became a pair is not an erasure
         const bool live = !kill_layer(g, i0, j0, k0);
         if (live) {
             float E[3], B[3];
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                     i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
                     if (!(si | sj | sk) || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
                 } else {
+                    converted = true;
                     // electron with r of the photon energy, positron with 1 - r
                     born_lepton32<PUSHER>(f, g, a, e_s, i0, j0, k0, o, ui, r * g_prev, r * chi, -q, -1.f, E, B, t0);
                     born_lepton32<PUSHER>(f, g, a, e_s, i0, j0, k0, o, ui, (1.f - r) * gm, (1.f - r) * chi, q, 1.f,
@@ -257,8 +260,18 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                     ph[0] += a3 * uph[0] * a.idx;
                     ph[1] += a3 * uph[1] * a.idy;
                     ph[2] += a3 * uph[2] * a.idz;
-                    append32(t0, g, a.dlo, a.dhi, i0, j0, k0, ph, uph, gph, fabsf(q), r * chi, true, a.status,
-                             a.diag);
+                    if (a.dcat) {
+                        // dump_photons: the photon is deleted as it is born (advance.cpp:302-306)
+                        const double px = (double)i0 + (double)ph[0];
+                        if ((int)floor(px) >= a.dlo && (int)floor(px) < a.dhi) {
+                            catch_particle(*a.dcat, t0.sp, a.step, 2, s, px, (double)j0 + (double)ph[1],
+                                           (double)k0 + (double)ph[2], uph[0], uph[1], uph[2], gph, fabsf(q), r * chi);
+                            atomicAdd(&a.diag->sum_erased[t0.sp], (double)gph * (double)fabsf(q));
+                        }
+                    } else {
+                        append32(t0, g, a.dlo, a.dhi, i0, j0, k0, ph, uph, gph, fabsf(q), r * chi, true, a.status,
+                                 a.diag);
+                    }
                     // recoil (advance.cpp:308-322)
                     chi = (1.f - r) * chi;
                     gm = (1.f - r) * g_prev;
@@ -293,9 +306,13 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
         }
         newcell[s] = nc;
-        if (nc < 0 && a.cat && i1 >= a.dlo && i1 < a.dhi)
+        const bool erased = nc < 0 && !converted && i1 >= a.dlo && i1 < a.dhi;
+        if (erased && a.cat)
             catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, (double)i1 + (double)o[0],
                            (double)j1 + (double)o[1], (double)k1 + (double)o[2], ux, uy, uz, gm, q, chi);
+        if (erased && a.track)  // erasures are few: one atomic each
+            atomicAdd(&a.diag->sum_erased[a.sp],
+                      KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q);
         if (nc >= 0) {
             dst.cell[s] = nc;
             dst.ox[s] = o[0]; dst.oy[s] = o[1]; dst.oz[s] = o[2];
@@ -415,7 +432,8 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.status = s.d_status; a.diag = s.d_diag;
     a.track = s.track_erased ? 1 : 0;
     a.step = (uint32_t)s.step_index;
-    a.cat = s.d_cat;
+    a.cat = s.catch_erasures ? s.d_cat : nullptr;
+    a.dcat = s.dump_photons ? s.d_cat : nullptr;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
@@ -476,9 +494,10 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
     a.idx = (float)(1.0 / s.prm.dx); a.idy = (float)(1.0 / s.prm.dy); a.idz = (float)(1.0 / s.prm.dz);
     a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
-    a.track = 0;
+    a.track = s.track_erased ? 1 : 0;
     a.step = (uint32_t)s.step_index;
-    a.cat = s.d_cat;
+    a.cat = s.catch_erasures ? s.d_cat : nullptr;
+    a.dcat = s.dump_photons ? s.d_cat : nullptr;
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;

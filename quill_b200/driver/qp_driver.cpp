@@ -155,6 +155,7 @@ struct Config {
     bool mwseed = true;            // main.cpp:2948-2950
     double t_add_mw = 0;           // main.cpp:2665-2679, 1/omega (0: last output time)
     bool catching = false;         // main.cpp:3531-3534
+    bool dump_photons = false;     // emitted photons deleted as they are born
     int n_tracks = 0;              // main.cpp:3408-3413
     std::string particles_to_track = "epgi";
     double tr_start = 0, xtr1 = 0, ytr1 = 0, ztr1 = 0, xtr2 = 0, ytr2 = 0, ztr2 = 0;  // main.cpp:3419-3480
@@ -387,7 +388,7 @@ Config parse(const std::vector<Var>& v) {
     }
     c.xtr1 = length(find(v, "xtr1"), c.lambda); c.ytr1 = length(find(v, "ytr1"), c.lambda); c.ztr1 = length(find(v, "ztr1"), c.lambda);
     c.xtr2 = length(find(v, "xtr2"), c.lambda); c.ytr2 = length(find(v, "ytr2"), c.lambda); c.ztr2 = length(find(v, "ztr2"), c.lambda);
-    if (find(v, "dump_photons").units == "on") throw std::runtime_error("dump_photons is not part of this build");
+    c.dump_photons = find(v, "dump_photons").units == "on" && c.qed;  // main.cpp:3545-3549
     auto mev = [&](const char* n) { const Var& w = find(v, n); return w.units == "mc^2" ? w.value * 0.511 : w.value; };
     c.deps_ph = mev("deps_ph");
     if (c.deps_ph == 0) c.deps_ph = mev("deps");
@@ -887,11 +888,15 @@ int main() {
     int i_particle = 0, i_particle_p = 0, i_particle_ph = 0, i_particle_i = 0;
     if (r == QP_OK && c.n_tracks > 0) r = qp_set_tracking(h, 1);
     std::ofstream fED;
-    if (r == QP_OK && c.catching) {
+    if (r == QP_OK && (c.catching || c.dump_photons)) {
         int64_t total = 0, np = 0;
         for (int s2 = 0; s2 < n; s2++) { qp_count_particles(h, s2, &np); total += np; }
-        r = qp_set_erased_tracking(h, 1);
-        if (r == QP_OK) r = qp_set_catching(h, 1, std::max<int64_t>(total, 1 << 16));
+        const int64_t cap = std::max<int64_t>(total, 1 << 16);
+        if (c.catching) {
+            r = qp_set_erased_tracking(h, 1);
+            if (r == QP_OK) r = qp_set_catching(h, 1, cap);
+        }
+        if (r == QP_OK && c.dump_photons) r = qp_set_dump_photons(h, 1, cap);
         fED.open(c.data_folder + "/energy_deleted");
     }
     if (r != QP_OK) {
@@ -919,7 +924,7 @@ int main() {
         L << "particles_for_output\n" << c.particles_for_output << "\n";
         L << "enthp\n" << c.enthp << "\n";
         L << "n_sr\n1\n$\n";
-        L << "catching\noff\ndump_photons\noff\nqed\n" << (c.qed ? "on" : "off") << "\n";
+        L << "catching\noff\ndump_photons\n" << (c.dump_photons ? "on" : "off") << "\nqed\n" << (c.qed ? "on" : "off") << "\n";
         L << "balancing\noff\noutput_mode\n" << (c.binary ? 1 : 0) << "\n";
         L << "#------------------------------\n";
         L << "polarization = " << c.polarization << "\n";
@@ -1185,7 +1190,7 @@ int main() {
             nmw++;
         }
         if (c.mwindow) fMW << ((nmw - 1) * c.dx / 2 / PI) << std::endl;  // write_mwcoordinate
-        if (c.catching) {
+        if (c.catching || c.dump_photons) {
             // drain the device records (deletion order inside a species)
             int64_t m = 0, dropped = 0;
             qp_get_caught(h, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -1265,7 +1270,7 @@ int main() {
                           << gg[t] << '\n' << chi[t] << '\n';
                 }
             }
-            if (c.catching) {
+            if (c.catching || c.dump_photons) {
                 // write_deleted_particles (main.cpp:189-345): 9 values per
                 // written particle, the reference's every-n-th counters, and
                 // the deleted photons' spectrum; the list is then cleared

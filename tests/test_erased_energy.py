@@ -155,3 +155,61 @@ def test_catching_capacity_overflow_is_counted():
     c = r.get_caught()
     r.close()
     assert c["x"].size == 100 and c["dropped"] == m - 100
+
+
+def _qed_region(precision, with_photons):
+    """Electrons across a strong Bz (chi ~ 1) and, optionally, energetic
+    photons for pair creation, in the middle of a 16^3 box."""
+    from quill_b200.api import Region
+    from tests import test_qed as Q
+    fields, e, ph = Q._emission_case(0)
+    r = Region(Q.N, Q.N, Q.N, Q.DX, Q.DX, Q.DX, Q.DT, species_cmr=(-1.0, 1.0, 0.0), solver="fdtd", pusher="boris",
+               qed=True, seed=11, precision=precision)
+    r.set_fields(*[fields[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
+    r.init_boundaries()
+    if with_photons:
+        r.add_particles(2, Q._sort(ph))
+    else:
+        r.add_particles(0, Q._sort(e))
+    return r
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_dump_photons_records_every_emitted_photon(precision):
+    """dump_photons (advance.cpp:302-306): the photons the electrons emit are
+    deleted as they are born; each is recorded with its energy, which is the
+    photon species' erased energy; the photon species stays empty."""
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    r = _qed_region(precision, with_photons=False)
+    r.set_dump_photons(True)
+    total = 0.0
+    n_rec = 0
+    for _ in range(3):
+        d = r.step(1)[0]
+        c = r.get_caught()
+        assert np.all(c["species"] == 2)
+        n_rec += c["x"].size
+        assert d.energy_erased_sp[2] == pytest.approx(np.sum(c["g"] * c["q"]) * _b(), rel=1e-12, abs=0)
+        total += d.energy_erased_sp[2]
+    assert r.count(2) == 0 and n_rec > 100 and total > 0
+    assert r.count(0) > 0
+    r.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_pair_creation_is_not_an_erasure(precision):
+    """A photon that becomes a pair is deleted without a record
+    (delete_particle without force_delete inside the box): with catching on,
+    photons in the middle of the box make pairs and nothing is recorded."""
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    r = _qed_region(precision, with_photons=True)
+    r.set_erased_tracking(True)
+    r.set_catching(True)
+    n0 = r.count(2)
+    d = r.step(1)[0]
+    assert r.count(0) > 0 and r.count(2) < n0    # pairs were made
+    c = r.get_caught()
+    assert c["x"].size == 0 and d.energy_erased == 0.0
+    r.close()
