@@ -26,7 +26,9 @@
 // pmerging crpc mwindow (off | on | auto) mwtolerance mwspeed mwseed
 // mwseed_ions mw_mcr t_add_mw ne_profile_x_coords ne_profile_x_values
 // ne_profile_r_coords ne_profile_r_values nfilm_y0 nfilm_y1 gradwidth_y
-// nelflow vlflow mcrlflow Tlflow nerflow vrflow mcrrflow Trflow and two
+// nelflow vlflow mcrlflow Tlflow nerflow vrflow mcrrflow Trflow catching
+// dump_photons n_tracks particles_to_track tr_init tr_start xtr1 ytr1 ztr1
+// xtr2 ytr2 ztr2 deps deps_ph neps neps_ph enthp_p enthp_ph enthp_i and two
 // additions: precision (fp64 | mixed) and seed.
 #include <algorithm>
 #include <cmath>
@@ -158,6 +160,7 @@ struct Config {
     bool dump_photons = false;     // emitted photons deleted as they are born
     int n_tracks = 0;              // main.cpp:3408-3413
     std::string particles_to_track = "epgi";
+    bool tr_volume = false;        // tr_init = volume: n_tracks random cells in the box (main.cpp:1612-1690)
     double tr_start = 0, xtr1 = 0, ytr1 = 0, ztr1 = 0, xtr2 = 0, ytr2 = 0, ztr2 = 0;  // main.cpp:3419-3480
     double deps_ph = 0;            // MeV, photon spectrum bin (main.cpp:3337-3359)
     int neps_ph = 0;               // photon spectrum bins (main.cpp:3363-3370)
@@ -377,7 +380,7 @@ Config parse(const std::vector<Var>& v) {
     c.particles_to_track = find(v, "particles_to_track").units;
     if (c.particles_to_track.empty()) c.particles_to_track = "epgi";
     if (c.particles_to_track == "none") c.particles_to_track = "";
-    if (find(v, "tr_init").units == "volume") throw std::runtime_error("tr_init = volume is not part of this build");
+    c.tr_volume = find(v, "tr_init").units == "volume";  // main.cpp:3414-3418
     {
         const Var& ts = find(v, "tr_start");
         double tv = ts.value;
@@ -1030,14 +1033,25 @@ int main() {
             return QP_OK;
         }
         std::vector<int64_t> cells;
-        int x1 = -1, y1 = 0, z1 = 0;
-        for (int i = 0; i < c.n_tracks; i++) {
-            const int x2 = (int)((c.xtr1 + (c.xtr2 - c.xtr1) * i / c.n_tracks) / c.dx);
-            const int y2 = (int)((c.ytr1 + (c.ytr2 - c.ytr1) * i / c.n_tracks) / c.dy);
-            const int z2 = (int)((c.ztr1 + (c.ztr2 - c.ztr1) * i / c.n_tracks) / c.dz);
-            if (x2 != x1 || y2 != y1 || z2 != z1) {
-                x1 = x2; y1 = y2; z1 = z2;
-                cells.push_back(((int64_t)x2 * g.ny + y2) * g.nz + z2);
+        if (!c.tr_volume) {
+            int x1 = -1, y1 = 0, z1 = 0;
+            for (int i = 0; i < c.n_tracks; i++) {
+                const int x2 = (int)((c.xtr1 + (c.xtr2 - c.xtr1) * i / c.n_tracks) / c.dx);
+                const int y2 = (int)((c.ytr1 + (c.ytr2 - c.ytr1) * i / c.n_tracks) / c.dy);
+                const int z2 = (int)((c.ztr1 + (c.ztr2 - c.ztr1) * i / c.n_tracks) / c.dz);
+                if (x2 != x1 || y2 != y1 || z2 != z1) {
+                    x1 = x2; y1 = y2; z1 = z2;
+                    cells.push_back(((int64_t)x2 * g.ny + y2) * g.nz + z2);
+                }
+            }
+        } else {
+            // volume: a uniformly drawn cell of the box per track (the reference draws with rand())
+            std::uniform_real_distribution<double> U(0.0, 1.0);
+            for (int i = 0; i < c.n_tracks; i++) {
+                const int x1 = (int)((c.xtr1 + (c.xtr2 - c.xtr1) * U(rng)) / c.dx);
+                const int y1 = (int)((c.ytr1 + (c.ytr2 - c.ytr1) * U(rng)) / c.dy);
+                const int z1 = (int)((c.ztr1 + (c.ztr2 - c.ztr1) * U(rng)) / c.dz);
+                cells.push_back(((int64_t)x1 * g.ny + y1) * g.nz + z1);
             }
         }
         // kinds in the reference's order per cell: e, p, g, then every ion population
@@ -1056,7 +1070,12 @@ int main() {
         int64_t trn = 1;
         for (size_t cc = 0; cc < cells.size(); cc++)
             for (size_t k = 0; k < kinds.size(); k++)
-                if (first[k][cc] >= 0) { pos[k].push_back(first[k][cc]); num[k].push_back(trn++); }
+                if (first[k][cc] >= 0) {
+                    // a cell drawn again renumbers its first particle, as the reference overwrites trn
+                    auto it = std::find(pos[k].begin(), pos[k].end(), first[k][cc]);
+                    if (it != pos[k].end()) num[k][it - pos[k].begin()] = trn++;
+                    else { pos[k].push_back(first[k][cc]); num[k].push_back(trn++); }
+                }
         for (size_t k = 0; k < kinds.size(); k++) {
             const int rr = qp_set_track_numbers(h, kinds[k], (int64_t)pos[k].size(), pos[k].data(), num[k].data());
             if (rr != QP_OK) return rr;

@@ -280,6 +280,30 @@ def test_driver_tracks(tmp_path):
         assert np.all(np.abs(np.diff(rec[:, 1])) <= 0.5 * 0.0625 + 1e-12)
 
 
+@pytest.mark.gpu
+def test_driver_tracks_in_a_volume(tmp_path):
+    """tr_init = volume (start_tracking, main.cpp:1612-1690): n_tracks cells
+    drawn uniformly in the box [xtr1, xtr2] x [ytr1, ytr2] x [ztr1, ztr2];
+    the first electron of each gets the next track number (a cell drawn
+    twice renumbers it)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    folder = str(tmp_path / "results")
+    conf = CONF + [("n_tracks", "12", "#"), ("particles_to_track", "#", "e"), ("tr_start", "0", "lambda"),
+                   ("tr_init", "#", "volume"),
+                   ("xtr1", "1.1", "lambda"), ("ytr1", "0.5", "lambda"), ("ztr1", "0.5", "lambda"),
+                   ("xtr2", "1.4", "lambda"), ("ytr2", "1.0", "lambda"), ("ztr2", "1.0", "lambda")]
+    _run_driver(conf, folder)
+    files = sorted((f for f in os.listdir(folder) if f.startswith("track_-1_")), key=lambda f: int(f.split("_")[-1]))
+    nums = [int(f.split("_")[-1]) for f in files]
+    assert 6 <= len(nums) <= 12 and all(1 <= n_ <= 12 for n_ in nums) and len(set(nums)) == len(nums)
+    for f in files:
+        rec = np.array(open(os.path.join(folder, f)).read().split(), dtype=float).reshape(-1, 9)
+        assert np.all(rec[:, 0] < 0)
+        assert np.all((rec[:, 1] > 1.0) & (rec[:, 1] < 1.6))
+        assert np.all((rec[:, 2] > 0.4) & (rec[:, 2] < 1.1)) and np.all((rec[:, 3] > 0.4) & (rec[:, 3] < 1.1))
+
+
 def _slices(folder, name, t, nx, ny, nz):
     """The xy line at k = nz/2 and the xz line at j = ny/2 per i, then the
     yz plane (the field and density slice layout)."""
