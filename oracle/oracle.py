@@ -111,6 +111,11 @@ def _load(kind: str, flavour: str):
         api["optimal_partition"] = fn("optimal_partition", None, _DP, C.c_int, C.c_int, C.c_int, _IP)
         api["normalize_partition"] = fn("normalize_partition", None, _IP, _IP, C.c_int, C.c_int, _IP)
         api["partition_imbalance"] = fn("partition_imbalance", _D, _DP, C.c_int, _IP, C.c_int, C.c_int)
+        I = C.c_int
+        api["f_init_cos"] = fn("f_init_cos", None, C.c_void_p, _D, _D, _D, _D, _D, _D, I, I, _D, _D, _D, _D, I, _D,
+                               _D, _D, _D)
+        api["f_init_focused"] = fn("f_init_focused", None, C.c_void_p, _D, _D, _D, _D, _D, _D, I, _D, _D, _D, I, _D,
+                                   I, _D, _D, _D, _D)
     _LIBS[key] = api
     return api
 
@@ -289,6 +294,19 @@ class Region:
         arrs = [np.ascontiguousarray(parts[k] if parts.get(k) is not None else np.zeros(n), dtype=np.float64)
                 for k in PARTICLE_KEYS]
         self.api["replace_particle_slab"](self.h, i0, width, n, *[_dp(a) for a in arrs])
+
+    # --- initial pulses (reference only; the reference's argument order) ---
+    def f_init_cos(self, a0y, a0z, xsigma, ysigma, zsigma, x0, sscos, b_sign, x1, phase, y0, z0, append, phi,
+                   xtarget=0.0, ytarget=0.0, ztarget=0.0):
+        """f_init_cos (init.cpp:6-210)."""
+        self.api["f_init_cos"](self.h, a0y, a0z, xsigma, ysigma, zsigma, x0, int(sscos), int(b_sign), x1, phase,
+                               y0, z0, int(append), phi, xtarget, ytarget, ztarget)
+
+    def f_init_focused(self, a0y, a0z, xsigma, sigma0, x0, x1, b_sign, phase, y0, z0, append, phi, sscos, K,
+                       xtarget=0.0, ytarget=0.0, ztarget=0.0):
+        """f_init_focused (init.cpp:212-385)."""
+        self.api["f_init_focused"](self.h, a0y, a0z, xsigma, sigma0, x0, x1, int(b_sign), phase, y0, z0,
+                                   int(append), phi, int(sscos), K, xtarget, ytarget, ztarget)
 
     def layer_counts(self) -> np.ndarray:
         out = np.zeros(self.shape[0], dtype=np.int64)

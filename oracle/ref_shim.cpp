@@ -118,6 +118,23 @@ void qref_get_fields(void* h, double* out) {
             }
 }
 
+// The initial pulses: f_init_cos (init.cpp:6-210) and f_init_focused
+// (init.cpp:212-385) on the region's E and B, with the reference's argument
+// order.
+void qref_f_init_cos(void* h, double a0y, double a0z, double xsigma, double ysigma, double zsigma, double x0,
+                     int sscos, int b_sign, double x1, double phase, double y0, double z0, int append, double phi,
+                     double xtarget, double ytarget, double ztarget) {
+    ((RefRegion*)h)->sr.f_init_cos(a0y, a0z, xsigma, ysigma, zsigma, x0, sscos, b_sign != 0, x1, phase, y0, z0,
+                                   append != 0, phi, xtarget, ytarget, ztarget);
+}
+
+void qref_f_init_focused(void* h, double a0y, double a0z, double xsigma, double sigma0, double x0, double x1,
+                         int b_sign, double phase, double y0, double z0, int append, double phi, int sscos, double K,
+                         double xtarget, double ytarget, double ztarget) {
+    ((RefRegion*)h)->sr.f_init_focused(a0y, a0z, xsigma, sigma0, x0, x1, b_sign != 0, phase, y0, z0, append != 0,
+                                       phi, sscos, K, xtarget, ytarget, ztarget);
+}
+
 // f_init_boundaries + interpolate_be, as src/main.cpp:2288-2289
 void qref_init_boundaries(void* h) {
     RefRegion* r = (RefRegion*)h;

@@ -16,7 +16,8 @@
 //
 // Supported parameters: dx dy dz dt lambda ne xlength ylength zlength t_end
 // output_period a0 a0y a0z polarization xsigma ysigma zsigma x0 y0 z0 phase
-// f_envelope (cos | sscos | pearl | tophat | uniformB) phi_rotate r0 theta
+// f_envelope (cos | sscos | pearl | tophat | uniformB | focused |
+// focussedSSC) shenergy shphase phi_rotate r0 theta
 // xtarget ytarget ztarget lp_reflection f_reflection beam beam_particles Nb
 // epsb xb rb x0b y0b phib
 // b_sign phi external_bz solver pusher qed film x0film filmwidth gradwidth
@@ -30,6 +31,12 @@
 // dump_photons n_tracks particles_to_track tr_init tr_start xtr1 ytr1 ztr1
 // xtr2 ytr2 ztr2 deps deps_ph neps neps_ph enthp_p enthp_ph enthp_i and two
 // additions: precision (fp64 | mixed) and seed.
+//
+//   qp_driver --initial-fields <file>
+//
+// stops after the initial fields (laser and beam fields, before any GPU
+// work) and writes them to <file>: Ex Ey Ez Bx By Bz, each nx*ny*nz doubles
+// with k fastest.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -127,6 +134,9 @@ struct Config {
     double a0y = 0, a0z = 0, xsigma = 0, ysigma = 0, zsigma = 0, x0 = 0, y00 = 0, z00 = 0, phase = 0, phi = 0;
     int sscos = 0;                 // f_envelope: cos 0, sscos 1, pearl 2, tophat 3 (main.cpp:2811-2825)
     bool uniform_b = false;        // f_envelope = uniformB (init.cpp:387-400)
+    bool focused = false;          // f_envelope = focused / focussedSSC (main.cpp:2906-2925)
+    double sigma0 = 0;             // focused: the waist, (ysigma + zsigma) / 2
+    double shenergy = 0, shphase = 0;  // focused: second-harmonic energy share and phase (main.cpp:2926-2931)
     double phi_rotate = 0, xtarget = 0, ytarget = 0, ztarget = 0;  // main.cpp:2835-2899
     std::string lp_reflection = "off", f_reflection = "off";        // main.cpp:3402-3407
     bool beam = false;             // main.cpp:2988-3053
@@ -231,14 +241,16 @@ Config parse(const std::vector<Var>& v) {
     c.phase = ph.units == "pi" ? ph.value * PI : ph.value;
     c.b_sign = find(v, "b_sign").value != -1;
     const Var& phi = find(v, "phi");
-    c.phi = phi.units == "deg" ? phi.value * PI / 180 : phi.value;
+    c.phi = phi.units == "pi" ? phi.value * PI : phi.value;
     const std::string env = find(v, "f_envelope").units;
     if (env.empty() || env == "cos") c.sscos = 0;
     else if (env == "sscos") c.sscos = 1;
     else if (env == "pearl") c.sscos = 2;
     else if (env == "tophat") c.sscos = 3;
     else if (env == "uniformB") c.uniform_b = true;
-    else throw std::runtime_error("f_envelope " + env + " is not part of this build (cos, sscos, pearl, tophat, uniformB)");
+    else if (env == "focused") c.focused = true;
+    else if (env == "focussedSSC") { c.focused = true; c.sscos = 1; }
+    else throw std::runtime_error("f_envelope " + env + " is not part of this build (cos, sscos, pearl, tophat, uniformB, focused, focussedSSC)");
     const Var& phr = find(v, "phi_rotate");
     c.phi_rotate = phr.units == "pi" ? phr.value * PI : phr.value;
     // the pulse position as (r0, theta) (main.cpp:2850-2867)
@@ -258,6 +270,18 @@ Config parse(const std::vector<Var>& v) {
     c.xtarget = target("xtarget");
     c.ytarget = target("ytarget");
     c.ztarget = target("ztarget");
+    if (c.focused) {
+        // the waist from the transverse sizes; the amplitude is given at the
+        // focus and scaled to the pulse's starting distance from it
+        const double x00 = std::sqrt(c.x0 * c.x0 + c.y00 * c.y00 + c.z00 * c.z00);
+        c.sigma0 = 0.5 * (c.ysigma + c.zsigma);
+        const double sigma = std::sqrt(c.sigma0 * c.sigma0 + 4 * x00 * x00 / (c.sigma0 * c.sigma0));
+        c.a0y = c.a0y * c.sigma0 / sigma;
+        c.a0z = c.a0z * c.sigma0 / sigma;
+    }
+    c.shenergy = find(v, "shenergy").value;
+    const Var& shp = find(v, "shphase");
+    c.shphase = shp.units == "pi" ? shp.value * PI : shp.value;
     c.lp_reflection = find(v, "lp_reflection").units;
     if (c.lp_reflection.empty()) c.lp_reflection = "off";
     c.f_reflection = find(v, "f_reflection").units;
@@ -508,6 +532,106 @@ void laser_cos(const Config& c, const Grid3& g, std::vector<double>* F, double a
             }
 }
 
+// f_init_focused with append = true (init.cpp:212-385): a pulse focused to
+// the waist sigma0, whose centre (x1, y0, z0) lies at distance L from the
+// focus on its axis r0; K is the harmonic (1, or 2 for the second harmonic).
+// xi is the phase coordinate along the axis with the wavefront curvature and
+// the Gouy phase; slocal the beam radius there.  Inside |xi| < xs and r <
+// slocal the envelope is cos^2 (sscos 0, only within the cone r <= 2 s0
+// (x1 - x) / xR, outside of which the paraxial fields have unphysical
+// wings) or super-cosine^2 in xi (sscos 1), times cos^2 (pi r / 2 slocal);
+// E_x and B_x follow from the transverse derivatives of the envelope.  The
+// scalar chain up to the envelope tests keeps the reference's operation
+// order, so that every cell falls on the same side of each test.
+void laser_focused(const Config& c, const Grid3& g, std::vector<double>* F, double a0y, double a0z, double xc,
+                   double x1, double y0, double z0, double phase, double phi, double K) {
+    const double sign = (x1 <= 0) - (x1 > 0);
+    x1 = std::sqrt(x1 * x1 + y0 * y0 + z0 * z0);
+    if (x1 == 0) x1 = c.dx;  // the pulse axis needs a direction
+    const double sigma0 = c.sigma0;
+    const double xR = K * sigma0 * sigma0 / 2;
+    const double sigma = sigma0 * std::sqrt(1 + x1 * x1 / xR / xR);
+    // the first harmonic's beam radius over this harmonic's at the start
+    const double amul = std::sqrt(1 + x1 * x1 / (sigma0 * sigma0 * sigma0 * sigma0 / 4)) /
+                        std::sqrt(1 + x1 * x1 / (xR * xR));
+    const double xs = c.sscos == 1 ? 0.822 * c.xsigma : c.xsigma * 2 * std::sqrt(2 * PI) / 3;
+    const double sn = std::sqrt(((double)3) / 16 - 1 / PI / PI);
+    const double s = sigma / 2 / sn, s0 = sigma0 / 2 / sn;
+    const double y12 = g.ny * c.dy / 2, z12 = g.nz * c.dz / 2;
+    const double r0x = sign * std::sqrt(x1 * x1 - y0 * y0 - z0 * z0) / x1, r0y = -y0 / x1, r0z = -z0 / x1;
+    double y0x, y0y, y0z = std::sqrt(r0x * r0x + r0y * r0y);
+    if (y0z != 0) { y0x = -r0y / y0z; y0y = r0x / y0z; y0z = 0; }
+    else { y0x = 0; y0y = 1; y0z = 0; }
+    double z0x = r0y * y0z - r0z * y0y, z0y = r0z * y0x - r0x * y0z, z0z = r0x * y0y - r0y * y0x;
+    if (phi != 0) {
+        const double cs = std::cos(phi), ss = std::sin(phi);
+        const double yx = y0x, yy = y0y, yz = y0z, zx = z0x, zy = z0y, zz = z0z;
+        y0x = yx * cs + zx * ss; y0y = yy * cs + zy * ss; y0z = yz * cs + zz * ss;
+        z0x = zx * cs - yx * ss; z0y = zy * cs - yy * ss; z0z = zz * cs - yz * ss;
+    }
+    const double gouy0 = std::atan(x1 / xR);
+    const double xs4 = xs * xs * xs * xs;
+    for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+            for (int k = 0; k < g.nz; k++) {
+                const double X = i * c.dx - xc - c.xtarget, Y = j * c.dy - y12 - y0 - c.ytarget,
+                             Z = k * c.dz - z12 - z0 - c.ztarget;
+                const double x = r0x * X + r0y * Y + r0z * Z;
+                const double r = std::sqrt(X * X + Y * Y + Z * Z - x * x);
+                const double xi = x + r * r / 2 * (x - x1) / ((x - x1) * (x - x1) + xR * xR) - std::atan((x - x1) / xR) - gouy0;
+                const double w = xi - x1 + gouy0;
+                const double slocal = s0 * std::sqrt(1 + w * w / (xR * xR));
+                const double alocal = s / slocal * amul;
+                if (!(xi > -xs && xi < xs && r < slocal)) continue;
+                double ex = 0, ey = 0, ez = 0, bx = 0, by = 0, bz = 0;
+                // longitudinal envelope cx = cos(ax), its derivative factor D:
+                // d(cx^2)/dxi = -2 D cx sx
+                double ax = 0, D = 0;
+                bool lit = true;
+                if (c.sscos == 1) {
+                    ax = PI * xi * xi * xi * xi / 2 / xs4;
+                    D = 4 * PI * xi * xi * xi / xs4;
+                } else if (-2 * s0 * (x1 - x) / xR <= r && r <= 2 * s0 * (x1 - x) / xR) {
+                    ax = PI * xi / 2 / xs;
+                    D = PI / xs;
+                } else {
+                    lit = false;
+                }
+                if (lit) {
+                    const double cx = std::cos(ax), sx = std::sin(ax);
+                    const double ar = PI * r / 2 / slocal;
+                    const double cr = std::cos(ar), sr = std::sin(ar);
+                    const double psi = K * xi + phase, cp = std::cos(psi), sp = std::sin(psi);
+                    const double C = cr * cr, cxx = cx * cx, cxs = cx * sx;
+                    // the phase-envelope combinations of the field formulas
+                    const double P = K * sp * cxx + D * cp * cxs;
+                    const double Q = K * cp * cxx - D * sp * cxs;
+                    const double Rr = K * cp * cxx + D * sp * cxs;
+                    const double Ay = alocal * a0y / K, Az = alocal * a0z / K;
+                    ey = Ay * C * Q;
+                    ez = -Az * C * P;
+                    bz = ey;
+                    by = -ez;
+                    if (r != 0) {
+                        // projections on the polarisation axes, the curvature factor
+                        const double Ly = X * y0x + Y * y0y + Z * y0z, Lz = X * z0x + Y * z0y + Z * z0z;
+                        const double G = (x - x1) / ((x - x1) * (x - x1) + xR * xR);
+                        const double T = cr * sr * PI / slocal / r;
+                        ex = Ay * (T * Ly * P - Ly * G * C * Q) - Az * (-T * Lz * Rr - Lz * G * C * P);
+                        bx = Ay * (T * Lz * P - Lz * G * C * Q) + Az * (-T * Ly * Rr - Ly * G * C * P);
+                    }
+                }
+                if (!c.b_sign) { bx = -bx; by = -by; bz = -bz; }
+                const long a = g.at(i, j, k);
+                F[0][a] += ex * r0x + ey * y0x + ez * z0x;
+                F[1][a] += ex * r0y + ey * y0y + ez * z0y;
+                F[2][a] += ex * r0z + ey * y0z + ez * z0z;
+                F[3][a] += bx * r0x + by * y0x + bz * z0x;
+                F[4][a] += bx * r0y + by * y0y + bz * z0y;
+                F[5][a] += bx * r0z + by * y0z + bz * z0z;
+            }
+}
+
 struct Parts {
     std::vector<double> x, y, z, ux, uy, uz, g, q;
     void add(double X, double Y, double Z, double UX, double UY, double UZ, double G, double Q) {
@@ -717,8 +841,13 @@ void write_slice(const std::string& path, const double* F, const Grid3& g, int i
 
 }  // namespace
 
-int main() {
+int main(int argc, char** argv) {
     std::ios::sync_with_stdio(false);
+    std::string initial_fields;  // --initial-fields <file>: write the initial E, B and stop
+    for (int a = 1; a < argc; a++) {
+        if (std::string(argv[a]) == "--initial-fields" && a + 1 < argc) initial_fields = argv[++a];
+        else { std::cerr << "usage: qp_driver [--initial-fields <file>] < parsed-input" << std::endl; return 2; }
+    }
     Config c;
     try {
         c = parse(read_stream(std::cin));
@@ -769,11 +898,6 @@ int main() {
     if (c.ions == "positrons" || c.qed || (c.beam && c.beam_particles == "p")) { sp_pos = n; p.cmr[n++] = 1; }
     if (c.qed || (c.beam && c.beam_particles == "ph")) { sp_ph = n; p.cmr[n++] = 0; }
     p.n_species = n;
-    qp_handle* h = nullptr;
-    if (qp_create(&p, &h) != QP_OK) {
-        std::cerr << "qp_driver: " << qp_last_error(nullptr) << std::endl;
-        return 1;
-    }
 
     // initial fields: the default call of init_fields (main.cpp:1186-1189),
     // plus the counter-propagating pulse for phi != 0 (main.cpp:1190-1192)
@@ -783,8 +907,9 @@ int main() {
         // f_init_uniformB (init.cpp:387-400)
         for (long a = 0; a < g.nc(); a++) { F[4][a] = c.a0y; F[5][a] = c.a0z; }
     } else if (c.a0y != 0 || c.a0z != 0) {
-        // init_fields, cos branch (main.cpp:1136-1229): the pulse, its
-        // counter-propagating copy for phi != 0, or its mirror images
+        // init_fields (main.cpp:1041-1229): the pulse, its
+        // counter-propagating copy for phi != 0, or its mirror images; the
+        // cos and focused branches place their pulses the same way
         const double A = c.a0y, Z = c.a0z, x0 = c.x0, y0 = c.y00, z0 = c.z00, xl = c.xlength / 2;
         auto split = [](const std::string& s) {
             std::vector<std::string> p(3);
@@ -796,12 +921,20 @@ int main() {
         auto sy = [&](int m) { return (1 - 2 * (fr[m] == "y")) * A; };
         auto sz = [&](int m) { return (1 - 2 * (fr[m] == "z")) * Z; };
         auto P = [&](double ay, double az, double xc, double x1, double yy, double zz, double ph) {
-            laser_cos(c, g, F, ay, az, xc, x1, yy, zz, ph);
+            if (c.focused) laser_focused(c, g, F, ay, az, xc, x1, yy, zz, c.phase, ph, 1);
+            else laser_cos(c, g, F, ay, az, xc, x1, yy, zz, ph);
         };
-        if (c.phi_rotate != 0) {
+        if (c.focused && c.shenergy != 0) {
+            // the second harmonic takes the share shenergy of the energy
+            const double al = std::sqrt(1 - c.shenergy), be = std::sqrt(c.shenergy);
+            laser_focused(c, g, F, A * al, Z * al, xl + x0, x0, y0, z0, c.phase, 0, 1);
+            laser_focused(c, g, F, A * be, Z * be, xl + x0, x0, y0, z0, c.shphase, 0, 2);
+        } else if (!c.focused && c.phi_rotate != 0) {
             P(A, Z, xl + x0, x0, y0, z0, c.phi_rotate);
         } else {
             P(A, Z, xl + x0, x0, y0, z0, 0);
+        }
+        if (c.focused || c.phi_rotate == 0) {  // (a rotated cos pulse has no copies)
             if (c.phi != 0) {
                 P(A, Z, xl - x0, -x0, -y0, -z0, c.phi);
             } else if (lp[0] == "xy") {
@@ -852,6 +985,16 @@ int main() {
             sp_beam = c.beam_particles == "p" ? sp_pos : sp_e;
             add_beam(c, g, F, B, c.beam_particles == "p" ? 1 : -1, n0, u0, x0b, rng);
         }
+    }
+    if (!initial_fields.empty()) {
+        std::ofstream o(initial_fields, std::ios::binary);
+        for (auto& f : F) o.write(reinterpret_cast<const char*>(f.data()), (std::streamsize)(f.size() * sizeof(double)));
+        return o ? 0 : 1;
+    }
+    qp_handle* h = nullptr;
+    if (qp_create(&p, &h) != QP_OK) {
+        std::cerr << "qp_driver: " << qp_last_error(nullptr) << std::endl;
+        return 1;
     }
     int r = qp_load_fields(h, F[0].data(), F[1].data(), F[2].data(), F[3].data(), F[4].data(), F[5].data());
     if (r == QP_OK) r = qp_init_boundaries(h);

@@ -352,6 +352,151 @@ def test_driver_laser_envelopes_and_uniform_b(tmp_path):
     np.testing.assert_allclose(bz[2:-2, 2:-2], 3.0, rtol=1e-12)
 
 
+def _split3(s):
+    p = ["", "", ""]
+    k = 0
+    for ch in s:
+        if ch == "&":
+            k += 1
+            if k == 3:
+                break
+        else:
+            p[k] += ch
+    return p
+
+
+def _reference_initial_fields(q, shape):
+    """init_fields (main.cpp:1041-1229) for one region (x0_sr = 0), calling
+    the reference's own f_init_cos / f_init_focused; q holds the parameters
+    in c/omega units after main.cpp's input handling (the focused waist and
+    amplitude of main.cpp:2906-2925 included)."""
+    from oracle import oracle
+    nx, ny, nz = shape
+    reg = oracle.Region(nx, ny, nz, q["dx"], q["dy"], q["dz"], q["dt"], kind="ref")
+    A, Z, x0, y0, z0 = q["a0y"], q["a0z"], q["x0"], q["y0"], q["z0"]
+    xl = q["xlength"] / 2
+    tg = (q["xt"], q["yt"], q["zt"])
+    lp, fr = _split3(q["lp"]), _split3(q["fr"])
+    sy = lambda m: (1 - 2 * (fr[m] == "y")) * A
+    sz = lambda m: (1 - 2 * (fr[m] == "z")) * Z
+    if q["focused"]:
+        def P(ay, az, xc, x1, yy, zz, append, phi, phase=q["phase"], K=1):
+            reg.f_init_focused(ay, az, q["xsigma"], q["sigma0"], xc, x1, q["b_sign"], phase, yy, zz, append, phi,
+                               q["sscos"], K, *tg)
+    else:
+        def P(ay, az, xc, x1, yy, zz, append, phi):
+            reg.f_init_cos(ay, az, q["xsigma"], q["ysigma"], q["zsigma"], xc, q["sscos"], q["b_sign"], x1,
+                           q["phase"], yy, zz, append, phi, *tg)
+    if not q["focused"] and q["phi_rotate"] != 0:
+        P(A, Z, xl + x0, x0, y0, z0, 1, q["phi_rotate"])
+    else:
+        if q["focused"] and q["sh"] != 0:
+            al, be = np.sqrt(1 - q["sh"]), np.sqrt(q["sh"])
+            P(A * al, Z * al, xl + x0, x0, y0, z0, 0, 0)
+            P(A * be, Z * be, xl + x0, x0, y0, z0, 1, 0, phase=q["shphase"], K=2)
+        else:
+            P(A, Z, xl + x0, x0, y0, z0, 0 if q["focused"] else 1, 0)
+        if q["phi"] != 0:
+            P(A, Z, xl - x0, -x0, -y0, -z0, 1, q["phi"])
+        elif lp[0] == "xy":
+            P(sy(0), sz(0), xl + x0, x0, y0, -z0, 1, 0)
+            if lp[1] == "xz":
+                P(sy(1), sz(1), xl + x0, x0, -y0, z0, 1, 0)
+                P(sy(1), sz(1), xl + x0, x0, -y0, -z0, 1, 0)
+                if lp[2] == "yz":
+                    for yy, zz in ((y0, z0), (y0, -z0), (-y0, z0), (-y0, -z0)):
+                        P(sy(2), sz(1), xl - x0, -x0, yy, zz, 1, 0)
+            elif lp[1] == "yz":
+                P(sy(1), sz(1), xl - x0, -x0, y0, z0, 1, 0)
+                P(sy(1), sz(1), xl - x0, -x0, y0, -z0, 1, 0)
+                if lp[2] == "xz":
+                    P(sy(2), sz(1), xl - x0, -x0, -y0, z0, 1, 0)
+                    P(sy(2), sz(1), xl + x0, x0, -y0, z0, 1, 0)
+                    P(sy(2), sz(1), xl - x0, -x0, -y0, -z0, 1, 0)
+                    P(sy(2), sz(1), xl + x0, x0, -y0, -z0, 1, 0)
+        elif lp[0] == "xz":
+            P(sy(0), sz(0), xl + x0, x0, -y0, z0, 1, 0)
+            if lp[1] == "yz":
+                P(sy(1), sz(1), xl - x0, -x0, -y0, z0, 1, 0)
+                P(sy(1), sz(1), xl - x0, -x0, y0, z0, 1, 0)
+        elif lp[0] == "yz":
+            P(sy(0), sz(0), xl - x0, -x0, y0, z0, 1, 0)
+    out = reg.get_fields()[:6].reshape(6, nx, ny, nz)
+    reg.close()
+    return out
+
+
+_PULSES = {  # extra records over CONF (lengths in lambda, as the records give them)
+    "cos": [],
+    "sscos": [("f_envelope", "#", "sscos")],
+    "pearl": [("f_envelope", "#", "pearl")],
+    "tophat": [("f_envelope", "#", "tophat")],
+    "cos_oblique_circular_phi": [("polarization", "#", "circular"), ("y0", "0.15", "lambda"),
+                                 ("z0", "-0.1", "lambda"), ("phi", "0.25", "pi"), ("phase", "0.3", "pi")],
+    "cos_reflections": [("y0", "0.15", "lambda"), ("z0", "0.1", "lambda"), ("lp_reflection", "#", "xy&xz&yz"),
+                        ("f_reflection", "#", "y&z&y")],
+    "cos_rotated_target": [("phi_rotate", "0.25", "pi"), ("xtarget", "0.1", "lambda"),
+                           ("ytarget", "-0.05", "lambda"), ("b_sign", "-1", "#")],
+    "focused": [("f_envelope", "#", "focused")],
+    "focussedSSC": [("f_envelope", "#", "focussedSSC")],
+    "focused_second_harmonic": [("f_envelope", "#", "focused"), ("shenergy", "0.2", "#"),
+                                ("shphase", "0.5", "pi"), ("a0z", "2", "#"), ("a0y", "4", "#")],
+    "focused_oblique_reflections": [("f_envelope", "#", "focused"), ("y0", "0.2", "lambda"),
+                                    ("z0", "-0.1", "lambda"), ("lp_reflection", "#", "xy&yz&xz"),
+                                    ("f_reflection", "#", "z&y&z")],
+    "focused_phi_target": [("f_envelope", "#", "focused"), ("phi", "0.5", "pi"), ("ztarget", "0.05", "lambda"),
+                           ("polarization", "#", "circular")],
+}
+
+
+@pytest.mark.parametrize("name", list(_PULSES))
+def test_driver_initial_pulses_match_reference(tmp_path, name):
+    """The driver's initial fields (qp_driver --initial-fields, no GPU
+    needed) equal the reference's own f_init_cos / f_init_focused, called in
+    init_fields' order, for every envelope, oblique incidence, the
+    counter-propagating copy, mirror images, rotation, targets and the
+    second harmonic."""
+    from oracle import oracle
+    if not oracle.available("ref"):
+        pytest.skip("reference library not built (make -C oracle ref)")
+    from quill_b200 import build
+    build.build()
+    extra = _PULSES[name]
+    keys = {k for k, _, _ in extra}
+    conf = [c for c in CONF if c[0] not in keys] + extra
+    out = str(tmp_path / "fields.bin")
+    r = subprocess.run([DRIVER, "--initial-fields", out], input=stream(conf, str(tmp_path / "res")), text=True,
+                       capture_output=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    shape = (32, 24, 24)
+    drv = np.fromfile(out).reshape((6,) + shape)
+    # values are read in float precision, as the reference's stof does (low-level.cpp:414)
+    rec = {k: (float(np.float32(v)) if v != "#" else 0.0, u) for k, v, u in conf}
+    L = lambda k: rec[k][0] * 2 * np.pi if k in rec else 0.0
+    ang = lambda k: (rec[k][0] * (np.pi if rec[k][1] == "pi" else 1.0)) if k in rec else 0.0
+    env = rec.get("f_envelope", (0.0, ""))[1]
+    a0y = rec["a0y"][0] if "a0y" in rec else rec["a0"][0]
+    a0z = rec["a0z"][0] if "a0z" in rec else (a0y if rec.get("polarization", (0.0, ""))[1] == "circular" else 0.0)
+    q = dict(dx=L("dx"), dy=L("dy"), dz=L("dz"), dt=L("dt"),
+             xlength=L("xlength"), xsigma=L("xsigma"), ysigma=L("ysigma"), zsigma=L("zsigma"),
+             x0=L("x0"), y0=L("y0"), z0=L("z0"), xt=L("xtarget"), yt=L("ytarget"), zt=L("ztarget"),
+             a0y=a0y, a0z=a0z, phase=ang("phase"), phi=ang("phi"), phi_rotate=ang("phi_rotate"),
+             b_sign=0 if rec.get("b_sign", (0.0,))[0] == -1 else 1,
+             lp=rec.get("lp_reflection", (0.0, "off"))[1], fr=rec.get("f_reflection", (0.0, "off"))[1],
+             focused=env in ("focused", "focussedSSC"),
+             sscos={"sscos": 1, "pearl": 2, "tophat": 3, "focussedSSC": 1}.get(env, 0),
+             sh=rec["shenergy"][0] if "shenergy" in rec else 0.0, shphase=ang("shphase"))
+    if q["focused"]:
+        x00 = np.sqrt(q["x0"] ** 2 + q["y0"] ** 2 + q["z0"] ** 2)
+        q["sigma0"] = 0.5 * (q["ysigma"] + q["zsigma"])
+        sigma = np.sqrt(q["sigma0"] ** 2 + 4 * x00 * x00 / q["sigma0"] ** 2)
+        q["a0y"] *= q["sigma0"] / sigma
+        q["a0z"] *= q["sigma0"] / sigma
+    ref = _reference_initial_fields(q, shape)
+    assert np.abs(ref).max() > 0.1
+    np.testing.assert_allclose(drv, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
 @pytest.mark.gpu
 def test_driver_reflected_pulses(tmp_path):
     """lp_reflection = xy (init_fields, main.cpp:1153-1229) adds the pulse's
