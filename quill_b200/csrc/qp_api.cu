@@ -329,6 +329,12 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.field_elem = s.fp64 ? 8 : 4;
     if (const char* mb = getenv("QP_PUSH_MINBLOCKS")) s.push_minblocks = atoi(mb) == 2 ? 2 : (atoi(mb) == 4 ? 4 : 3);
     if (const char* mb = getenv("QP_PUSH_MINBLOCKS_MIXED")) s.push_minblocks_mixed = atoi(mb) == 4 ? 4 : 3;
+    if (const char* w = getenv("QP_PUSH_WAVES")) s.push_waves = atoi(w) > 0 ? atoi(w) : 0;
+    {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device) == cudaSuccess && sms > 0)
+            s.sm_count = sms;
+    }
     cudaError_t e = cudaSetDevice(p.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;

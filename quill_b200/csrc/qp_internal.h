@@ -135,6 +135,12 @@ struct State {
     int push_minblocks = 3;
     // the same for the mixed push (3 or 4; QP_PUSH_MINBLOCKS_MIXED)
     int push_minblocks_mixed = 3;
+    // grid of the mixed non-QED push: at most push_waves x (SMs x CTAs per
+    // SM) blocks striding over the particles (QP_PUSH_WAVES; 0: one thread
+    // per particle).  The FP64 push keeps one thread per particle: its
+    // loop form measured slower.
+    int push_waves = 16;
+    int sm_count = 148;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
     // diagnostics + J reset)
@@ -164,6 +170,14 @@ struct State {
         int64_t step_index = 0;
     } snap[4];
 };
+
+// Blocks of 256 threads for a grid-stride push over n particles.
+inline int push_blocks(const State& s, int64_t n, int minb) {
+    const int64_t full = (n + 255) / 256;
+    if (s.push_waves <= 0) return (int)full;
+    const int64_t cap = (int64_t)s.sm_count * minb * s.push_waves;
+    return (int)(full < cap ? full : cap);
+}
 
 // Device copy of the full state into a snapshot / back (qp_checkpoint,
 // qp_restore, the adjoint's checkpoints); snapshot_free releases one.

@@ -32,88 +32,91 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
     return r;
 }
 
-// One thread per particle in traversal order (see k_push64): the move runs in
-// the particle's cell frame (offsets in [0, 1)), the current through the
-// warp's segment-slot run reduction (deposit_runs).
+// The particles in traversal order as k_push64 takes them, but with a grid of
+// a few waves striding over block-sized chunks: the diagnostics are summed
+// per thread over its chunks and block-reduced once, which measured 17 %
+// faster than one thread per particle (the FP64 kernel in this form measured
+// slower).  The move runs in the particle's cell frame (offsets in [0, 1)),
+// the current through the warp's segment-slot run reduction (deposit_runs).
 template <int PUSHER, int KIND, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs32 a) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    double dq = 0.0, de = 0.0;
+    double dq = 0.0, de = 0.0, er = 0.0;
     unsigned long long dc = 0;
-    int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
-    bool nc_owned = true;
-    bool live = false, active = false;
-    float o[3] = {0.f, 0.f, 0.f}, d[3] = {0.f, 0.f, 0.f};
-    float ux = 0.f, uy = 0.f, uz = 0.f, gm = 1.f, q = 0.f;
-    if (s < a.n) {
-        p = perm[s];
-        const int c0 = src.cell[p];
-        i0 = g.div_nynz.div(c0);
-        const int r0 = c0 - i0 * g.nynz;
-        j0 = g.div_nz.div(r0);
-        k0 = r0 - j0 * g.nz;
-        o[0] = src.ox[p]; o[1] = src.oy[p]; o[2] = src.oz[p];
-        ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
-        q = src.q[p];
-        live = !kill_layer(g, i0, j0, k0);
-        if (live) {
-            float E[3], B[3];
-            gather(f, g, i0, j0, k0, o[0], o[1], o[2], E, B);
-            B[2] += a.ext_bz;
-            if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
-            const float t = a.dt / gm;
-            d[0] = ux * t * a.idx; d[1] = uy * t * a.idy; d[2] = uz * t * a.idz;
-            if (KIND == KIND_PHOTON) {
-                o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
-            } else {
-                active = true;
-            }
-            if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
-        }
-    }
-    deposit_runs(f, g, o, d, q, i0, j0, k0, active, a.status);
-    if (s < a.n) {
-        int i1 = i0, j1 = j0, k1 = k0;
-        if (live) {
-            int si, sj, sk;
-            o[0] = wrap_offset(o[0], si);
-            o[1] = wrap_offset(o[1], sj);
-            o[2] = wrap_offset(o[2], sk);
-            i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
-            const bool moved = si | sj | sk;
-            if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
-        }
-        newcell[s] = nc;
-        // an erasure in the exchange area of an x-slab is not one of the whole box (delete_particle,
-        // low-level.cpp:247-259): only erasures inside [dlo, dhi) are caught and counted
-        if (nc < 0 && !(i1 >= a.dlo && i1 < a.dhi)) nc_owned = false;
-        if (nc < 0 && a.cat && nc_owned)
-            catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, (double)i1 + (double)o[0], (double)j1 + (double)o[1],
-                           (double)k1 + (double)o[2], ux, uy, uz, gm, q, src.chi ? (double)src.chi[p] : 0.0);
-        if (nc >= 0) {
-            dst.cell[s] = nc;
-            dst.ox[s] = o[0]; dst.oy[s] = o[1]; dst.oz[s] = o[2];
-            dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
-            dst.g[s] = gm; dst.q[s] = q;
-            if (dst.chi) dst.chi[s] = src.chi[p];
-            if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
-            if (i1 >= a.dlo && i1 < a.dhi) {
-                dq = (double)q;
-                de = KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
-                dc = 1;
+    for (int base = blockIdx.x * blockDim.x; base < a.n; base += gridDim.x * blockDim.x) {
+        const int s = base + threadIdx.x;
+        int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+        bool nc_owned = true;
+        bool live = false, active = false;
+        float o[3] = {0.f, 0.f, 0.f}, d[3] = {0.f, 0.f, 0.f};
+        float ux = 0.f, uy = 0.f, uz = 0.f, gm = 1.f, q = 0.f;
+        if (s < a.n) {
+            p = perm[s];
+            const int c0 = src.cell[p];
+            i0 = g.div_nynz.div(c0);
+            const int r0 = c0 - i0 * g.nynz;
+            j0 = g.div_nz.div(r0);
+            k0 = r0 - j0 * g.nz;
+            o[0] = src.ox[p]; o[1] = src.oy[p]; o[2] = src.oz[p];
+            ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
+            q = src.q[p];
+            live = !kill_layer(g, i0, j0, k0);
+            if (live) {
+                float E[3], B[3];
+                gather(f, g, i0, j0, k0, o[0], o[1], o[2], E, B);
+                B[2] += a.ext_bz;
+                if (KIND != KIND_PHOTON) push<PUSHER>(a.cmr, ux, uy, uz, gm, E, B, a.dt);
+                const float t = a.dt / gm;
+                d[0] = ux * t * a.idx; d[1] = uy * t * a.idy; d[2] = uz * t * a.idz;
+                if (KIND == KIND_PHOTON) {
+                    o[0] += d[0]; o[1] += d[1]; o[2] += d[2];
+                } else {
+                    active = true;
+                }
+                if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
             }
         }
+        deposit_runs(f, g, o, d, q, i0, j0, k0, active, a.status);
+        if (s < a.n) {
+            int i1 = i0, j1 = j0, k1 = k0;
+            if (live) {
+                int si, sj, sk;
+                o[0] = wrap_offset(o[0], si);
+                o[1] = wrap_offset(o[1], sj);
+                o[2] = wrap_offset(o[2], sk);
+                i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
+                const bool moved = si | sj | sk;
+                if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
+            }
+            newcell[s] = nc;
+            // an erasure in the exchange area of an x-slab is not one of the whole box (delete_particle,
+            // low-level.cpp:247-259): only erasures inside [dlo, dhi) are caught and counted
+            if (nc < 0 && !(i1 >= a.dlo && i1 < a.dhi)) nc_owned = false;
+            if (nc < 0 && a.cat && nc_owned)
+                catch_particle(*a.cat, a.sp, a.step, live ? 1 : 0, s, (double)i1 + (double)o[0], (double)j1 + (double)o[1],
+                               (double)k1 + (double)o[2], ux, uy, uz, gm, q, src.chi ? (double)src.chi[p] : 0.0);
+            if (nc >= 0) {
+                dst.cell[s] = nc;
+                dst.ox[s] = o[0]; dst.oy[s] = o[1]; dst.oz[s] = o[2];
+                dst.ux[s] = ux; dst.uy[s] = uy; dst.uz[s] = uz;
+                dst.g[s] = gm; dst.q[s] = q;
+                if (dst.chi) dst.chi[s] = src.chi[p];
+                if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
+                if (i1 >= a.dlo && i1 < a.dhi) {
+                    dq += (double)q;
+                    de += KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
+                    dc += 1;
+                }
+            }
+            // energy of the particles erased in this push
+            if (a.track && nc < 0 && nc_owned)
+                er += KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
+        }
+        warp_count_runs(count, nc);
     }
-    warp_count_runs(count, nc);
     block_diag(a.diag, a.sp, dq, de, dc);
-    if (a.track) {  // uniform: energy of the particles erased in this push
-        const double er = (s < a.n && nc < 0 && nc_owned)
-                              ? (KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q)
-                              : 0.0;
-        block_sum(&a.diag->sum_erased[a.sp], er);
-    }
+    if (a.track) block_sum(&a.diag->sum_erased[a.sp], er);  // (uniform)
 }
 
 // ----------------------------------------------------------------------------
@@ -437,7 +440,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
-    const int nb = (int)((sp.n + 255) / 256);
+    const int nb = push_blocks(s, sp.n, s.push_minblocks_mixed);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LP(P, K)                                                                                          \
