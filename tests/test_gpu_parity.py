@@ -97,6 +97,57 @@ def test_steps_fp64(solver, pusher):
         np.testing.assert_allclose(dg.as_array(), dc, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("crowd", [2, 3, 5, 9, 40, 150])
+def test_rebin_front_orders_crowded_cell(crowd):
+    """`crowd` particles from the 26 neighbours of one cell enter it in the
+    same step, beside stayers: the front part of the cell's new list
+    (arrivals in descending old traversal order, plist.cpp:22-39) goes
+    through the pair exchange, the 4- and 8-entry networks, the insertion
+    sort or the long-part kernel by its length.  Cell indices and order equal
+    the reference's, and the positions are exact."""
+    from tests._cases import small_case as _sc
+    case, fields, _ = _sc("fdtd", "boris", n=(12, 12, 12))
+    for k in fields:
+        fields[k] = np.zeros_like(fields[k])
+    rng = np.random.default_rng(crowd)
+    T = np.array([6, 6, 6])
+    offs = [np.array([a, b, c]) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1) if (a, b, c) != (0, 0, 0)]
+    pos, u = [], []
+    for m in range(crowd):
+        dl = offs[m % 26]
+        cell = T + dl
+        frac = np.where(dl < 0, 0.93 + 0.05 * rng.random(3), np.where(dl > 0, 0.02 + 0.05 * rng.random(3),
+                                                                       0.2 + 0.6 * rng.random(3)))
+        pos.append(cell + frac)
+        u.append(-0.3 * dl + np.where(dl == 0, 0.02 * rng.standard_normal(3), 0.0))
+    for _ in range(3):  # stayers of the crowded cell
+        pos.append(T + 0.3 + 0.4 * rng.random(3))
+        u.append(0.01 * rng.standard_normal(3))
+    pos, u = np.array(pos), np.array(u)
+    cells = (pos[:, 0].astype(int) * case.ny + pos[:, 1].astype(int)) * case.nz + pos[:, 2].astype(int)
+    o = np.argsort(cells, kind="stable")
+    p = {"x": pos[o, 0], "y": pos[o, 1], "z": pos[o, 2], "ux": u[o, 0], "uy": u[o, 1], "uz": u[o, 2]}
+    p["g"] = np.sqrt(1 + p["ux"] ** 2 + p["uy"] ** 2 + p["uz"] ** 2)
+    p["q"] = -0.01 * (1 + 0.1 * rng.random(p["x"].size))
+    p["cmr"] = np.full(p["x"].size, -1.0)
+    g, c = _load_both(case, fields, [p], (-1.0,))
+    Tc = (T[0] * case.ny + T[1]) * case.nz + T[2]
+    for step in range(2):
+        g.step(1)
+        c.step(1)
+        gp, cp = g.get_particles(0), c.get_particles()
+        np.testing.assert_array_equal(gp["cell"], cp["cell"], err_msg=f"step {step}")
+        for k in ("x", "y", "z"):
+            # exact while the fields are the loaded zeros; then J's atomics
+            # enter E (1e-12, as test_steps_fp64)
+            if step == 0:
+                np.testing.assert_array_equal(gp[k], cp[k], err_msg=f"step {step} {k}")
+            else:
+                assert _rel(gp[k], cp[k]) <= RTOL64, (step, k)
+        # every particle sits in the crowded cell
+        assert np.count_nonzero(gp["cell"] == Tc) == crowd + 3
+
+
 def test_single_particle_bitwise():
     case, fields, parts = small_case("fdtd", "boris")
     p = {k: v[1000:1001] for k, v in parts[0].items()}
