@@ -131,15 +131,15 @@ struct State {
     bool boundaries_done = false;
     int sp_e = -1, sp_p = -1, sp_ph = -1;  // QED species (cmr -1, +1, 0)
     // CTAs per SM the FP64 push's register budget targets (2, 3 or 4; more
-    // CTAs, fewer registers per thread); QP_PUSH_MINBLOCKS selects
-    int push_minblocks = 3;
+    // CTAs, fewer registers per thread); QP_PUSH_MINBLOCKS selects.  2: the
+    // grid-stride kernel needs 128 registers to run without spills
+    int push_minblocks = 2;
     // the same for the mixed push (3 or 4; QP_PUSH_MINBLOCKS_MIXED)
     int push_minblocks_mixed = 3;
-    // grid of the mixed non-QED push: at most push_waves x (SMs x CTAs per
-    // SM) blocks striding over the particles (QP_PUSH_WAVES; 0: one thread
-    // per particle).  The FP64 push keeps one thread per particle: its
-    // loop form measured slower.
-    int push_waves = 16;
+    // grid of the non-QED pushes: at most push_waves x (SMs x CTAs per SM)
+    // blocks striding over the particles (QP_PUSH_WAVES; 0: one thread per
+    // particle)
+    int push_waves = 32;
     int sm_count = 148;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,

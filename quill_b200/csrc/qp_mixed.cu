@@ -32,12 +32,10 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
     return r;
 }
 
-// The particles in traversal order as k_push64 takes them, but with a grid of
-// a few waves striding over block-sized chunks: the diagnostics are summed
-// per thread over its chunks and block-reduced once, which measured 17 %
-// faster than one thread per particle (the FP64 kernel in this form measured
-// slower).  The move runs in the particle's cell frame (offsets in [0, 1)),
-// the current through the warp's segment-slot run reduction (deposit_runs).
+// The particles in traversal order as k_push64 takes them (a grid of a few
+// waves striding over block-sized chunks, diagnostics reduced once).  The
+// move runs in the particle's cell frame (offsets in [0, 1)), the current
+// through the warp's segment-slot run reduction (deposit_runs).
 template <int PUSHER, int KIND, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
