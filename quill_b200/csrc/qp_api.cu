@@ -731,7 +731,9 @@ static void fill_diag(State& s, qp_diag* d) {
     for (const auto& sp : s.sp) nion += sp.kind == KIND_ION;
     d->n_ion = nion;
     d->N_e = Ne * aN; d->N_p = Np * aN; d->N_ph = Nph * aN;
-    d->energy_f = a.field * aE;
+    double wf = 0.0;
+    for (int k = 0; k < FIELD_SLOTS; k++) wf += a.field[k];
+    d->energy_f = wf * aE;
     d->energy_e = ee * bE; d->energy_p = ep * bE; d->energy_ph = eph * bE;
     d->energy_erased = er * bE;
 }
@@ -777,14 +779,14 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
             if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i], counted);
         QP_CUDA_CHECK(s, cudaGetLastError());
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[3], s.stream));
-        // compute_energy field term on E, B before fadvance (main.cpp:2327)
-        if (s.fp64) launch_field_energy_fp64(s);
-        else launch_field_energy_mixed(s);
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[4], s.stream));
-        // fadvance: half B, E, half B, Bbar (maxwell.cpp:10-22, advance.cpp:13-18)
+        // fadvance: half B, E, half B, Bbar (maxwell.cpp:10-22, advance.cpp:13-18);
+        // the first half B also sums compute_energy's field term on E, B
+        // before the update (main.cpp:2327)
         for (int ph = 0; ph < 4; ph++) {
-            if (s.fp64) launch_fields_fp64(s, ph == 2 ? 0 : ph);
-            else launch_fields_mixed(s, ph == 2 ? 0 : ph);
+            const int kp = ph == 0 ? 4 : (ph == 2 ? 0 : ph);
+            if (s.fp64) launch_fields_fp64(s, kp);
+            else launch_fields_mixed(s, kp);
         }
         QP_CUDA_CHECK(s, cudaGetLastError());
         QP_CUDA_CHECK(s, cudaMemcpyAsync(s.h_diag, s.d_diag, sizeof(DiagAccum), cudaMemcpyDeviceToHost, s.stream));

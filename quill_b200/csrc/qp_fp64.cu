@@ -366,8 +366,12 @@ void launch_fields_fp64(State& s, int phase) {
     dim3 blk(32, 8, 1);
     dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, s.grid.nx);
     const int sol = s.prm.solver;
-#define QP_LF(SOL, PH) k_field<double, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c)
-    if (phase == 0 || phase == 2) {
+#define QP_LF(SOL, PH) k_field<double, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c, s.d_diag, s.diag_lo, s.diag_hi)
+    if (phase == 4) {
+        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 4);
+        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 4);
+        else QP_LF(QP_SOLVER_FIVE_POINT, 4);
+    } else if (phase == 0 || phase == 2) {
         if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 0);
         else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 0);
         else QP_LF(QP_SOLVER_FIVE_POINT, 0);
@@ -517,13 +521,5 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     s.launches++;
 }
 
-void launch_field_energy_fp64(State& s) {
-    Fields<double> f = fields64(s);
-    const size_t off = (size_t)s.diag_lo * s.grid.nynz;
-    Fields<double> fo = f;
-    fo.ex += off; fo.ey += off; fo.ez += off; fo.bx += off; fo.by += off; fo.bz += off;
-    k_field_energy<double><<<148 * 4, 256, 0, s.stream>>>(fo, (s.diag_hi - s.diag_lo) * s.grid.nynz, s.d_diag);
-    s.launches++;
-}
 
 }  // namespace qp

@@ -87,12 +87,16 @@ struct Species {
     int32_t* trn[2] = {nullptr, nullptr};  // track numbers (0 = untracked), per buffer; tracking only
 };
 
+constexpr int FIELD_SLOTS = 64;
+
 struct DiagAccum {
     // per species: live count, sum q, sum of (g-1)q (or g q for photons)
     double sum_q[QP_MAX_SPECIES];
     double sum_e[QP_MAX_SPECIES];
     unsigned long long cnt[QP_MAX_SPECIES];
-    double field;  // sum over cells of E^2 + B^2
+    // sum over cells of E^2 + B^2, in FIELD_SLOTS partial sums (the blocks of
+    // the first half-B kernel add into slot blockIdx % FIELD_SLOTS)
+    double field[FIELD_SLOTS];
     double sum_erased[QP_MAX_SPECIES];  // sum of (g-1)q (g q for photons) of erased particles
 };
 
@@ -192,12 +196,13 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
                    double* loss_out);
 
 // ---- kernels / launchers (FP64, qp_fp64.cu) ----
-void launch_fields_fp64(State& s, int phase);          // phase: 0 half B, 1 E, 2 half B, 3 Bbar
+// phase: 0 half B, 1 E, 2 half B, 3 Bbar, 4 half B summing E^2 + B^2 of the
+// cells [diag_lo, diag_hi) before the update (compute_energy's field term)
+void launch_fields_fp64(State& s, int phase);
 void launch_init_boundaries_fp64(State& s);
 void launch_push_fp64(State& s, int species, double external_bz);
 int launch_push_fp64_qed(State& s, int species, double external_bz);
 int launch_vacuum_fp64(State& s);
-void launch_field_energy_fp64(State& s);
 
 // ---- mixed precision (qp_mixed.cu) ----
 void launch_fields_mixed(State& s, int phase);
@@ -205,7 +210,6 @@ void launch_init_boundaries_mixed(State& s);
 void launch_push_mixed(State& s, int species, double external_bz);
 int launch_push_mixed_qed(State& s, int species, double external_bz);
 int launch_vacuum_mixed(State& s);
-void launch_field_energy_mixed(State& s);
 
 // ---- rebin and scans (qp_rebin.cu) ----
 // Rebin after a push: count -> scan -> assign; leaves the new traversal

@@ -14,26 +14,60 @@ struct FieldCells { static constexpr int value = 1; };
 template <>
 struct FieldCells<float> { static constexpr int value = 2; };
 
+template <typename V>
+__device__ __forceinline__ V warp_sum(V v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// PHASE 0 half B, 1 E, 3 B at E points; 4 half B that first sums E^2 + B^2
+// of its cells with i in [dlo, dhi) in FP64 (compute_energy's field term,
+// fout.cpp:101-102, on the fields before fadvance): the values are loaded by
+// the stencil anyway, and one atomic per block goes to slot blockIdx %
+// FIELD_SLOTS of acc->field.
 template <typename T, int SOLVER, int PHASE>
-__global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c) {
+__global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c, DiagAccum* acc, int dlo, int dhi) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (k >= g.nz || j >= g.ny) return;
     constexpr int CPT = FieldCells<T>::value;
+    double es = 0.0;
+    if (k < g.nz && j < g.ny) {
 #pragma unroll
-    for (int u = 0; u < CPT; u++) {
-        const int i = blockIdx.z * CPT + u;
-        if (i >= g.nx) break;
-        if (PHASE == 0) {
-            if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
-            else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
-            else fp_b(f, g, c, i, j, k);
-        } else if (PHASE == 1) {
-            if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
-            else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
-            else fp_e(f, g, c, i, j, k);
-        } else {
-            bbar(f, g, i, j, k);
+        for (int u = 0; u < CPT; u++) {
+            const int i = blockIdx.z * CPT + u;
+            if (i >= g.nx) break;
+            if (PHASE == 4 && i >= dlo && i < dhi) {
+                const int x = cidx(g, i, j, k);
+                const double ex = f.ex[x], ey = f.ey[x], ez = f.ez[x], bx = f.bx[x], by = f.by[x], bz = f.bz[x];
+                es += ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
+            }
+            if (PHASE == 0 || PHASE == 4) {
+                if (SOLVER == QP_SOLVER_FDTD) fdtd_b(f, g, c, i, j, k);
+                else if (SOLVER == QP_SOLVER_NDFX) ndfx_b(f, g, c, i, j, k);
+                else fp_b(f, g, c, i, j, k);
+            } else if (PHASE == 1) {
+                if (SOLVER == QP_SOLVER_FDTD) fdtd_e(f, g, c, i, j, k);
+                else if (SOLVER == QP_SOLVER_NDFX) ndfx_e(f, g, c, i, j, k);
+                else fp_e(f, g, c, i, j, k);
+            } else {
+                bbar(f, g, i, j, k);
+            }
+        }
+    }
+    if (PHASE == 4) {
+        __shared__ double sh[8];
+        const int t = threadIdx.y * blockDim.x + threadIdx.x;
+        es = warp_sum(es);
+        if ((t & 31) == 0) sh[t >> 5] = es;
+        __syncthreads();
+        if (t < 32) {
+            es = t < (int)((blockDim.x * blockDim.y) >> 5) ? sh[t] : 0.0;
+            es = warp_sum(es);
+            if (t == 0 && es != 0.0) {
+                const unsigned b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+                atomicAdd(&acc->field[b % FIELD_SLOTS], es);
+            }
         }
     }
 }
@@ -57,13 +91,6 @@ __global__ void k_zero_plane(Fields<T> f, Grid g, int axis, int plane, int comps
     if (comps & 8) f.bx[x] = T(0);
     if (comps & 16) f.by[x] = T(0);
     if (comps & 32) f.bz[x] = T(0);
-}
-
-template <typename V>
-__device__ __forceinline__ V warp_sum(V v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
 }
 
 // Block-wide sums of three values, one atomic per block into the species'
@@ -109,27 +136,6 @@ __device__ __forceinline__ void block_sum(double* acc, double v) {
         v = lane < (int)((blockDim.x + 31) >> 5) ? s_v[lane] : 0.0;
         v = warp_sum(v);
         if (lane == 0 && v != 0.0) atomicAdd(acc, v);
-    }
-}
-
-// Sum of E^2 + B^2 over all cells (compute_energy's field term,
-// fout.cpp:101-102), FP64 accumulation.
-template <typename T>
-__global__ void __launch_bounds__(256) k_field_energy(Fields<T> f, int nc, DiagAccum* acc) {
-    double s = 0.0;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nc; x += gridDim.x * blockDim.x) {
-        const double ex = f.ex[x], ey = f.ey[x], ez = f.ez[x], bx = f.bx[x], by = f.by[x], bz = f.bz[x];
-        s += ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz;
-    }
-    __shared__ double sh[32];
-    s = warp_sum(s);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = s;
-    __syncthreads();
-    if (wid == 0) {
-        s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-        s = warp_sum(s);
-        if (lane == 0) atomicAdd(&acc->field, s);
     }
 }
 

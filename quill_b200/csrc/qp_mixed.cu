@@ -384,8 +384,12 @@ void launch_fields_mixed(State& s, int phase) {
     constexpr int CPT = FieldCells<float>::value;
     dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, (s.grid.nx + CPT - 1) / CPT);
     const int sol = s.prm.solver;
-#define QP_LF(SOL, PH) k_field<float, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c)
-    if (phase == 0 || phase == 2) {
+#define QP_LF(SOL, PH) k_field<float, SOL, PH><<<grd, blk, 0, s.stream>>>(f, s.grid, c, s.d_diag, s.diag_lo, s.diag_hi)
+    if (phase == 4) {
+        if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 4);
+        else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 4);
+        else QP_LF(QP_SOLVER_FIVE_POINT, 4);
+    } else if (phase == 0 || phase == 2) {
         if (sol == QP_SOLVER_FDTD) QP_LF(QP_SOLVER_FDTD, 0);
         else if (sol == QP_SOLVER_NDFX) QP_LF(QP_SOLVER_NDFX, 0);
         else QP_LF(QP_SOLVER_FIVE_POINT, 0);
@@ -546,13 +550,5 @@ int launch_vacuum_mixed(State& s) {
     return QP_OK;
 }
 
-void launch_field_energy_mixed(State& s) {
-    Fields<float> f = fields32(s);
-    const size_t off = (size_t)s.diag_lo * s.grid.nynz;
-    Fields<float> fo = f;
-    fo.ex += off; fo.ey += off; fo.ez += off; fo.bx += off; fo.by += off; fo.bz += off;
-    k_field_energy<float><<<148 * 4, 256, 0, s.stream>>>(fo, (s.diag_hi - s.diag_lo) * s.grid.nynz, s.d_diag);
-    s.launches++;
-}
 
 }  // namespace qp
