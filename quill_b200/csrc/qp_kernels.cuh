@@ -7,12 +7,12 @@
 namespace qp {
 
 // (k, j, i) = (x, y, z) launch axes; each thread updates the cells (i, j, k)
-// for FIELD_CELLS<T> consecutive i (two in FP32, where one cell's bytes are
+// for FieldCells<T> consecutive i (four in FP32, where one cell's bytes are
 // too few to keep enough loads in flight), every cell independently.
 template <typename T>
 struct FieldCells { static constexpr int value = 1; };
 template <>
-struct FieldCells<float> { static constexpr int value = 2; };
+struct FieldCells<float> { static constexpr int value = 4; };
 
 template <typename V>
 __device__ __forceinline__ V warp_sum(V v) {
