@@ -494,7 +494,7 @@ int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz,
         w.release(gam);
     }
     const SolverCoef C = solver_coef(P);
-    PushArgs pa;
+    PushArgs pa{};
     pa.cmr = -1.0; pa.dt = P.dt; pa.dx = P.dx; pa.dy = P.dy; pa.dz = P.dz; pa.ext_bz = ext_bz;
     pa.n = 0; pa.sp = 0; pa.kind = KIND_LEPTON; pa.status = s.d_status; pa.diag = s.d_diag;
     pa.track = 0;

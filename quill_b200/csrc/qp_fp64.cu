@@ -433,7 +433,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
         return QP_OK;
     }
     PStore64 src = store64(sp, sp.cur), dst = store64(sp, 1 - sp.cur);
-    PushArgs a;
+    PushArgs a{};
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
@@ -493,7 +493,7 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     cudaMemsetAsync(sp.count, 0, (size_t)s.grid.nc * sizeof(int32_t), s.stream);
     if (sp.n == 0) return;
     PStore64 src = store64(sp, sp.cur), dst = store64(sp, 1 - sp.cur);
-    PushArgs a;
+    PushArgs a{};
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;

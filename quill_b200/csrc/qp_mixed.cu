@@ -430,7 +430,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
         *ps[a] = (float*)sp.buf[sp.cur][1 + a];
         *pd[a] = (float*)sp.buf[1 - sp.cur][1 + a];
     }
-    PushArgs32 a;
+    PushArgs32 a{};
     a.cmr = (float)sp.cmr; a.dt = (float)s.prm.dt;
     a.idx = (float)(1.0 / s.prm.dx); a.idy = (float)(1.0 / s.prm.dy); a.idz = (float)(1.0 / s.prm.dz);
     a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
@@ -494,7 +494,7 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
         return QP_OK;
     }
     PStore32 src = store32(sp, sp.cur), dst = store32(sp, 1 - sp.cur);
-    PushArgs32 a;
+    PushArgs32 a{};
     a.cmr = (float)sp.cmr; a.dt = (float)s.prm.dt;
     a.idx = (float)(1.0 / s.prm.dx); a.idy = (float)(1.0 / s.prm.dy); a.idz = (float)(1.0 / s.prm.dz);
     a.ext_bz = (float)external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
