@@ -56,7 +56,8 @@ BYTES = {"fp64": (120, 168), "mixed": (68, 84)}
 # capture of k_push64 / k_push32 on the same physics at 160^3 (15,250,622
 # particles).  At fixed ppc the traffic grows with the particle count, so the
 # figure is scaled by Np.
-TRAFFIC_PER_PARTICLE = {"fp64": 2498516000 / 15250622, "mixed": 1427013632 / 15250622}
+TRAFFIC_PER_PARTICLE = {"fp64": (2471789056 + 1296481536) / 15250622,
+                        "mixed": (934635776 + 669794048) / 15250622}
 
 
 class Clocks:

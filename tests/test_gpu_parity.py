@@ -148,6 +148,37 @@ def test_rebin_front_orders_crowded_cell(crowd):
         assert np.count_nonzero(gp["cell"] == Tc) == crowd + 3
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("waves", ["1", "0"])
+def test_push_chunks_per_block(monkeypatch, precision, waves):
+    """The pushes take block-sized chunks of the traversal, several per block
+    when the grid is smaller than the particle count (QP_PUSH_WAVES = 1: one
+    resident wave of blocks, here about ten chunks each) and one per block
+    with QP_PUSH_WAVES = 0; the diagnostics summed per thread over its chunks
+    and the particles equal the reference's (FP64 to 1e-12; mixed to its
+    tolerances)."""
+    monkeypatch.setenv("QP_PUSH_WAVES", waves)
+    species = (-1.0,)
+    case, fields, parts = small_case("fdtd", "boris", n=(48, 48, 48), ppc=8, species=species)
+    assert parts[0]["x"].size > 600000
+    g, c = _load_both(case, fields, parts, species, precision=precision)
+    for step in range(2):
+        dg = g.step(1)[0]
+        dc = c.step(1)[0]
+    gp, cp = g.get_particles(0), c.get_particles()
+    if precision == "fp64":
+        np.testing.assert_array_equal(gp["cell"], cp["cell"])
+        for k in ("x", "y", "z", "ux", "uy", "uz", "g"):
+            assert _rel(gp[k], cp[k]) <= RTOL64, k
+        # the diagnostics are sums over n particles (or cells) taken in
+        # another order than the reference's loop: they agree to n x 2^-53
+        n = max(gp["x"].size, case.nx * case.ny * case.nz)
+        np.testing.assert_allclose(dg.as_array(), dc, rtol=n * 2.0 ** -53, atol=0)
+    else:
+        assert abs(gp["x"].size - cp["x"].size) <= max(2, gp["x"].size // 2000)
+        np.testing.assert_allclose(dg.as_array(), dc, rtol=2e-5, atol=0)
+
+
 def test_single_particle_bitwise():
     case, fields, parts = small_case("fdtd", "boris")
     p = {k: v[1000:1001] for k, v in parts[0].items()}
