@@ -69,6 +69,57 @@ __device__ __forceinline__ void fdtd_e(const Fields<T>& f, const Grid& g, const 
         f.ez[x] += c.dtdx * (f.by[x] - f.by[xi]) - c.dtdy * (f.bx[x] - f.bx[xj]) - f.jz[x] * c.dz;
 }
 
+// fdtd_b / fdtd_e for CPT consecutive interior cells (i0 .. i0+CPT-1, j, k
+// all in the main region): the E (B) values the i-difference reads are
+// loaded once per plane and shared by neighbouring cells; each update is the
+// main-region formula in the same operation order.  es (PHASE 4 of k_field)
+// receives E^2 + B^2 of the cells with i in [dlo, dhi) before the update.
+template <typename T, int CPT, bool ENERGY>
+__device__ __forceinline__ void fdtd_b_run(const Fields<T>& f, const Grid& g, const Coef<T>& c, int i0, int j, int k,
+                                           int dlo, int dhi, double& es) {
+    const int I = g.nynz, J = g.nz;
+    const int x0 = cidx(g, i0, j, k);
+    T ey_[CPT + 1], ez_[CPT + 1];
+#pragma unroll
+    for (int p = 0; p <= CPT; p++) {
+        ey_[p] = f.ey[x0 + p * I];
+        ez_[p] = f.ez[x0 + p * I];
+    }
+#pragma unroll
+    for (int u = 0; u < CPT; u++) {
+        const int x = x0 + u * I;
+        const T ex = f.ex[x], exj = f.ex[x + J], exk = f.ex[x + 1], eyk = f.ey[x + 1], ezj = f.ez[x + J];
+        const T bx = f.bx[x], by = f.by[x], bz = f.bz[x];
+        if (ENERGY && i0 + u >= dlo && i0 + u < dhi) {
+            const double a = ex, b = ey_[u], d = ez_[u], e = bx, h = by, m = bz;
+            es += a * a + b * b + d * d + e * e + h * h + m * m;
+        }
+        f.bx[x] = bx + T(0.5) * (-c.dtdy * (ezj - ez_[u]) + c.dtdz * (eyk - ey_[u]));
+        f.by[x] = by + T(0.5) * (c.dtdx * (ez_[u + 1] - ez_[u]) - c.dtdz * (exk - ex));
+        f.bz[x] = bz + T(0.5) * (c.dtdy * (exj - ex) - c.dtdx * (ey_[u + 1] - ey_[u]));
+    }
+}
+
+template <typename T, int CPT>
+__device__ __forceinline__ void fdtd_e_run(const Fields<T>& f, const Grid& g, const Coef<T>& c, int i0, int j, int k) {
+    const int I = g.nynz, J = g.nz;
+    const int x0 = cidx(g, i0, j, k);
+    T by_[CPT + 1], bz_[CPT + 1];  // planes i0-1 .. i0+CPT-1
+#pragma unroll
+    for (int p = 0; p <= CPT; p++) {
+        by_[p] = f.by[x0 + (p - 1) * I];
+        bz_[p] = f.bz[x0 + (p - 1) * I];
+    }
+#pragma unroll
+    for (int u = 0; u < CPT; u++) {
+        const int x = x0 + u * I;
+        const T bx = f.bx[x], bxj = f.bx[x - J], bxk = f.bx[x - 1], byk = f.by[x - 1], bzj = f.bz[x - J];
+        f.ex[x] = f.ex[x] + (c.dtdy * (bz_[u + 1] - bzj) - c.dtdz * (by_[u + 1] - byk) - f.jx[x] * c.dx);
+        f.ey[x] = f.ey[x] + (-c.dtdx * (bz_[u + 1] - bz_[u]) + c.dtdz * (bx - bxk) - f.jy[x] * c.dy);
+        f.ez[x] = f.ez[x] + (c.dtdx * (by_[u + 1] - by_[u]) - c.dtdy * (bx - bxj) - f.jz[x] * c.dz);
+    }
+}
+
 // ---------------------------------------------------------------- NDFX ----
 // maxwell.cpp:251-328.  B and E: [2, n-1)^3 plus the i/j/k = 1 planes for the
 // components tangential to them.
@@ -210,6 +261,35 @@ __device__ __forceinline__ void bbar(const Fields<T>& f, const Grid& g, int i, i
     else if (j0) f.bez[x] = T(0.25) * (bz[x] + bz[x - I] + bz[x + 1] + bz[x - I + 1]);
     else if (k1) f.bez[x] = T(0.25) * (bz[x] + bz[x - I] + bz[x - J] + bz[x - I - J]);
     else f.bez[x] = T(0.125) * (bz[x] + bz[x - I] + bz[x + 1] + bz[x - I + 1] + bz[x - J] + bz[x - I - J] + bz[x - J + 1] + bz[x - I - J + 1]);
+}
+
+// bbar for CPT consecutive interior cells (i0 .. i0+CPT-1, j, k all in the
+// main region): the B values of the CPT+1 planes each component's stencil
+// spans are loaded once into registers and shared by neighbouring cells; the
+// sums are bbar's 8-point sums in bbar's order.
+template <typename T, int CPT>
+__device__ __forceinline__ void bbar_run(const Fields<T>& f, const Grid& g, int i0, int j, int k) {
+    const int I = g.nynz, J = g.nz;
+    const int x0 = cidx(g, i0, j, k);
+    T ax[CPT + 1][4], ay[CPT + 1][4], az[CPT + 1][4];
+#pragma unroll
+    for (int p = 0; p <= CPT; p++) {
+        const int bx0 = x0 + p * I;        // bx: planes i0 .. i0+CPT
+        ax[p][0] = f.bx[bx0]; ax[p][1] = f.bx[bx0 - 1]; ax[p][2] = f.bx[bx0 - J]; ax[p][3] = f.bx[bx0 - J - 1];
+        const int b0 = x0 + (p - 1) * I;   // by, bz: planes i0-1 .. i0+CPT-1
+        ay[p][0] = f.by[b0]; ay[p][1] = f.by[b0 - 1]; ay[p][2] = f.by[b0 + J]; ay[p][3] = f.by[b0 + J - 1];
+        az[p][0] = f.bz[b0]; az[p][1] = f.bz[b0 + 1]; az[p][2] = f.bz[b0 - J]; az[p][3] = f.bz[b0 - J + 1];
+    }
+#pragma unroll
+    for (int u = 0; u < CPT; u++) {
+        const int x = x0 + u * I;
+        f.bex[x] = T(0.125) * (ax[u][0] + ax[u + 1][0] + ax[u][1] + ax[u + 1][1] + ax[u][2] + ax[u + 1][2] +
+                               ax[u][3] + ax[u + 1][3]);
+        f.bey[x] = T(0.125) * (ay[u + 1][0] + ay[u][0] + ay[u + 1][1] + ay[u][1] + ay[u + 1][2] + ay[u][2] +
+                               ay[u + 1][3] + ay[u][3]);
+        f.bez[x] = T(0.125) * (az[u + 1][0] + az[u][0] + az[u + 1][1] + az[u][1] + az[u + 1][2] + az[u][2] +
+                               az[u + 1][3] + az[u][3]);
+    }
 }
 
 // init_boundaries (maxwell.cpp:135-236, 338-438, 532-597): components set to

@@ -13,6 +13,12 @@ template <typename T>
 struct FieldCells { static constexpr int value = 1; };
 template <>
 struct FieldCells<float> { static constexpr int value = 4; };
+// whether the FDTD half-B and E updates of interior threads take the fast
+// path (fdtd_b_run / fdtd_e_run)
+template <typename T>
+struct FDTD_RUN { static constexpr bool value = true; };
+template <>
+struct FDTD_RUN<float> { static constexpr bool value = false; };
 
 template <typename V>
 __device__ __forceinline__ V warp_sum(V v) {
@@ -32,7 +38,17 @@ __global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c, D
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     constexpr int CPT = FieldCells<T>::value;
     double es = 0.0;
-    if (k < g.nz && j < g.ny) {
+    const int ib = blockIdx.z * CPT;
+    // a thread whose cells are all interior takes the fast path: no face
+    // cases, the loads along i shared between its cells
+    const bool interior = k >= 1 && k < g.nz - 1 && j >= 1 && j < g.ny - 1 && ib >= 1 && ib + CPT <= g.nx - 1;
+    if (interior && PHASE == 3) {
+        bbar_run<T, CPT>(f, g, ib, j, k);
+    } else if (FDTD_RUN<T>::value && interior && SOLVER == QP_SOLVER_FDTD && (PHASE == 0 || PHASE == 4)) {
+        fdtd_b_run<T, CPT, PHASE == 4>(f, g, c, ib, j, k, dlo, dhi, es);
+    } else if (FDTD_RUN<T>::value && interior && SOLVER == QP_SOLVER_FDTD && PHASE == 1) {
+        fdtd_e_run<T, CPT>(f, g, c, ib, j, k);
+    } else if (k < g.nz && j < g.ny) {
 #pragma unroll
         for (int u = 0; u < CPT; u++) {
             const int i = blockIdx.z * CPT + u;
