@@ -7,18 +7,12 @@
 namespace qp {
 
 // (k, j, i) = (x, y, z) launch axes; each thread updates the cells (i, j, k)
-// for FieldCells<T> consecutive i (four in FP32, where one cell's bytes are
+// for FieldCells<T> consecutive i (two in FP32, where one cell's bytes are
 // too few to keep enough loads in flight), every cell independently.
 template <typename T>
 struct FieldCells { static constexpr int value = 1; };
 template <>
-struct FieldCells<float> { static constexpr int value = 4; };
-// whether the FDTD half-B and E updates of interior threads take the fast
-// path (fdtd_b_run / fdtd_e_run)
-template <typename T>
-struct FDTD_RUN { static constexpr bool value = true; };
-template <>
-struct FDTD_RUN<float> { static constexpr bool value = false; };
+struct FieldCells<float> { static constexpr int value = 2; };
 
 template <typename V>
 __device__ __forceinline__ V warp_sum(V v) {
@@ -44,9 +38,9 @@ __global__ void __launch_bounds__(256) k_field(Fields<T> f, Grid g, Coef<T> c, D
     const bool interior = k >= 1 && k < g.nz - 1 && j >= 1 && j < g.ny - 1 && ib >= 1 && ib + CPT <= g.nx - 1;
     if (interior && PHASE == 3) {
         bbar_run<T, CPT>(f, g, ib, j, k);
-    } else if (FDTD_RUN<T>::value && interior && SOLVER == QP_SOLVER_FDTD && (PHASE == 0 || PHASE == 4)) {
+    } else if (interior && SOLVER == QP_SOLVER_FDTD && (PHASE == 0 || PHASE == 4)) {
         fdtd_b_run<T, CPT, PHASE == 4>(f, g, c, ib, j, k, dlo, dhi, es);
-    } else if (FDTD_RUN<T>::value && interior && SOLVER == QP_SOLVER_FDTD && PHASE == 1) {
+    } else if (interior && SOLVER == QP_SOLVER_FDTD && PHASE == 1) {
         fdtd_e_run<T, CPT>(f, g, c, ib, j, k);
     } else if (k < g.nz && j < g.ny) {
 #pragma unroll
