@@ -116,6 +116,22 @@ struct GlobalSink {
 // with lower corner w (deposition.cpp:13-39).  p and w are in the particle's
 // frame; the global cell of the corner is base + w.  Out-of-grid targets are
 // skipped and flagged (cannot happen for dt < dx, dy, dz).
+// x / 3.  In FP64 by Markstein's correction of a reciprocal product
+// (P. W. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Develop. 34(1), 1990): r = RN(1/3) is
+// a third of an ulp from 1/3, so q = RN(x r) lies within one ulp of x / 3;
+// the residual x - 3 q is exact in one FMA, and RN(q + r (x - 3 q)) is the
+// correctly rounded quotient, i.e. what IEEE division returns (for results
+// above the subnormal range; the sign of a zero is copied from x).  Three
+// dependent operations instead of a full division.
+__device__ __forceinline__ double div3(double x) {
+    const double r = 0x1.5555555555555p-2;  // RN(1/3)
+    const double q = x * r;
+    return copysign(fma(fma(-q, 3.0, x), r, q), x);
+}
+template <typename T>
+__device__ __forceinline__ T div3(T x) { return x / T(3); }
+
 template <typename T, typename Sink>
 __device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const T p[3], const T d[3], T q,
                                         const int w[3], int bi, int bj, int bk, unsigned int* status) {
@@ -130,19 +146,18 @@ __device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const 
     }
     const int c = cidx(gr, wi, wj, wk);
     const int cj1 = c + gr.nz, ck1 = c + 1, ci1 = c + gr.nynz;
-    const T third = T(3);
-    sink.add(0, wi, wj + 1, wk + 1, cj1 + 1, dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third));
-    sink.add(0, wi, wj, wk + 1, ck1, dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - dy * dz / third));
-    sink.add(0, wi, wj + 1, wk, cj1, dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - dy * dz / third));
-    sink.add(0, wi, wj, wk, c, dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + dy * dz / third));
-    sink.add(1, wi + 1, wj, wk + 1, ci1 + 1, dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + dx * dz / third));
-    sink.add(1, wi, wj, wk + 1, ck1, dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - dx * dz / third));
-    sink.add(1, wi + 1, wj, wk, ci1, dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - dx * dz / third));
-    sink.add(1, wi, wj, wk, c, dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + dx * dz / third));
-    sink.add(2, wi + 1, wj + 1, wk, ci1 + gr.nz, dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + dx * dy / third));
-    sink.add(2, wi, wj + 1, wk, cj1, dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third));
-    sink.add(2, wi + 1, wj, wk, ci1, dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third));
-    sink.add(2, wi, wj, wk, c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third));
+    sink.add(0, wi, wj + 1, wk + 1, cj1 + 1, dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + div3(dy * dz)));
+    sink.add(0, wi, wj, wk + 1, ck1, dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - div3(dy * dz)));
+    sink.add(0, wi, wj + 1, wk, cj1, dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - div3(dy * dz)));
+    sink.add(0, wi, wj, wk, c, dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + div3(dy * dz)));
+    sink.add(1, wi + 1, wj, wk + 1, ci1 + 1, dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + div3(dx * dz)));
+    sink.add(1, wi, wj, wk + 1, ck1, dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - div3(dx * dz)));
+    sink.add(1, wi + 1, wj, wk, ci1, dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - div3(dx * dz)));
+    sink.add(1, wi, wj, wk, c, dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + div3(dx * dz)));
+    sink.add(2, wi + 1, wj + 1, wk, ci1 + gr.nz, dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + div3(dx * dy)));
+    sink.add(2, wi, wj + 1, wk, cj1, dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - div3(dx * dy)));
+    sink.add(2, wi + 1, wj, wk, ci1, dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - div3(dx * dy)));
+    sink.add(2, wi, wj, wk, c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + div3(dx * dy)));
 }
 
 // The 12 contributions of one segment from its start offsets in the cell
@@ -154,19 +169,18 @@ template <typename T>
 __device__ __forceinline__ void seg_values_at(T xa, T ya, T za, const T d[3], T q, T v[12]) {
     const T xb = T(1) - xa, yb = T(1) - ya, zb = T(1) - za;
     const T dx = d[0], dy = d[1], dz = d[2];
-    const T third = T(3);
-    v[0] = dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + dy * dz / third);
-    v[1] = dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - dy * dz / third);
-    v[2] = dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - dy * dz / third);
-    v[3] = dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + dy * dz / third);
-    v[4] = dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + dx * dz / third);
-    v[5] = dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - dx * dz / third);
-    v[6] = dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - dx * dz / third);
-    v[7] = dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + dx * dz / third);
-    v[8] = dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + dx * dy / third);
-    v[9] = dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - dx * dy / third);
-    v[10] = dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - dx * dy / third);
-    v[11] = dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + dx * dy / third);
+    v[0] = dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + div3(dy * dz));
+    v[1] = dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - div3(dy * dz));
+    v[2] = dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - div3(dy * dz));
+    v[3] = dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + div3(dy * dz));
+    v[4] = dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + div3(dx * dz));
+    v[5] = dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - div3(dx * dz));
+    v[6] = dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - div3(dx * dz));
+    v[7] = dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + div3(dx * dz));
+    v[8] = dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + div3(dx * dy));
+    v[9] = dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - div3(dx * dy));
+    v[10] = dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - div3(dx * dy));
+    v[11] = dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + div3(dx * dy));
 }
 
 // The same from the start point p and the cell's lower corner w.
