@@ -159,9 +159,12 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
                                                     const int32_t* __restrict__ perm,
                                                     int32_t* __restrict__ newcell, PushArgs a, QedArgs qa,
                                                     AppendTarget<PStore64> t0, AppendTarget<PStore64> t1) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
+    // block-sized chunks with the grid striding over them, diagnostics
+    // reduced once per block (as in the pushes without QED)
+    for (int ch = blockIdx.x; (long long)ch * blockDim.x < a.n; ch += gridDim.x) {
+    const int s = ch * blockDim.x + threadIdx.x;
     if (s < a.n) {
         const int p = perm[s];
         double pos[3] = {src.x[p], src.y[p], src.z[p]};
@@ -282,11 +285,12 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
             if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
             const int ii = (int)pos[0];
             if (ii >= a.dlo && ii < a.dhi) {
-                dq = q;
-                de = KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
-                dc = 1;
+                dq += q;
+                de += KIND == KIND_PHOTON ? gm * q : (gm - 1) * q;
+                dc += 1;
             }
         }
+    }
     }
     block_diag(a.diag, a.sp, dq, de, dc);
 }
@@ -453,7 +457,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
         t0 = target64(s, s.sp_ph, true);
         t1 = t0;
     }
-    const int nb = (int)((sp.n + 255) / 256);
+    const int nb = push_blocks(s, sp.n, 2);  // chunked grid (2 resident blocks per SM assumed)
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push64_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)

@@ -187,9 +187,12 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                                                     const int32_t* __restrict__ perm,
                                                     int32_t* __restrict__ newcell, PushArgs32 a, QedArgs qa,
                                                     AppendTarget<PStore32> t0, AppendTarget<PStore32> t1) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
     double dq = 0.0, de = 0.0;
     unsigned long long dc = 0;
+    // block-sized chunks with the grid striding over them, diagnostics
+    // reduced once per block (as in the pushes without QED)
+    for (int ch = blockIdx.x; (long long)ch * blockDim.x < a.n; ch += gridDim.x) {
+    const int s = ch * blockDim.x + threadIdx.x;
     if (s < a.n) {
         const int p = perm[s];
         const int c0 = src.cell[p];
@@ -321,11 +324,12 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
             dst.g[s] = gm; dst.q[s] = q; dst.chi[s] = chi;
             if (a.trn_dst) a.trn_dst[s] = a.trn_src[p];
             if (i1 >= a.dlo && i1 < a.dhi) {
-                dq = (double)q;
-                de = KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
-                dc = 1;
+                dq += (double)q;
+                de += KIND == KIND_PHOTON ? (double)gm * (double)q : ((double)gm - 1.0) * (double)q;
+                dc += 1;
             }
         }
+    }
     }
     block_diag(a.diag, a.sp, dq, de, dc);
 }
@@ -515,7 +519,7 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
         t0 = target32(s, s.sp_ph, true);
         t1 = t0;
     }
-    const int nb = (int)((sp.n + 255) / 256);
+    const int nb = push_blocks(s, sp.n, 2);  // chunked grid (2 resident blocks per SM assumed)
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push32_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
