@@ -46,7 +46,9 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
             // division by the cell size (advance.cpp:281-284)
             const double t = a.dt / gm;
             d[0] = ux * t; d[1] = uy * t; d[2] = uz * t;
-            d[0] = d[0] / a.dx; d[1] = d[1] / a.dy; d[2] = d[2] / a.dz;
+            d[0] = div_fixed(d[0], a.dx, a.rdx);
+            d[1] = div_fixed(d[1], a.dy, a.rdy);
+            d[2] = div_fixed(d[2], a.dz, a.rdz);
             if (KIND == KIND_PHOTON) {
                 pos[0] = pos[0] + d[0]; pos[1] = pos[1] + d[1]; pos[2] = pos[2] + d[2];
             } else {
@@ -499,6 +501,7 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     PStore64 src = store64(sp, sp.cur), dst = store64(sp, 1 - sp.cur);
     PushArgs a{};
     a.cmr = sp.cmr; a.dt = s.prm.dt; a.dx = s.prm.dx; a.dy = s.prm.dy; a.dz = s.prm.dz;
+    a.rdx = 1.0 / s.prm.dx; a.rdy = 1.0 / s.prm.dy; a.rdz = 1.0 / s.prm.dz;
     a.ext_bz = external_bz; a.n = (int)sp.n; a.sp = si; a.kind = sp.kind;
     a.status = s.d_status; a.diag = s.d_diag;
     a.track = s.track_erased ? 1 : 0;

@@ -335,6 +335,7 @@ __device__ __forceinline__ void catch_particle(const CatchBuf& c, int sp, uint32
 
 struct PushArgs {
     double cmr, dt, dx, dy, dz, ext_bz;
+    double rdx, rdy, rdz;  // RN(1 / dx) ... for div_fixed
     int n, sp, kind;
     int track;  // sum the energy of erased particles into diag->sum_erased
     uint32_t step;

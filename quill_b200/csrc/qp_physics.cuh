@@ -132,6 +132,17 @@ __device__ __forceinline__ double div3(double x) {
 template <typename T>
 __device__ __forceinline__ T div3(T x) { return x / T(3); }
 
+// x / y in FP64 for a divisor y > 0 fixed over a launch, given r = RN(1/y)
+// (an IEEE division on the host): q0 = RN(x r) is within about 1.5 ulp of
+// x / y, one FMA correction makes it faithful, and a second one gives the
+// correctly rounded quotient (Markstein's theorem, as div3), i.e. the value
+// of IEEE division, for results above the subnormal range.
+__device__ __forceinline__ double div_fixed(double x, double y, double r) {
+    const double q0 = x * r;
+    const double q1 = fma(fma(-q0, y, x), r, q0);
+    return copysign(fma(fma(-q1, y, x), r, q1), x);
+}
+
 template <typename T, typename Sink>
 __device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const T p[3], const T d[3], T q,
                                         const int w[3], int bi, int bj, int bk, unsigned int* status) {
