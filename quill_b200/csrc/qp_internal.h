@@ -143,7 +143,7 @@ struct State {
     // grid of the non-QED pushes: at most push_waves x (SMs x CTAs per SM)
     // blocks striding over the particles (QP_PUSH_WAVES; 0: one thread per
     // particle)
-    int push_waves = 32;
+    int push_waves = 128;
     int sm_count = 148;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
