@@ -53,11 +53,12 @@ def hbm_peak():
 BYTES = {"fp64": (120, 168), "mixed": (68, 84)}
 # DRAM traffic of one push launch per particle (dram__bytes_read.sum +
 # dram__bytes_write.sum over the particles of the launch), from one ncu
-# capture of k_push64 / k_push32 on the same physics at 160^3 (15,250,622
-# particles).  At fixed ppc the traffic grows with the particle count, so the
-# figure is scaled by Np.
-TRAFFIC_PER_PARTICLE = {"fp64": (2471789056 + 1296481536) / 15250622,
-                        "mixed": (934635776 + 669794048) / 15250622}
+# capture of the 4th k_push64 / k_push32 launch of the 512^3 benchmark itself
+# (526,539,513 particles; the three metrics are collected in one pass, without
+# replay).  At fixed ppc the traffic grows with the particle count, so the
+# figure is scaled by Np for other grids.
+TRAFFIC_PER_PARTICLE = {"fp64": (78.90e9 + 44.88e9) / 526539513,
+                        "mixed": (50.38e9 + 26.46e9) / 526539513}
 
 
 class Clocks:
@@ -414,7 +415,7 @@ def main():
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": np_avg * TRAFFIC_PER_PARTICLE[prec],
-                         "traffic_source": "ncu capture at 160^3 scaled by the particle count",
+                         "traffic_source": "ncu capture of a 512^3 launch (1 pass), per particle x Np",
                          "algorithmic_bytes_per_launch": np_avg * bp},
             "step_roofline_frac": (np_avg * bp + nc * bc) / (ms * 1e-3 / t["steps"]) / 1e9 / peak,
             "energy_drift": (w1 - w0) / w0 if w0 else None,

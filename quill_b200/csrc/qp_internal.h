@@ -2,6 +2,8 @@
 // kernel entry points shared between translation units.
 #pragma once
 
+#include <algorithm>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
@@ -175,12 +177,20 @@ struct State {
     } snap[4];
 };
 
-// Blocks of 256 threads for a grid-stride push over n particles.
-inline int push_blocks(const State& s, int64_t n, int minb) {
-    const int64_t full = (n + 255) / 256;
-    if (s.push_waves <= 0) return (int)full;
-    const int64_t cap = (int64_t)s.sm_count * minb * s.push_waves;
-    return (int)(full < cap ? full : cap);
+// Blocks of 256 threads for a push over n particles in block-sized chunks
+// (chunk_range): up to push_waves groups of `resident` blocks (the blocks
+// resident at once: SMs x CTAs per SM); one chunk per block if push_waves is
+// 0 or the chunks are fewer than the resident blocks.
+inline int push_blocks(const State& s, int64_t n, int minb, int* resident) {
+    const int64_t nch = (n + 255) / 256;
+    const int64_t r = (int64_t)s.sm_count * minb;
+    if (s.push_waves <= 0 || nch <= r) {
+        *resident = (int)(nch > 0 ? nch : 1);
+        return (int)nch;
+    }
+    const int64_t w = std::min<int64_t>(s.push_waves, (nch + r - 1) / r);
+    *resident = (int)r;
+    return (int)(r * w);
 }
 
 // Device copy of the full state into a snapshot / back (qp_checkpoint,

@@ -333,9 +333,27 @@ __device__ __forceinline__ void catch_particle(const CatchBuf& c, int sp, uint32
     c.key[slot] = ((int64_t)step << 33) | ((int64_t)phase << 32) | (int64_t)(uint32_t)s;
 }
 
+// Chunk order of the push grids.  The grid is `waves` groups of `resident`
+// blocks; group w takes the w-th contiguous part of the block-sized chunks
+// of the traversal, its blocks striding over that part by `resident`.  The
+// chunks in flight at any time are then neighbours in memory (the field and
+// J tiles they share stay in L2), and the later groups take over as blocks
+// finish, which balances the load.
+struct ChunkRange {
+    int first, end, step;
+};
+__device__ __forceinline__ ChunkRange chunk_range(int n, int resident) {
+    const int nch = (int)(((long long)n + blockDim.x - 1) / blockDim.x);
+    const int waves = gridDim.x / resident;
+    const int per = (nch + waves - 1) / waves;
+    const int w = blockIdx.x / resident, r = blockIdx.x % resident;
+    return ChunkRange{w * per + r, min(nch, (w + 1) * per), resident};
+}
+
 struct PushArgs {
     double cmr, dt, dx, dy, dz, ext_bz;
     double rdx, rdy, rdz;  // RN(1 / dx) ... for div_fixed
+    int resident;          // blocks per group of the chunk order (chunk_range)
     int n, sp, kind;
     int track;  // sum the energy of erased particles into diag->sum_erased
     uint32_t step;

@@ -20,6 +20,7 @@ struct PushArgs32 {
     const int32_t* trn_src;  // track numbers in, by slot / out, by traversal position; nullptr: off
     int32_t* trn_dst;
     int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)
+    int resident;  // blocks per group of the chunk order (chunk_range)
 };
 
 __device__ __forceinline__ float wrap_offset(float o, int& shift) {
@@ -42,8 +43,9 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
                                                    int32_t* __restrict__ count, PushArgs32 a) {
     double dq = 0.0, de = 0.0, er = 0.0;
     unsigned long long dc = 0;
-    for (int base = blockIdx.x * blockDim.x; base < a.n; base += gridDim.x * blockDim.x) {
-        const int s = base + threadIdx.x;
+    const ChunkRange cr = chunk_range(a.n, a.resident);
+    for (int ch = cr.first; ch < cr.end; ch += cr.step) {
+        const int s = ch * blockDim.x + threadIdx.x;
         int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
         bool nc_owned = true;
         bool live = false, active = false;
@@ -191,7 +193,8 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
     unsigned long long dc = 0;
     // block-sized chunks with the grid striding over them, diagnostics
     // reduced once per block (as in the pushes without QED)
-    for (int ch = blockIdx.x; (long long)ch * blockDim.x < a.n; ch += gridDim.x) {
+    const ChunkRange cr = chunk_range(a.n, a.resident);
+    for (int ch = cr.first; ch < cr.end; ch += cr.step) {
     const int s = ch * blockDim.x + threadIdx.x;
     if (s < a.n) {
         const int p = perm[s];
@@ -446,7 +449,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
-    const int nb = push_blocks(s, sp.n, s.push_minblocks_mixed);
+    const int nb = push_blocks(s, sp.n, s.push_minblocks_mixed, &a.resident);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LP(P, K)                                                                                          \
@@ -519,7 +522,7 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
         t0 = target32(s, s.sp_ph, true);
         t1 = t0;
     }
-    const int nb = push_blocks(s, sp.n, 2);  // chunked grid (2 resident blocks per SM assumed)
+    const int nb = push_blocks(s, sp.n, 2, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push32_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
