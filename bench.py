@@ -52,13 +52,14 @@ def hbm_peak():
 # writes E B Bbar, the deposit flush writes J once)
 BYTES = {"fp64": (120, 168), "mixed": (68, 84)}
 # DRAM traffic of one push launch per particle (dram__bytes_read.sum +
-# dram__bytes_write.sum over the particles of the launch), from one ncu
-# capture of the 4th k_push64 / k_push32 launch of the 512^3 benchmark itself
-# (526,539,513 particles; the three metrics are collected in one pass, without
-# replay).  At fixed ppc the traffic grows with the particle count, so the
-# figure is scaled by Np for other grids.
-TRAFFIC_PER_PARTICLE = {"fp64": (78.90e9 + 44.88e9) / 526539513,
-                        "mixed": (50.38e9 + 26.46e9) / 526539513}
+# dram__bytes_write.sum over the particles of the launch), from an ncu
+# capture of one k_push64 / k_push32 launch on the same physics at 160^3
+# (15,250,622 particles, about 2.5 GB on the device).  At fixed ppc the
+# traffic grows in proportion to the particle count, so the per-particle
+# figure is scaled by Np for the grid being measured.
+TRAFFIC_PER_PARTICLE = {"fp64": (2.472e9 + 1.296e9) / 15250622,
+                        "mixed": (0.935e9 + 0.670e9) / 15250622}
+TRAFFIC_SOURCE = "ncu capture of one launch at 160^3 (same physics), per particle x Np"
 
 
 class Clocks:
@@ -415,7 +416,7 @@ def main():
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": np_avg * TRAFFIC_PER_PARTICLE[prec],
-                         "traffic_source": "ncu capture of a 512^3 launch (1 pass), per particle x Np",
+                         "traffic_source": TRAFFIC_SOURCE,
                          "algorithmic_bytes_per_launch": np_avg * bp},
             "step_roofline_frac": (np_avg * bp + nc * bc) / (ms * 1e-3 / t["steps"]) / 1e9 / peak,
             "energy_drift": (w1 - w0) / w0 if w0 else None,

@@ -173,7 +173,9 @@ int qp_eval_qed_rates(int device, double lambda_cm, int64_t n, const double* in,
  * fixed array inside the library (at most 16384 samples per call; larger n
  * is rejected with QP_ERR_ARG).  All calls share that array: calls that
  * overlap on the GPU race.  The first call on a device looks the array up
- * and should come before any stream capture.  Errors: qp_last_error(NULL). */
+ * and should come before any stream capture; the address it finds is kept,
+ * so the call must not be used after cudaDeviceReset.  The caller's current
+ * device is left as it was.  Errors: qp_last_error(NULL). */
 int qp_eval_qed_rates_noalloc(int device, double lambda_cm, int64_t n, const double* in, double* out);
 
 /* Per-phase CUDA-event timing of qp_step on the handle's stream: enable

@@ -17,7 +17,11 @@
 // several host threads, or on several devices sharing a host thread without
 // waiting) race on the array.  The first call on a device looks up the
 // array's device address (cudaGetSymbolAddress) with that device current;
-// make that first call before any stream capture.
+// make that first call before any stream capture.  The address is kept for
+// the life of the process: after cudaDeviceReset on that device the module
+// is loaded again and the kept address is stale, so the entry point must not
+// be used after a device reset.  The call leaves the caller's current device
+// as it found it.
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -71,7 +75,9 @@ extern "C" int qp_eval_qed_rates_noalloc(int device, double lambda_cm, int64_t n
         return QP_ERR_ARG;
     }
     if (n == 0) return QP_OK;
-    cudaError_t e = cudaSetDevice(device);
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e == cudaSuccess && prev != device) e = cudaSetDevice(device);
     double* base = nullptr;
     if (e == cudaSuccess) e = staging_ptr(device, &base);
     if (e == cudaSuccess) {
@@ -81,6 +87,11 @@ extern "C" int qp_eval_qed_rates_noalloc(int device, double lambda_cm, int64_t n
         if (e == cudaSuccess) e = qp::launch_qed_rates((int)n, d_in, d_out, lambda_cm / 2.4263086e-10, 0);
         if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, (size_t)n * 5 * sizeof(double), cudaMemcpyDefault, 0);
         if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    }
+    // the caller's current device is restored whatever happened above
+    if (prev >= 0 && prev != device) {
+        const cudaError_t e2 = cudaSetDevice(prev);
+        if (e == cudaSuccess) e = e2;
     }
     if (e != cudaSuccess) {
         set_global_error(std::string("qp_eval_qed_rates_noalloc: ") + cudaGetErrorString(e));
