@@ -109,36 +109,66 @@ class Clocks:
 
 
 # ----------------------------------------------------------------------------
-# CPU side: the reference build on a bounded sample
+# CPU side: the reference build on the same workload
 # ----------------------------------------------------------------------------
+# The reference's only parallelism is its cut of the box into x-slab regions,
+# one per MPI rank (main.cpp:2232-2267), neighbours overlapping by 8 cells.
+# Here each host process is one such region of the benchmark box, built by
+# the reference's own code (oracle/_ref, Release flags): its slab of the
+# laser fields and its slab of the plasma, its diagnostics over the cells it
+# owns.  The regions step concurrently; what is left out is the MPI exchange
+# of halos and crossing particles between steps (no MPI on the host).
 
-def _cpu_sample(args_tuple):
-    """One process: the reference (or the restatement) stepping a sub-box of
-    the configuration's plasma; returns (particle-steps, cell-updates, s)."""
-    kind, cfg_name, box, steps, warm, seed = args_tuple
-    sys.path.insert(0, ROOT)
-    import numpy as np
-    from oracle import oracle as O
-    from quill_b200 import workloads as W
-    case = W.scaled(W.config(cfg_name), box, box, box)
-    case.seed = seed
-    fields, parts = W.build(case)
-    solver = {"fdtd": 0, "ndfx": 1, "five_point": 2}[case.solver]
-    pusher = {"vay": 0, "boris": 1}[case.pusher]
-    icmr = tuple(sp.cmr for sp in case.species if sp.cmr not in (-1.0, 1.0, 0.0))
-    r = O.Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt, solver=solver, pusher=pusher,
-                 icmr=icmr, kind=kind, flavour="fast")
-    r.set_fields(*[fields[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
-    r.init_boundaries()
-    r.add_particles({k: np.concatenate([p[k] for p in parts]) for k in parts[0]})
-    r.step(warm)
-    n0 = r.count()
-    t0 = time.perf_counter()
-    d = r.step(steps)
-    dt = time.perf_counter() - t0
-    n1 = r.count()
-    nc = case.nx * case.ny * case.nz
-    return (0.5 * (n0 + n1) * steps, nc * steps, dt, n0)
+def _ref_region_job(job, barrier, queue):
+    """One x-slab region of the workload on one host core: build, warm up,
+    wait for the other regions, time `steps` steps.  Puts (region, units,
+    cell-updates, t0, t1, particles, error) on the queue."""
+    kind, cfg_name, grid, nreg, r, steps, warm, seed = job
+    try:
+        sys.path.insert(0, ROOT)
+        import numpy as np
+        from oracle import oracle as O
+        from quill_b200 import workloads as W
+        from quill_b200.slabs import SlabLayout
+        case = W.config(cfg_name)
+        if grid:
+            case = W.scaled(case, *grid)
+        lay = SlabLayout.even(case.nx, nreg)
+        x0, nxr = lay.x0[r], lay.nx[r]
+        solver = {"fdtd": 0, "ndfx": 1, "five_point": 2}[case.solver]
+        pusher = {"vay": 0, "boris": 1}[case.pusher]
+        icmr = tuple(sp.cmr for sp in case.species if sp.cmr not in (-1.0, 1.0, 0.0))
+        reg = O.Region(nxr, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt, solver=solver, pusher=pusher,
+                       icmr=icmr, kind=kind, flavour="fast")
+        f = W.make_fields(case, x0, nxr)
+        reg.set_fields(*[f[k] for k in ("ex", "ey", "ez", "bx", "by", "bz")])
+        del f
+        reg.init_boundaries()
+        rng = np.random.default_rng(seed + r)
+        for sp in case.species:
+            for part in W.particle_layers(case, sp, rng, x0, nxr):
+                reg.add_particles(part)
+        lo, hi = lay.diag_range(r)
+        reg.set_diag_range(lo, hi)
+        if warm:
+            reg.step(warm)
+        d0 = reg.compute_diag()
+        barrier.wait(timeout=1800)
+        t0 = time.monotonic()
+        d = reg.step(steps)
+        t1 = time.monotonic()
+
+        def count(row):  # N_qp_e + N_qp_p + N_qp_g + ions (the diagnostic row layout)
+            return float(row[3] + row[4] + row[5] + sum(row[10 + 2 * m] for m in range(reg.n_ion)))
+
+        units = count(d0) + sum(count(row) for row in d[:-1])
+        queue.put((r, units, (hi - lo) * case.ny * case.nz * steps, t0, t1, reg.count(), None))
+    except Exception as e:  # reported by the parent
+        try:
+            barrier.abort()
+        except Exception:
+            pass
+        queue.put((r, 0.0, 0, 0.0, 0.0, 0, f"{type(e).__name__}: {e}"))
 
 
 def cpu_kind():
@@ -146,20 +176,55 @@ def cpu_kind():
     return "reference" if O.available("ref", "fast") else "port"
 
 
-def run_cpu(cfg_name, procs, box=64, steps=30, warm=2):
+def _mem_available_bytes():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
+
+
+def run_reference_regions(cfg_name, grid, nreg, steps, warm, regions=None):
+    """The reference stepping regions `regions` (default: all) of the
+    workload cut into `nreg` x-slabs, one process each, concurrently.
+    Returns the units over the common timed window."""
+    import multiprocessing as mp
     kind = "ref" if cpu_kind() == "reference" else "port"
-    work = [(kind, cfg_name, box, steps, warm, 1000 + r) for r in range(procs)]
-    if procs == 1:
-        res = [_cpu_sample(work[0])]
-    else:
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(procs) as pool:
-            res = pool.map(_cpu_sample, work)
-    ps = sum(r[0] for r in res)
-    cu = sum(r[1] for r in res)
-    tmax = max(r[2] for r in res)
-    return {"particle_steps_per_s": ps / tmax, "cell_updates_per_s": cu / tmax, "seconds": tmax,
-            "particles_per_box": res[0][3], "kind": cpu_kind(), "procs": procs, "box": box, "steps": steps}
+    regions = list(range(nreg)) if regions is None else list(regions)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(len(regions))
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ref_region_job, args=((kind, cfg_name, grid, nreg, r, steps, warm, 1000), barrier, q))
+             for r in regions]
+    for pr in procs:
+        pr.start()
+    res = []
+    for _ in procs:
+        res.append(q.get(timeout=3600))
+    for pr in procs:
+        pr.join()
+    errs = [x[6] for x in res if x[6]]
+    if errs:
+        raise RuntimeError("reference region failed: " + errs[0])
+    t = max(x[4] for x in res) - min(x[3] for x in res)
+    units = sum(x[1] for x in res)
+    cells = sum(x[2] for x in res)
+    return {"particle_steps_per_s": units / t, "cell_updates_per_s": cells / t, "seconds": t,
+            "particles": sum(x[5] for x in res), "kind": cpu_kind(), "procs": len(regions), "regions": nreg,
+            "steps": steps, "units": units}
+
+
+def reference_bytes_estimate(case, nreg):
+    """Host memory of the reference's regions: about 104 B per particle
+    (its particle record, containers.h:54-66) and 112 B per cell (list
+    heads and the four field3d arrays), overlaps included, plus the
+    generator's transient arrays."""
+    ppc = sum(sp.ppc for sp in case.species)
+    cells = (case.nx + 8 * (nreg - 1)) * case.ny * case.nz
+    return cells * (112 + 104 * ppc) + nreg * (1 << 30)
 
 
 # ----------------------------------------------------------------------------

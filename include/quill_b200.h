@@ -188,6 +188,19 @@ int qp_set_timing(qp_handle* h, int enable);
  * diagnostics; *steps = timed steps (nullable). */
 int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
 
+/* Reference-order current deposition (parity switch; FP64, QED off): each
+ * step sums every J element's terms from zero in the order the reference's
+ * padvance adds them (cells lexicographic, each cell's list of all species
+ * from its head, then segment and term; advance.cpp:90-387,
+ * deposition.cpp:13-39), instead of with atomics, so that the region stays
+ * bit-identical to the reference over any number of steps.  Several times
+ * slower than the default deposition and 1.3 kB of scratch per particle;
+ * for parity runs.  With several species the cross-species list order
+ * starts, after a load, as species 0's particles of each cell first, then
+ * species 1's, and so on.  enable = 0 releases the scratch.  QP_ERR_CONFIG
+ * for mixed precision or QED. */
+int qp_set_ordered_current(qp_handle* h, int enable);
+
 /* Sum the energy of the particles each step erases (p_boundary before the
  * push, place() after it) into qp_diag.energy_erased, so that
  * energy_f + energy_e + energy_p + energy_ph + ienergy plus the erased energy

@@ -61,6 +61,12 @@ class Diag(C.Structure):
         ("energy_erased_sp", C.c_double * QP_MAX_SPECIES),
     ]
 
+    def total_energy(self) -> float:
+        """Fields + electrons + positrons + photons + ions (the sum of the
+        `energy` output's columns)."""
+        return (self.energy_f + self.energy_e + self.energy_p + self.energy_ph
+                + sum(self.ienergy[m] for m in range(self.n_ion)))
+
     def as_array(self) -> np.ndarray:
         """Same layout as the CPU checkers' diagnostic rows: N_e N_p N_ph
         N_qp_e N_qp_p N_qp_g energy_f energy_e energy_p energy_ph, then
@@ -108,6 +114,7 @@ def load_library(path: str | None = None):
         "qp_eval_qed_rates_noalloc": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
         "qp_set_erased_tracking": (C.c_int, [VP, C.c_int]),
+        "qp_set_ordered_current": (C.c_int, [VP, C.c_int]),
         "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
         "qp_moving_window": (C.c_int, [VP]),
         "qp_set_catching": (C.c_int, [VP, C.c_int, I64]),
@@ -417,6 +424,11 @@ class Region:
         """Report in Diag.energy_erased the energy of the particles each step
         erases (QED-off steps)."""
         self._check(self.lib.qp_set_erased_tracking(self.h, int(bool(enable))))
+
+    def set_ordered_current(self, enable: bool = True):
+        """Sum J in the reference's order (FP64, QED off): the region then
+        stays bit-identical to the reference over any number of steps."""
+        self._check(self.lib.qp_set_ordered_current(self.h, int(bool(enable))))
 
     def set_timing(self, enable: bool = True):
         self._check(self.lib.qp_set_timing(self.h, int(bool(enable))))

@@ -35,6 +35,7 @@ SOURCES = [
     ("qp_load.cu", []),
     ("qp_noalloc.cu", []),
     ("qp_adjoint.cu", ["--fmad=false"]),
+    ("qp_ordered.cu", ["--fmad=false"]),
     ("qp_merge.cu", []),
     ("qp_window.cu", []),
     ("qp_catch.cu", []),

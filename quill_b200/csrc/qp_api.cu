@@ -69,6 +69,7 @@ static int merge_sorted_slots(State& s, int si, int64_t slot0, int64_t n_new, co
     cudaFree(nstart);
     sp.n += n_new;
     sp.slots = slot0 + n_new;
+    s.layout_epoch++;
     return QP_OK;
 }
 static size_t arr_elem(const State& s, int a) { return s.fp64 ? 8 : 4; }
@@ -161,6 +162,7 @@ static void free_state(State* s) {
     cudaFree(s->long_list);
     cudaFree(s->window_scratch);
     catch_release(*s);
+    ordered_release(*s);
     s->window_scratch = nullptr;
     s->long_list = nullptr;
     cudaFree(s->scan_tmp);
@@ -232,6 +234,7 @@ int snapshot_restore(State& s, State::Snap& sn) {
         sp.n = sn.n[i];
         sp.slots = sn.slots[i];
     }
+    s.layout_epoch++;
     s.step_index = sn.step_index;
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
     return QP_OK;
@@ -766,6 +769,9 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
             QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
             for (size_t i = 0; i < s.sp.size(); i++)
                 born[i] = (int)std::min<int64_t>(born[i], s.sp[i].cap - s.sp[i].n);
+        } else if (s.ord.on) {
+            int r = ordered_push_all(s, external_bz);
+            if (r != QP_OK) return r;
         } else {
             for (size_t i = 0; i < s.sp.size(); i++) {
                 if (s.fp64) launch_push_fp64(s, (int)i, external_bz);
@@ -777,6 +783,10 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[2], s.stream));
         for (size_t i = 0; i < s.sp.size(); i++)
             if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i], counted);
+        if (s.ord.on) {
+            int r = ordered_after_rebin(s);
+            if (r != QP_OK) return r;
+        }
         QP_CUDA_CHECK(s, cudaGetLastError());
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[3], s.stream));
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[4], s.stream));

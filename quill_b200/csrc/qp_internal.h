@@ -87,6 +87,12 @@ struct Species {
     int32_t* count = nullptr;      // nc, rebin histogram
     int* d_counter = nullptr;      // device append counter (QED)
     int32_t* trn[2] = {nullptr, nullptr};  // track numbers (0 = untracked), per buffer; tracking only
+    // reference-order deposition with several species: order keys of the
+    // merged list of all species, by slot, per buffer; gstep: this step's
+    // key by traversal position (qp_ordered.cu)
+    int32_t* grank[2] = {nullptr, nullptr};
+    int32_t* gstep = nullptr;
+    int64_t gcap = 0;
 };
 
 constexpr int FIELD_SLOTS = 64;
@@ -166,6 +172,25 @@ struct State {
     // rebin: entry 0 counts them, entries 1.. list them
     int32_t* long_list = nullptr;
     int64_t long_cap = 0;
+    // bumped by every change of the particle layout other than a step's
+    // rebin, merging and the moving window (loads, restores, slab
+    // replacements): the reference-order deposition then rebuilds its keys
+    int64_t layout_epoch = 0;
+    // reference-order deposition (qp_set_ordered_current, qp_ordered.cu)
+    struct Ordered {
+        bool on = false;
+        int64_t epoch = -1;          // layout_epoch the order keys belong to
+        int64_t cap_particles = 0;   // entry buffers sized for this many particles
+        int32_t* tgt = nullptr;      // 48 entries per particle: target (component * nc + cell)
+        int64_t* key = nullptr;      //   order key (rank * 48 + term index)
+        double* val = nullptr;       //   term
+        int32_t* nent = nullptr;     // entries used per particle
+        int64_t* skey = nullptr;     // entries bucketed by target
+        double* sval = nullptr;
+        int32_t* jcount = nullptr;   // 3 nc + 1: entries per target, then claim cursors
+        int32_t* jstart = nullptr;   // 3 nc + 1: bucket starts
+        void* scan_tmp = nullptr;    // tile sums of the 3 nc scan
+    } ord;
     // checkpoints (device-resident copies)
     struct Snap {
         bool valid = false;
@@ -204,6 +229,13 @@ void catch_release(State& s);  // frees the catching buffer (qp_catch.cu)
 // Adjoint of qp_step's FP64 FDTD/Boris path (qp_adjoint.cu).
 int adjoint_energy(State& s, qp_handle* h, int nsteps, int every, double ext_bz, double* grad6, double* grad_q,
                    double* loss_out);
+
+// Reference-order deposition (qp_ordered.cu): every species pushed with its
+// current terms summed per J element in the reference's order; the order
+// keys of several species rebuilt after the rebin; buffers released.
+int ordered_push_all(State& s, double external_bz);
+int ordered_after_rebin(State& s);
+void ordered_release(State& s);
 
 // ---- kernels / launchers (FP64, qp_fp64.cu) ----
 // phase: 0 half B, 1 E, 2 half B, 3 Bbar, 4 half B summing E^2 + B^2 of the

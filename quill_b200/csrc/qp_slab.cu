@@ -330,6 +330,7 @@ extern "C" int qp_replace_particle_slab(qp_handle* h, int species, int i0, int w
             std::swap(sp.perm, sp.newcell);
             std::swap(sp.cell_start, sp.cell_next);
             sp.n = nn - (b - a);
+            s.layout_epoch++;
         }
     }
     if (n == 0) return QP_OK;

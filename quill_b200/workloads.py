@@ -125,13 +125,15 @@ def _profile(sp: SpeciesSpec, case: Case, ci: np.ndarray, cj: np.ndarray, ck: np
     raise KeyError(sp.density)
 
 
-def make_particles(case: Case, sp: SpeciesSpec, rng: np.random.Generator) -> dict:
+def make_particles(case: Case, sp: SpeciesSpec, rng: np.random.Generator, i_range=None) -> dict:
     """Particles in traversal order (cells lexicographic), ppc per occupied
     cell, uniform-random positions inside the cell, Maxwellian or cold
     momenta.  Only cells the reference keeps (is_inside: 1..n-3 per axis,
-    plist.cpp:42-48) are filled."""
+    plist.cpp:42-48) are filled; i_range = (a, b) limits them to the
+    x-layers [a, b)."""
     nx, ny, nz = case.nx, case.ny, case.nz
-    ii, jj, kk = np.meshgrid(np.arange(1, nx - 2), np.arange(1, ny - 2), np.arange(1, nz - 2), indexing="ij")
+    ia, ib = (1, nx - 2) if i_range is None else i_range
+    ii, jj, kk = np.meshgrid(np.arange(ia, ib), np.arange(1, ny - 2), np.arange(1, nz - 2), indexing="ij")
     ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
     n = _profile(sp, case, ii, jj, kk)
     occ = n > 0
@@ -161,10 +163,13 @@ def make_particles(case: Case, sp: SpeciesSpec, rng: np.random.Generator) -> dic
             "cmr": np.full(m, sp.cmr)}
 
 
-def make_fields(case: Case) -> dict:
-    """Initial E and B: the laser pulse (zero elsewhere)."""
+def make_fields(case: Case, i0: int = 0, nxr: int | None = None) -> dict:
+    """Initial E and B: the laser pulse (zero elsewhere).  With i0 / nxr,
+    only the x-layers [i0, i0 + nxr) of the box (an x-slab region)."""
     nx, ny, nz = case.nx, case.ny, case.nz
-    shape = (nx, ny, nz)
+    if nxr is None:
+        nxr = nx
+    shape = (nxr, ny, nz)
     f = {k: np.zeros(shape) for k in ("ex", "ey", "ez", "bx", "by", "bz")}
     L = case.laser
     if L is None:
@@ -182,7 +187,7 @@ def make_fields(case: Case) -> dict:
 
     # staggered positions (cell units): Ey at (i, j+1/2, k), Ez at (i, j, k+1/2),
     # Bz at (i+1/2, j+1/2, k), By at (i+1/2, j, k+1/2)
-    i = np.arange(nx)[:, None, None].astype(np.float64)
+    i = np.arange(i0, i0 + nxr)[:, None, None].astype(np.float64)
     j = np.arange(ny)[None, :, None].astype(np.float64)
     k = np.arange(nz)[None, None, :].astype(np.float64)
 
@@ -201,10 +206,28 @@ def make_fields(case: Case) -> dict:
         f["ez"] = pol[1] * wave(i, -0.5 * math.pi) * trans(j, k + 0.5)
         f["by"] = -pol[1] * wave(i + 0.5, -0.5 * math.pi) * trans(j, k + 0.5)
     if L.counter:
+        if nxr != nx:
+            raise ValueError("counter-propagating pulse: whole box only")
         # mirror pulse: x -> nx-1-x, travelling towards -x (B changes sign)
         for key, sgn in (("ey", 1), ("ez", 1), ("by", -1), ("bz", -1)):
             f[key] = f[key] + sgn * f[key][::-1, :, :]
     return {kk_: np.ascontiguousarray(v) for kk_, v in f.items()}
+
+
+def particle_layers(case: Case, sp: SpeciesSpec, rng: np.random.Generator, i0: int, nxr: int,
+                    layers_per_chunk: int = 4):
+    """Particles of the x-layers [i0, i0 + nxr) of the box (an x-slab region,
+    positions in its frame: x - i0), in groups of layers, each in traversal
+    order; the same plasma as make_particles (cells the reference keeps,
+    ppc per occupied cell, uniform-random positions, Maxwellian or cold
+    momenta)."""
+    lo, hi = max(i0, 1), min(i0 + nxr, case.nx - 2)
+    for a in range(lo, hi, layers_per_chunk):
+        b = min(a + layers_per_chunk, hi)
+        part = make_particles(case, sp, rng, i_range=(a, b))
+        if part["x"].size:
+            part["x"] = part["x"] - i0
+            yield part
 
 
 def build(case: Case):
