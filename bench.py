@@ -39,6 +39,21 @@ sys.path.insert(0, ROOT)
 PEAK_FALLBACK_GBS = 6650.0
 
 
+METRIC = "particle-steps/s & field cell-updates/s, FP64 vs mixed, 1 B200, at stated drift"
+
+
+def workload_config(case):
+    """The `config` of both arms' lines: the workload, nothing that differs
+    between them."""
+    sp = case.species[0]
+    ppc = sum(x.ppc for x in case.species)
+    return {"workload": f"{case.name}: {case.nx}x{case.ny}x{case.nz} cells, dx=lambda/{round(1 / case.dx_lambda)}, "
+                        f"dt={case.dt_over_dx:g}dx, {case.solver.upper()} + {case.pusher}, "
+                        f"QED {'on' if case.qed else 'off'}, {ppc} ppc at {sp.n0:g} n_cr, "
+                        f"T={sp.theta / 1.957e-3:g} keV, laser a0={case.laser.a0:g}",
+            "l2_flush": "not needed: particle and field arrays exceed L2"}
+
+
 def hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -394,8 +409,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=30)
-    ap.add_argument("--drift-steps", type=int, default=0,
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-regions", type=int, default=0,
+                    help="x-slab regions of the reference runs (default: the host's core count)")
+    ap.add_argument("--drift-steps", type=int, default=1000,
                     help="also run this many untimed steps per precision and report the relative drift of the "
                          "total energy (field + particles) over them")
     args = ap.parse_args()
@@ -409,24 +426,35 @@ def main():
     if args.grid:
         case = W.scaled(case, *args.grid)
     nc = case.nx * case.ny * case.nz
-    metric = "particle-steps/s & field cell-updates/s, FP64 vs mixed, 1 B200, at stated drift"
 
     if args.impl == "reference":
         if rank != 0:
             return
-        procs = os.cpu_count() or 1
-        r = run_cpu(args.config, procs, steps=max(args.steps, 5), warm=min(args.warmup, 2))
+        nreg = args.ref_regions or (os.cpu_count() or 1)
+        need, have = reference_bytes_estimate(case, nreg), _mem_available_bytes()
+        regions = None
+        if have is not None and need > 0.8 * have:
+            # not enough host memory for every region: a bounded sample of
+            # the regions, their units only
+            per = need / nreg
+            regions = list(range(max(1, int(0.8 * have // per))))
+        r = run_reference_regions(args.config, args.grid, nreg, args.steps, args.warmup, regions)
+        sample = (f"all {nreg} x-slab regions of the box (the reference's own decomposition, n_sr = {nreg}, "
+                  f"neighbours overlapping by 8 cells), one process each, stepped concurrently; "
+                  f"{r['particles']} particles held (overlaps included); no halo exchange between steps")
+        if regions is not None:
+            sample = (f"regions 0..{len(regions) - 1} of the box's {nreg} x-slab regions (host memory for "
+                      f"{len(regions)}), one process each; their particle-steps only")
         line = {
-            "impl": "reference", "metric": metric, "value": r["particle_steps_per_s"], "unit": "particle-steps/s",
-            "n_gpus": 0, "steps": r["steps"], "warmup": min(args.warmup, 2),
-            "ms_per_step": 1e3 * r["seconds"] / r["steps"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "metric": METRIC, "value": r["particle_steps_per_s"], "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * r["seconds"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "cell_updates_per_s": r["cell_updates_per_s"],
-            "config": {"workload": f"{args.config} physics on {r['procs']} independent {r['box']}^3 sub-boxes "
-                                   f"(one per host core, {r['particles_per_box']} particles each)",
-                       "parallelism": f"{r['procs']} processes"},
+            "config": workload_config(case),
+            "parallelism": f"{r['procs']} host processes (one x-slab region each)",
             "cpu_baseline": {"value": r["particle_steps_per_s"], "unit": "particle-steps/s", "cores": r["procs"],
-                             "kind": r["kind"], "sample": f"{r['procs']} x {r['box']}^3 boxes x {r['steps']} steps"},
+                             "kind": r["kind"], "sample": sample},
             "e2e": {"value": r["particle_steps_per_s"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         }
@@ -492,6 +520,7 @@ def main():
         }
     # long untimed runs for the energy drift (opt-in)
     if args.drift_steps > 0:
+        drift_fields = {}
         for prec in results:
             reg = build_region(case, prec, dev)
             reg.set_erased_tracking(True)
@@ -504,6 +533,10 @@ def main():
                     w.append(total_energy(x))
                     closed.append(w[-1] + lost)
                 left -= k
+            f_end = torch.empty((12, case.nx, case.ny, case.nz), dtype=torch.float64, device=f"cuda:{dev}")
+            reg._check(reg.lib.qp_dump_fields(reg.h, _tp(f_end)))
+            drift_fields[prec] = f_end[:6].clone()
+            del f_end
             reg.close()
             del reg
             torch.cuda.empty_cache()
@@ -519,6 +552,11 @@ def main():
     if args.drift_steps > 0 and "mixed" in results:
         a, b = results["mixed"]["long_run_energy_drift"], results["fp64"]["long_run_energy_drift"]
         a["drift_minus_fp64"] = a["relative_drift_with_erased"] - b["relative_drift_with_erased"]
+        x, y = drift_fields["mixed"], drift_fields["fp64"]
+        a["field_rel_l2_vs_fp64"] = float(torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y))
+    if args.drift_steps > 0:
+        del drift_fields
+        torch.cuda.empty_cache()
     # mixed vs FP64 field error after the same steps from the same state
     if "mixed" in results:
         a, b = results["mixed"]["fields_end"], results["fp64"]["fields_end"]
@@ -542,10 +580,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        c = run_cpu(args.config, 1, steps=args.cpu_steps, warm=2)
+        # one core: one x-slab region of the box (the one the laser enters)
+        # for a bounded sample of steps
+        nreg = args.ref_regions or (os.cpu_count() or 1)
+        c = run_reference_regions(args.config, args.grid, nreg, args.cpu_steps, 1, regions=[0])
         cpu = {"value": c["particle_steps_per_s"], "unit": "particle-steps/s", "cores": 1, "kind": c["kind"],
-               "sample": f"{args.config} physics on one 64^3 box ({c['particles_per_box']} particles), "
-                         f"{c['steps']} steps after 2 warm-up steps, {c['seconds']:.1f} s",
+               "sample": f"region 0 of the box cut into {nreg} x-slab regions (the reference's decomposition; "
+                         f"{c['particles']} particles), {c['steps']} steps after 1 warm-up step, "
+                         f"{c['seconds']:.1f} s",
                "cell_updates_per_s": c["cell_updates_per_s"], "host_cores_total": os.cpu_count()}
 
     if dist:
@@ -555,15 +597,13 @@ def main():
         return
     f64 = results["fp64"]
     line = {
-        "metric": metric, "value": f64["value"], "unit": "particle-steps/s", "n_gpus": world,
+        "metric": METRIC, "value": f64["value"], "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": f64["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, generated on the GPU)",
         "cell_updates_per_s": f64["cell_updates_per_s"],
-        "config": {"workload": f"{case.name}: {case.nx}x{case.ny}x{case.nz} cells, dx=lambda/{round(1 / case.dx_lambda)}, "
-                               f"dt=dx/2, {case.solver.upper()} + {case.pusher}, QED off, "
-                               f"{f64['particles']} electrons (4 ppc, 0.05 n_cr, 10 keV)",
-                   "l2_flush": "not needed: particle and field arrays (>70 GB) exceed L2",
-                   "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas (one region per GPU)"},
+        "config": workload_config(case),
+        "particles": f64["particles"],
+        "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas (one region per GPU)",
         "roofline": f64["roofline"], "step_roofline_frac": f64["step_roofline_frac"],
         "energy_drift": f64["energy_drift"], "drift_steps": f64["drift_steps"],
         "phase_ms_per_step": f64["phase_ms_per_step"],
