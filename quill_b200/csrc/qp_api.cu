@@ -159,6 +159,8 @@ static void free_state(State* s) {
     cudaFree(s->d_diag);
     cudaFreeHost(s->h_diag);
     cudaFree(s->d_status);
+    cudaFree(s->d_xcount);
+    cudaFree(s->xbuf);
     cudaFree(s->long_list);
     cudaFree(s->window_scratch);
     catch_release(*s);
@@ -170,6 +172,21 @@ static void free_state(State* s) {
         if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     s->stream = nullptr;
+}
+
+void* cross_storage(State& s, int64_t cap, size_t rec) {
+    const size_t need = (size_t)cap * rec;
+    if (need > s.xbuf_bytes) {
+        cudaFree(s.xbuf);
+        s.xbuf = nullptr;
+        s.xbuf_bytes = 0;
+        if (cudaMalloc(&s.xbuf, need) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        s.xbuf_bytes = need;
+    }
+    return s.xbuf;
 }
 
 int snapshot_take(State& s, State::Snap& sn) {
@@ -348,6 +365,7 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_diag, sizeof(DiagAccum), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(unsigned int), s.stream);
+    if (e == cudaSuccess) e = cudaMalloc(&s.d_xcount, CROSS_COUNTER_BYTES);
     s.scan_tmp_bytes = ((nc + 4095) / 4096 + 2) * sizeof(int32_t);
     if (e == cudaSuccess) e = cudaMalloc(&s.scan_tmp, s.scan_tmp_bytes);
     int ion = 0;

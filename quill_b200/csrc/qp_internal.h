@@ -172,6 +172,11 @@ struct State {
     // rebin: entry 0 counts them, entries 1.. list them
     int32_t* long_list = nullptr;
     int64_t long_cap = 0;
+    // crossing list of the pushes (moves that cross a cell face, deposited by
+    // k_deposit_crossings): one buffer reused by every push, and its counter
+    void* xbuf = nullptr;
+    size_t xbuf_bytes = 0;
+    int* d_xcount = nullptr;
     // bumped by every change of the particle layout other than a step's
     // rebin, merging and the moving window (loads, restores, slab
     // replacements): the reference-order deposition then rebuilds its keys
@@ -217,6 +222,17 @@ inline int push_blocks(const State& s, int64_t n, int minb, int* resident) {
     *resident = (int)r;
     return (int)(r * w);
 }
+
+// Sub-lists of the crossing list and the spacing of their counters (ints:
+// one 128-byte line per counter).
+constexpr int CROSS_LISTS = 128;
+constexpr int CROSS_COUNTER_STRIDE = 32;
+constexpr size_t CROSS_COUNTER_BYTES = (size_t)CROSS_LISTS * CROSS_COUNTER_STRIDE * sizeof(int);
+
+// Storage for a crossing list of `cap` records of `rec` bytes (grown as
+// needed, kept across steps); nullptr if it cannot be allocated (the pushes
+// then deposit crossing moves in place).
+void* cross_storage(State& s, int64_t cap, size_t rec);
 
 // Device copy of the full state into a snapshot / back (qp_checkpoint,
 // qp_restore, the adjoint's checkpoints); snapshot_free releases one.

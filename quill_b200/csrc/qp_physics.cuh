@@ -112,10 +112,13 @@ struct GlobalSink {
     }
 };
 
-// 12 contributions of one straight segment d starting at p, lying in the cell
-// with lower corner w (deposition.cpp:13-39).  p and w are in the particle's
-// frame; the global cell of the corner is base + w.  Out-of-grid targets are
-// skipped and flagged (cannot happen for dt < dx, dy, dz).
+// A sink that drops the contributions: jdeposition_to with it only moves the
+// particle along its segments (the compiler removes the unused terms).
+struct NullSink {
+    template <typename T>
+    __device__ __forceinline__ void add(int, int, int, int, int, T) const {}
+};
+
 // x / 3.  In FP64 by Markstein's correction of a reciprocal product
 // (P. W. Markstein, "Computation of elementary functions on the IBM RISC
 // System/6000 processor", IBM J. Res. Develop. 34(1), 1990): r = RN(1/3) is
@@ -143,34 +146,6 @@ __device__ __forceinline__ double div_fixed(double x, double y, double r) {
     return copysign(fma(fma(-q1, y, x), r, q1), x);
 }
 
-template <typename T, typename Sink>
-__device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const T p[3], const T d[3], T q,
-                                        const int w[3], int bi, int bj, int bk, unsigned int* status) {
-    const T xa = p[0] - T(w[0]), xb = T(1) - xa;
-    const T ya = p[1] - T(w[1]), yb = T(1) - ya;
-    const T za = p[2] - T(w[2]), zb = T(1) - za;
-    const int wi = bi + w[0], wj = bj + w[1], wk = bk + w[2];
-    const T dx = d[0], dy = d[1], dz = d[2];
-    if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= gr.nx || wj + 1 >= gr.ny || wk + 1 >= gr.nz) {
-        atomicOr(status, (unsigned int)ST_BOUNDS);
-        return;
-    }
-    const int c = cidx(gr, wi, wj, wk);
-    const int cj1 = c + gr.nz, ck1 = c + 1, ci1 = c + gr.nynz;
-    sink.add(0, wi, wj + 1, wk + 1, cj1 + 1, dx * q * (ya * za + T(0.5) * (dz * ya + dy * za) + div3(dy * dz)));
-    sink.add(0, wi, wj, wk + 1, ck1, dx * q * (yb * za + T(0.5) * (dz * yb - dy * za) - div3(dy * dz)));
-    sink.add(0, wi, wj + 1, wk, cj1, dx * q * (ya * zb + T(0.5) * (-dz * ya + dy * zb) - div3(dy * dz)));
-    sink.add(0, wi, wj, wk, c, dx * q * (yb * zb - T(0.5) * (dz * yb + dy * zb) + div3(dy * dz)));
-    sink.add(1, wi + 1, wj, wk + 1, ci1 + 1, dy * q * (xa * za + T(0.5) * (dx * za + dz * xa) + div3(dx * dz)));
-    sink.add(1, wi, wj, wk + 1, ck1, dy * q * (xb * za + T(0.5) * (-dx * za + dz * xb) - div3(dx * dz)));
-    sink.add(1, wi + 1, wj, wk, ci1, dy * q * (xa * zb + T(0.5) * (dx * zb - dz * xa) - div3(dx * dz)));
-    sink.add(1, wi, wj, wk, c, dy * q * (xb * zb - T(0.5) * (dx * zb + dz * xb) + div3(dx * dz)));
-    sink.add(2, wi + 1, wj + 1, wk, ci1 + gr.nz, dz * q * (xa * ya + T(0.5) * (dx * ya + dy * xa) + div3(dx * dy)));
-    sink.add(2, wi, wj + 1, wk, cj1, dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - div3(dx * dy)));
-    sink.add(2, wi + 1, wj, wk, ci1, dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - div3(dx * dy)));
-    sink.add(2, wi, wj, wk, c, dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + div3(dx * dy)));
-}
-
 // The 12 contributions of one segment from its start offsets in the cell
 // (xa, ya, za) = p - w, its displacement d and charge q, with seg_dep's
 // arithmetic and order; targets relative to the corner cell c: jx at
@@ -192,6 +167,65 @@ __device__ __forceinline__ void seg_values_at(T xa, T ya, T za, const T d[3], T 
     v[9] = dz * q * (xb * ya + T(0.5) * (-dx * ya + dy * xb) - div3(dx * dy));
     v[10] = dz * q * (xa * yb + T(0.5) * (dx * yb - dy * xa) - div3(dx * dy));
     v[11] = dz * q * (xb * yb - T(0.5) * (dx * yb + dy * xb) + div3(dx * dy));
+}
+
+// The same in FP32 (mixed precision), factored: with A = ya + dy/2,
+// B = za + dz/2 and c = dy dz / 12 the four jx terms are dx q (A B + c),
+// dx q ((1 - A) B - c), dx q (A (1 - B) - c) and dx q ((1 - A)(1 - B) + c),
+// equal to the expanded ones in exact arithmetic (likewise jy with x, z and
+// jz with x, y), in about half the operations.  Their sum is dx q, as the
+// expanded terms' is.
+__device__ __forceinline__ void seg_values_at(float xa, float ya, float za, const float d[3], float q, float v[12]) {
+    const float dx = d[0], dy = d[1], dz = d[2];
+    const float ax = fmaf(0.5f, dx, xa), ay = fmaf(0.5f, dy, ya), az = fmaf(0.5f, dz, za);
+    const float k12 = 1.0f / 12.0f;
+    const float cx = dy * dz * k12, cy = dx * dz * k12, cz = dx * dy * k12;
+    const float wx = dx * q, wy = dy * q, wz = dz * q;
+    float ab = ay * az;
+    v[0] = wx * (ab + cx);
+    v[1] = wx * (az - ab - cx);
+    v[2] = wx * (ay - ab - cx);
+    v[3] = wx * (1.0f - ay - az + ab + cx);
+    ab = ax * az;
+    v[4] = wy * (ab + cy);
+    v[5] = wy * (az - ab - cy);
+    v[6] = wy * (ax - ab - cy);
+    v[7] = wy * (1.0f - ax - az + ab + cy);
+    ab = ax * ay;
+    v[8] = wz * (ab + cz);
+    v[9] = wz * (ay - ab - cz);
+    v[10] = wz * (ax - ab - cz);
+    v[11] = wz * (1.0f - ax - ay + ab + cz);
+}
+
+// 12 contributions of one straight segment d starting at p, lying in the cell
+// with lower corner w (deposition.cpp:13-39).  p and w are in the particle's
+// frame; the global cell of the corner is base + w.  Out-of-grid targets are
+// skipped and flagged (cannot happen for dt < dx, dy, dz).
+template <typename T, typename Sink>
+__device__ __forceinline__ void seg_dep(const Sink& sink, const Grid& gr, const T p[3], const T d[3], T q,
+                                        const int w[3], int bi, int bj, int bk, unsigned int* status) {
+    const int wi = bi + w[0], wj = bj + w[1], wk = bk + w[2];
+    if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= gr.nx || wj + 1 >= gr.ny || wk + 1 >= gr.nz) {
+        atomicOr(status, (unsigned int)ST_BOUNDS);
+        return;
+    }
+    T v[12];
+    seg_values_at(p[0] - T(w[0]), p[1] - T(w[1]), p[2] - T(w[2]), d, q, v);
+    const int c = cidx(gr, wi, wj, wk);
+    const int cj1 = c + gr.nz, ck1 = c + 1, ci1 = c + gr.nynz;
+    sink.add(0, wi, wj + 1, wk + 1, cj1 + 1, v[0]);
+    sink.add(0, wi, wj, wk + 1, ck1, v[1]);
+    sink.add(0, wi, wj + 1, wk, cj1, v[2]);
+    sink.add(0, wi, wj, wk, c, v[3]);
+    sink.add(1, wi + 1, wj, wk + 1, ci1 + 1, v[4]);
+    sink.add(1, wi, wj, wk + 1, ck1, v[5]);
+    sink.add(1, wi + 1, wj, wk, ci1, v[6]);
+    sink.add(1, wi, wj, wk, c, v[7]);
+    sink.add(2, wi + 1, wj + 1, wk, ci1 + gr.nz, v[8]);
+    sink.add(2, wi, wj + 1, wk, cj1, v[9]);
+    sink.add(2, wi + 1, wj, wk, ci1, v[10]);
+    sink.add(2, wi, wj, wk, c, v[11]);
 }
 
 // The same from the start point p and the cell's lower corner w.
