@@ -158,10 +158,11 @@ static void free_state(State* s) {
     }
     cudaFree(s->d_diag);
     cudaFreeHost(s->h_diag);
+    cudaFreeHost(s->h_count);
     cudaFree(s->d_status);
-    cudaFree(s->d_xcount);
-    cudaFree(s->xbuf);
     cudaFree(s->long_list);
+    cudaFree(s->crowd_bits);
+    s->crowd_bits = nullptr;
     cudaFree(s->window_scratch);
     catch_release(*s);
     ordered_release(*s);
@@ -172,21 +173,6 @@ static void free_state(State* s) {
         if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     s->stream = nullptr;
-}
-
-void* cross_storage(State& s, int64_t cap, size_t rec) {
-    const size_t need = (size_t)cap * rec;
-    if (need > s.xbuf_bytes) {
-        cudaFree(s.xbuf);
-        s.xbuf = nullptr;
-        s.xbuf_bytes = 0;
-        if (cudaMalloc(&s.xbuf, need) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        s.xbuf_bytes = need;
-    }
-    return s.xbuf;
 }
 
 int snapshot_take(State& s, State::Snap& sn) {
@@ -363,11 +349,12 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     if (e == cudaSuccess) e = cudaMemsetAsync(s.fields, 0, 12 * nc * s.field_elem, s.stream);
     if (e == cudaSuccess) e = cudaMalloc(&s.d_diag, sizeof(DiagAccum));
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_diag, sizeof(DiagAccum), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_count, QP_MAX_SPECIES * sizeof(int32_t), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&s.d_status, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(unsigned int), s.stream);
-    if (e == cudaSuccess) e = cudaMalloc(&s.d_xcount, CROSS_COUNTER_BYTES);
     s.scan_tmp_bytes = ((nc + 4095) / 4096 + 2) * sizeof(int32_t);
     if (e == cudaSuccess) e = cudaMalloc(&s.scan_tmp, s.scan_tmp_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&s.crowd_bits, (nc + 31) / 32 * sizeof(uint32_t));
     int ion = 0;
     s.sp.resize(p.n_species);
     for (int i = 0; i < p.n_species && e == cudaSuccess; i++) {
@@ -799,8 +786,12 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
         const bool counted = !s.prm.qed;
         QP_CUDA_CHECK(s, cudaGetLastError());
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[2], s.stream));
+        std::vector<char> rebinned(s.sp.size(), 0);
         for (size_t i = 0; i < s.sp.size(); i++)
-            if (s.sp[i].n > 0 || born[i] > 0) rebin(s, (int)i, born[i], counted);
+            if (s.sp[i].n > 0 || born[i] > 0) {
+                rebin(s, (int)i, born[i], counted);
+                rebinned[i] = 1;
+            }
         if (s.ord.on) {
             int r = ordered_after_rebin(s);
             if (r != QP_OK) return r;
@@ -821,6 +812,8 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
         unsigned int st = 0;
         QP_CUDA_CHECK(s, cudaMemcpyAsync(&st, s.d_status, sizeof(unsigned int), cudaMemcpyDeviceToHost, s.stream));
         QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+        for (size_t i = 0; i < s.sp.size(); i++)
+            if (rebinned[i]) s.sp[i].n = s.h_count[i];
         if (s.timing) {
             cudaEvent_t end = nullptr;
             QP_CUDA_CHECK(s, cudaEventCreate(&end));

@@ -10,10 +10,8 @@ namespace qp {
 // off: photons fly straight without current, :155-252; leptons and ions are
 // pushed and deposit, :253-371).  The particle is read through perm from the
 // previous layout and written at its traversal position into the other
-// buffer.  Moves inside the cell deposit through the warp's run reduction,
-// moves across faces through the crossing list (deposit_split); the end
-// point of a crossing move is reached segment by segment as in the
-// reference.  newcell (-1 = erased, place(), plist.cpp:7-39) and the
+// buffer.  The current goes through the warp's segment-slot run reduction
+// (deposit_runs).  newcell (-1 = erased, place(), plist.cpp:7-39) and the
 // particles-per-new-cell histogram (count) feed the rebin.
 template <int PUSHER, int KIND, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
@@ -60,7 +58,7 @@ __global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, 
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
         }
     }
-    deposit_split<double, true>(f, g, pos, d, q, 0, 0, 0, active, a.xl, a.status);
+    deposit_runs(f, g, pos, d, q, 0, 0, 0, active, a.status);
     if (s < a.n) {
         if (live) {
             const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
@@ -518,8 +516,6 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     const int nb = push_blocks(s, sp.n, s.push_minblocks, &a.resident);
     Fields<double> f = fields64(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-    a.xl = make_cross_list<double>(s, sp.n, false);
-    cudaMemsetAsync(s.d_xcount, 0, CROSS_COUNTER_BYTES, s.stream);
 #define QP_LP(P, K)                                                                                          \
     if (s.push_minblocks == 2)                                                                                \
         k_push64<P, K, 2><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
@@ -532,10 +528,6 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
 #undef QP_LP
     s.launches++;
-    if (sp.kind != KIND_PHOTON) {
-        k_deposit_crossings<double><<<cross_grid(s), 256, 0, s.stream>>>(f, s.grid, a.xl, s.d_status);
-        s.launches++;
-    }
 }
 
 

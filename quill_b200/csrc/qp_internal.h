@@ -133,6 +133,7 @@ struct State {
     std::vector<Species> sp;
     DiagAccum* d_diag = nullptr;  // device accumulators
     DiagAccum* h_diag = nullptr;  // pinned host copy
+    int32_t* h_count = nullptr;   // pinned: each species' count after the step's rebin
     unsigned int* d_status = nullptr;
     void* scan_tmp = nullptr;     // block sums for the exclusive scans
     size_t scan_tmp_bytes = 0;
@@ -172,11 +173,9 @@ struct State {
     // rebin: entry 0 counts them, entries 1.. list them
     int32_t* long_list = nullptr;
     int64_t long_cap = 0;
-    // crossing list of the pushes (moves that cross a cell face, deposited by
-    // k_deposit_crossings): one buffer reused by every push, and its counter
-    void* xbuf = nullptr;
-    size_t xbuf_bytes = 0;
-    int* d_xcount = nullptr;
+    // one bit per cell: the rebin's front part of the cell has two entries or
+    // more (the front order's work)
+    uint32_t* crowd_bits = nullptr;
     // bumped by every change of the particle layout other than a step's
     // rebin, merging and the moving window (loads, restores, slab
     // replacements): the reference-order deposition then rebuilds its keys
@@ -223,17 +222,6 @@ inline int push_blocks(const State& s, int64_t n, int minb, int* resident) {
     return (int)(r * w);
 }
 
-// Sub-lists of the crossing list and the spacing of their counters (ints:
-// one 128-byte line per counter).
-constexpr int CROSS_LISTS = 128;
-constexpr int CROSS_COUNTER_STRIDE = 32;
-constexpr size_t CROSS_COUNTER_BYTES = (size_t)CROSS_LISTS * CROSS_COUNTER_STRIDE * sizeof(int);
-
-// Storage for a crossing list of `cap` records of `rec` bytes (grown as
-// needed, kept across steps); nullptr if it cannot be allocated (the pushes
-// then deposit crossing moves in place).
-void* cross_storage(State& s, int64_t cap, size_t rec);
-
 // Device copy of the full state into a snapshot / back (qp_checkpoint,
 // qp_restore, the adjoint's checkpoints); snapshot_free releases one.
 int snapshot_take(State& s, State::Snap& sn);
@@ -271,9 +259,11 @@ int launch_vacuum_mixed(State& s);
 
 // ---- rebin and scans (qp_rebin.cu) ----
 // Rebin after a push: count -> scan -> assign; leaves the new traversal
-// order in sp.perm / sp.cell_next and swaps buffers.  Returns the new count.
-// counted: sp.count already holds the particles per new cell (tiled push).
-int64_t rebin(State& s, int species, int64_t born, bool counted);
+// order in sp.perm / sp.cell_start and swaps buffers.  The new particle
+// count is copied to s.h_count[species] on the stream (the caller sets sp.n
+// after synchronising).  counted: sp.count already holds the particles per
+// new cell (tiled push).
+void rebin(State& s, int species, int64_t born, bool counted);
 // Cells with more particles than this are ordered by a block each.
 constexpr int REBIN_LONG_SEG = 64;
 // Loading (qp_load.cu)

@@ -208,119 +208,109 @@ __device__ __forceinline__ void warp_deposit_runs(const Fields<T>& f, const Grid
     }
 }
 
-// Moves that cross a cell face, kept for k_deposit_crossings: the start
-// point p (absolute cell units in FP64; the offset in the particle's cell in
-// mixed precision, whose cell is then in `cell`), the displacement d and the
-// weight q.  Structure of arrays split into CROSS_LISTS sub-lists of `cap`
-// slots each (sub-list l at [l cap, (l + 1) cap)), each claimed with its own
-// counter (counter[l * CROSS_COUNTER_STRIDE]): the warps of the push spread
-// their appends over the sub-lists instead of queueing on one address.
+// Current deposition of the whole warp's moves (deposition.cpp:41-356).
+// Every move's first segment starts in the particle's own cell, so the first
+// segments of a cell's particles share their 12 targets: they are summed over
+// runs of equal cells in the warp and added to J once per run.  Moves that
+// cross faces then deposit their further segments directly.  The segment
+// arithmetic per crossing case is the reference's (see jdeposition_to); p is
+// advanced segment by segment.  Every lane of the warp must call this; lanes
+// with active == false take no part.
 template <typename T>
-struct CrossList {
-    T *px, *py, *pz, *dx, *dy, *dz, *q;
-    int32_t* cell;  // mixed precision: the cell the offsets are relative to; FP64: nullptr
-    int* counter;
-    int cap;        // slots per sub-list
-};
-
-// Slots for the lanes with `want`, one atomic per warp on the warp's
-// sub-list; -1 for the other lanes and for slots beyond the sub-list's
-// capacity.  Every lane of the warp must call this.
-template <typename T>
-__device__ __forceinline__ int cross_slot(const CrossList<T>& xl, bool want) {
-    const unsigned m = __ballot_sync(0xffffffffu, want);
-    if (!m) return -1;
-    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-    const int l = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % CROSS_LISTS);
-    int base = 0;
-    if (lane == leader) base = atomicAdd(xl.counter + l * CROSS_COUNTER_STRIDE, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (!want) return -1;
-    const int slot = base + __popc(m & ((1u << lane) - 1u));
-    return slot < xl.cap ? l * xl.cap + slot : -1;
-}
-
-// Current deposition of the warp's moves with the crossing moves split off
-// (deposition.cpp:41-356).  A move that stays in its cell is one segment; the
-// moves of a cell's particles share their 12 targets, so they are summed
-// over runs of equal cells in the warp and added to J once per run.  A move
-// that crosses a face is appended to the crossing list, whose kernel
-// deposits all of its segments with full warps (about one move in six at
-// the benchmark's temperature: run in place, they held the whole warp).  If
-// the list is full the lane deposits its segments itself.
-//
-// p: start point, in the frame whose lattice is the cell lattice shifted by
-// (bi, bj, bk) (0 for absolute FP64 positions, the particle's cell for the
-// mixed offsets); on return the end point.  EXACT: the end point of a
-// crossing move is reached segment by segment with the reference's
-// arithmetic (FP64 parity); otherwise it is p + d.  Every lane of the warp
-// must call this; lanes with active == false take no part.
-template <typename T, bool EXACT>
-__device__ __forceinline__ void deposit_split(const Fields<T>& f, const Grid& g, T p[3], const T d[3], T q, int bi,
-                                              int bj, int bk, bool active, const CrossList<T>& xl,
-                                              unsigned int* status) {
-    bool cross = false;
-    int c1x = 0, c1y = 0, c1z = 0;
-    if (active) {
-        c1x = ifloor(p[0]); c1y = ifloor(p[1]); c1z = ifloor(p[2]);
-        cross = c1x != ifloor(p[0] + d[0]) || c1y != ifloor(p[1] + d[1]) || c1z != ifloor(p[2] + d[2]);
-    }
+__device__ __forceinline__ void deposit_runs(const Fields<T>& f, const Grid& g, T p[3], const T d[3], T q, int bi,
+                                             int bj, int bk, bool active, unsigned int* status) {
+    int c1x = 0, c1y = 0, c1z = 0, c2x = 0, c2y = 0, c2z = 0;
+    int nx_ = 0;
+    bool cx = false, cy = false, cz = false;
+    // case data: 1 crossing: u = first segment; 2: u0 = p1, u1 = p2 - p1,
+    // u2 = 1 - p2, fa / sa2 = axes of the first / second crossing; 3: u =
+    // (vx, vy, vz), the crossing fractions sorted descending
+    T u0 = T(0), u1 = T(0), u2 = T(0);
+    int fa = 0, sa2 = 0;
     T v[12];
     int corner = -1;
-    if (active && !cross) {
+    if (active) {
+        c1x = ifloor(p[0]); c1y = ifloor(p[1]); c1z = ifloor(p[2]);
+        c2x = ifloor(p[0] + d[0]); c2y = ifloor(p[1] + d[1]); c2z = ifloor(p[2] + d[2]);
+        cx = c1x != c2x; cy = c1y != c2y; cz = c1z != c2z;
+        nx_ = (int)cx + (int)cy + (int)cz;
+        T s[3];
+        if (nx_ == 0) {
+            s[0] = d[0]; s[1] = d[1]; s[2] = d[2];
+        } else if (nx_ == 1) {
+            const T pa = cx ? p[0] : (cy ? p[1] : p[2]);
+            const T da = cx ? d[0] : (cy ? d[1] : d[2]);
+            const int ma = cx ? max(c1x, c2x) : (cy ? max(c1y, c2y) : max(c1z, c2z));
+            const T sa = T(ma) - pa;
+            u0 = cx ? sa : d[0] * sa / da;
+            u1 = cy ? sa : d[1] * sa / da;
+            u2 = cz ? sa : d[2] * sa / da;
+            s[0] = u0; s[1] = u1; s[2] = u2;
+        } else if (nx_ == 2) {
+            const bool A0 = cx && !cy, B0 = cx && cy;
+            const T pA = A0 ? p[0] : p[1], dA = A0 ? d[0] : d[1];
+            const int mA = A0 ? max(c1x, c2x) : max(c1y, c2y);
+            const T pB = B0 ? p[0] : p[2], dB = B0 ? d[0] : d[2];
+            const int mB = B0 ? max(c1x, c2x) : max(c1z, c2z);
+            const T pa = (T(mA) - pA) / dA;
+            const T pb = (T(mB) - pB) / dB;
+            const bool bfirst = pa > pb;
+            const T p1 = bfirst ? pb : pa, p2 = bfirst ? pa : pb;
+            fa = bfirst ? (B0 ? 0 : 2) : (A0 ? 0 : 1);
+            sa2 = bfirst ? (A0 ? 0 : 1) : (B0 ? 0 : 2);
+            u0 = p1;
+            u1 = p2 - p1;
+            u2 = T(1) - p2;
+            s[0] = d[0] * u0; s[1] = d[1] * u0; s[2] = d[2] * u0;
+        } else {
+            const T path0 = (T(max(c1x, c2x)) - p[0]) / d[0];
+            const T path1 = (T(max(c1y, c2y)) - p[1]) / d[1];
+            const T path2 = (T(max(c1z, c2z)) - p[2]) / d[2];
+            sort3_desc(path0, path1, path2, u0, u1, u2);
+            s[0] = d[0] * u2; s[1] = d[1] * u2; s[2] = d[2] * u2;
+        }
+        const int w0[3] = {c1x, c1y, c1z};
         const int wi = bi + c1x, wj = bj + c1y, wk = bk + c1z;
         if (wi < 0 || wj < 0 || wk < 0 || wi + 1 >= g.nx || wj + 1 >= g.ny || wk + 1 >= g.nz) {
             atomicOr(status, (unsigned int)ST_BOUNDS);
         } else {
-            const int w0[3] = {c1x, c1y, c1z};
-            seg_values(p, d, q, w0, v);
+            seg_values(p, s, q, w0, v);
             corner = cidx(g, wi, wj, wk);
         }
-        p[0] = p[0] + d[0]; p[1] = p[1] + d[1]; p[2] = p[2] + d[2];
+        p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
     }
     if (corner < 0) {
 #pragma unroll
         for (int k = 0; k < 12; k++) v[k] = T(0);
     }
     warp_deposit_runs(f, g, corner, v);
-    const int slot = cross_slot(xl, cross);
-    if (!cross) return;
-    if (slot >= 0) {
-        xl.px[slot] = p[0]; xl.py[slot] = p[1]; xl.pz[slot] = p[2];
-        xl.dx[slot] = d[0]; xl.dy[slot] = d[1]; xl.dz[slot] = d[2];
-        xl.q[slot] = q;
-        if (xl.cell) xl.cell[slot] = cidx(g, bi, bj, bk);
-        if (EXACT) {
-            NullSink ns;
-            jdeposition_to(ns, g, p, d, q, bi, bj, bk, status);
-        } else {
-            p[0] = p[0] + d[0]; p[1] = p[1] + d[1]; p[2] = p[2] + d[2];
+    if (nx_ > 0) {
+        GlobalSink<T> sink{f};
+        int w[3] = {c1x, c1y, c1z};
+        for (int sg = 1; sg <= nx_; sg++) {
+            T s[3];
+            if (nx_ == 1) {
+                s[0] = d[0] - u0; s[1] = d[1] - u1; s[2] = d[2] - u2;
+                if (cx) w[0] = c2x;
+                if (cy) w[1] = c2y;
+                if (cz) w[2] = c2z;
+            } else if (nx_ == 2) {
+                const T fr = sg == 1 ? u1 : u2;
+                s[0] = d[0] * fr; s[1] = d[1] * fr; s[2] = d[2] * fr;
+                const int ax = sg == 1 ? fa : sa2;
+                if (ax == 0) w[0] = c2x;
+                if (ax == 1) w[1] = c2y;
+                if (ax == 2) w[2] = c2z;
+            } else {
+                const T fr = sg == 1 ? u1 - u2 : (sg == 2 ? u0 - u1 : T(1) - u0);
+                s[0] = d[0] * fr; s[1] = d[1] * fr; s[2] = d[2] * fr;
+                w[0] = ifloor(p[0] + T(0.5) * s[0]);
+                w[1] = ifloor(p[1] + T(0.5) * s[1]);
+                w[2] = ifloor(p[2] + T(0.5) * s[2]);
+            }
+            seg_dep(sink, g, p, s, q, w, bi, bj, bk, status);
+            p[0] = p[0] + s[0]; p[1] = p[1] + s[1]; p[2] = p[2] + s[2];
         }
-    } else {
-        jdeposition(f, g, p, d, q, bi, bj, bk, status);
-    }
-}
-
-// The crossing moves of one push: every segment of each move, one thread per
-// move; blockIdx.y is the sub-list, whose count is read on the device.
-template <typename T>
-__global__ void __launch_bounds__(256) k_deposit_crossings(Fields<T> f, Grid g, CrossList<T> xl,
-                                                           unsigned int* status) {
-    const int l = blockIdx.y;
-    const int n = min(xl.counter[l * CROSS_COUNTER_STRIDE], xl.cap);
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        const int64_t e = (int64_t)l * xl.cap + r;
-        T p[3] = {xl.px[e], xl.py[e], xl.pz[e]};
-        const T d[3] = {xl.dx[e], xl.dy[e], xl.dz[e]};
-        int bi = 0, bj = 0, bk = 0;
-        if (xl.cell) {
-            const int c = xl.cell[e];
-            bi = g.div_nynz.div(c);
-            const int rr = c - bi * g.nynz;
-            bj = g.div_nz.div(rr);
-            bk = rr - bj * g.nz;
-        }
-        jdeposition(f, g, p, d, xl.q[e], bi, bj, bk, status);
     }
 }
 
@@ -374,31 +364,7 @@ struct PushArgs {
     int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)
     unsigned int* status;
     DiagAccum* diag;
-    CrossList<double> xl;  // crossing moves of the non-QED push
 };
-
-// Crossing list over the storage of a State (host side): records for up to
-// a quarter of the n particles (about one move in six crosses a face at the
-// benchmark's temperature; beyond a sub-list's capacity the push deposits in
-// place).
-template <typename T>
-inline CrossList<T> make_cross_list(State& s, int64_t n, bool with_cell) {
-    CrossList<T> xl{};
-    xl.counter = s.d_xcount;
-    const int64_t per = (std::min<int64_t>(n, n / 4 + 256) + CROSS_LISTS - 1) / CROSS_LISTS;
-    const int64_t total = per * CROSS_LISTS;
-    const size_t rec = 7 * sizeof(T) + (with_cell ? sizeof(int32_t) : 0);
-    char* b = (char*)cross_storage(s, total, rec);
-    if (!b) return xl;  // cap 0: every crossing move deposits in place
-    T** arr[7] = {&xl.px, &xl.py, &xl.pz, &xl.dx, &xl.dy, &xl.dz, &xl.q};
-    for (int a = 0; a < 7; a++) *arr[a] = (T*)(b + (size_t)a * total * sizeof(T));
-    if (with_cell) xl.cell = (int32_t*)(b + 7 * (size_t)total * sizeof(T));
-    xl.cap = (int)per;
-    return xl;
-}
-
-// Launch geometry of k_deposit_crossings: blocks per sub-list, sub-lists.
-inline dim3 cross_grid(const State& s) { return dim3((unsigned)std::max(1, s.sm_count * 8 / CROSS_LISTS), CROSS_LISTS); }
 
 // Destination of particles born during a push (QED): slots
 // [base, cap) of the target species' output buffer, claimed with *counter.

@@ -21,7 +21,6 @@ struct PushArgs32 {
     int32_t* trn_dst;
     int dlo, dhi;  // the diagnostics count particles whose new cell has i in [dlo, dhi)
     int resident;  // blocks per group of the chunk order (chunk_range)
-    CrossList<float> xl;  // crossing moves (non-QED push)
 };
 
 __device__ __forceinline__ float wrap_offset(float o, int& shift) {
@@ -36,9 +35,8 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
 
 // The particles in traversal order as k_push64 takes them (a grid of a few
 // waves striding over block-sized chunks, diagnostics reduced once).  The
-// move runs in the particle's cell frame (offsets in [0, 1)); moves inside
-// the cell deposit through the warp's run reduction, moves across faces
-// through the crossing list (deposit_split), and the new offset is o + d.
+// move runs in the particle's cell frame (offsets in [0, 1)), the current
+// through the warp's segment-slot run reduction (deposit_runs).
 template <int PUSHER, int KIND, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
@@ -79,7 +77,7 @@ __global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, P
                 if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
             }
         }
-        deposit_split<float, false>(f, g, o, d, q, i0, j0, k0, active, a.xl, a.status);
+        deposit_runs(f, g, o, d, q, i0, j0, k0, active, a.status);
         if (s < a.n) {
             int i1 = i0, j1 = j0, k1 = k0;
             if (live) {
@@ -454,8 +452,6 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     const int nb = push_blocks(s, sp.n, s.push_minblocks_mixed, &a.resident);
     Fields<float> f = fields32(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-    a.xl = make_cross_list<float>(s, sp.n, true);
-    cudaMemsetAsync(s.d_xcount, 0, CROSS_COUNTER_BYTES, s.stream);
 #define QP_LP(P, K)                                                                                          \
     if (s.push_minblocks_mixed == 4)                                                                          \
         k_push32<P, K, 4><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
@@ -466,10 +462,6 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
 #undef QP_LP
     s.launches++;
-    if (sp.kind != KIND_PHOTON) {
-        k_deposit_crossings<float><<<cross_grid(s), 256, 0, s.stream>>>(f, s.grid, a.xl, s.d_status);
-        s.launches++;
-    }
 }
 
 static PStore32 store32(Species& sp, int b) {

@@ -112,13 +112,6 @@ struct GlobalSink {
     }
 };
 
-// A sink that drops the contributions: jdeposition_to with it only moves the
-// particle along its segments (the compiler removes the unused terms).
-struct NullSink {
-    template <typename T>
-    __device__ __forceinline__ void add(int, int, int, int, int, T) const {}
-};
-
 // x / 3.  In FP64 by Markstein's correction of a reciprocal product
 // (P. W. Markstein, "Computation of elementary functions on the IBM RISC
 // System/6000 processor", IBM J. Res. Develop. 34(1), 1990): r = RN(1/3) is

@@ -10,12 +10,12 @@
 // cos envelope, init.cpp:6-210) and the plasma films (film /
 // fill_cell_by_particles, init.cpp:402-646), runs the time loop of
 // main.cpp:2319-2432 through qp_step and writes QUILL's output files in its
-// formats so that python/resread.py reads them: log, N, energy, field slices
-// ex..bz (text or binary, fout.cpp:180-235), rho (and rho_p / rho_ph), and
-// phasespace (9 values per particle).
+// formats so that python/resread.py reads them (the list is below).
 //
-// Supported parameters: dx dy dz dt lambda ne xlength ylength zlength t_end
-// output_period a0 a0y a0z polarization xsigma ysigma zsigma x0 y0 z0 phase
+// Supported parameters: dx dy dz dt (either may be left out: automatic dx / dt
+// as main.cpp:2600-2615) lambda (cm, um, lambda_p) ne xlength ylength zlength
+// t_end output_period a0 a0y a0z P I W polarization xsigma ysigma zsigma x0
+// y0 z0 x0fout phase
 // f_envelope (cos | sscos | pearl | tophat | uniformB | focused |
 // focussedSSC) shenergy shphase phi_rotate r0 theta
 // xtarget ytarget ztarget lp_reflection f_reflection beam beam_particles Nb
@@ -29,8 +29,16 @@
 // ne_profile_r_coords ne_profile_r_values nfilm_y0 nfilm_y1 gradwidth_y
 // nelflow vlflow mcrlflow Tlflow nerflow vrflow mcrrflow Trflow catching
 // dump_photons n_tracks particles_to_track tr_init tr_start xtr1 ytr1 ztr1
-// xtr2 ytr2 ztr2 deps deps_ph neps neps_ph enthp_p enthp_ph enthp_i and two
-// additions: precision (fp64 | mixed) and seed.
+// xtr2 ytr2 ztr2 deps deps_p deps_ph deps_i neps neps_p neps_ph neps_i
+// enthp_p enthp_ph enthp_i j_components_for_output balancing_particle_weight
+// and three additions: precision (fp64 | mixed), seed, and current_order
+// (atomic | reference: J summed in the reference's order, FP64, QED off).
+//
+// Output files: log, N, energy, ex..bz, jx..jz (scaled by dx/dt), w, inv,
+// rho, rho_p, rho_ph, irho_<mcr>_, spectrum, spectrum_p, spectrum_ph,
+// spectrum_<mcr>_, phasespace, phasespace_p, phasespace_ph,
+// phasespace_<mcr>_, weights, mwcoordinate, energy_deleted, deleted*,
+// spectrum_deleted_ph, track files, each as the reference writes it.
 //
 //   qp_driver --initial-fields <file>
 //
@@ -172,8 +180,14 @@ struct Config {
     std::string particles_to_track = "epgi";
     bool tr_volume = false;        // tr_init = volume: n_tracks random cells in the box (main.cpp:1612-1690)
     double tr_start = 0, xtr1 = 0, ytr1 = 0, ztr1 = 0, xtr2 = 0, ytr2 = 0, ztr2 = 0;  // main.cpp:3419-3480
-    double deps_ph = 0;            // MeV, photon spectrum bin (main.cpp:3337-3359)
-    int neps_ph = 0;               // photon spectrum bins (main.cpp:3363-3370)
+    double deps = 0, deps_p = 0, deps_ph = 0, deps_i = 0;  // MeV (MeV per nucleon for ions), spectrum bins
+                                   // (main.cpp:3337-3362)
+    int neps = 0, neps_p = 0, neps_ph = 0, neps_i = 0;      // spectrum bins (main.cpp:3363-3373)
+    bool write_p = false, write_ph = false;  // particles_for_output ep / eph / epph (main.cpp:3390-3395)
+    bool write_j[3] = {false, false, false};  // j_components_for_output (main.cpp:2961-2978)
+    double x0fout = 0;             // yz plane of the field/density files at xlength - x0fout (main.cpp:2718-2731)
+    double balancing_particle_weight = 3.0;  // layer weights (main.cpp:3599)
+    bool ordered_current = false;  // addition: current_order = reference (J summed in the reference's order)
     int enthp_p = 0, enthp_ph = 0, enthp_i = 0;  // main.cpp:3374-3385
     std::string pmerging = "off";  // off | ti | nl (main.cpp:3397-3399)
     double crpc = 0;               // critical macro-particles per cell (main.cpp:3400-3401)
@@ -187,11 +201,26 @@ Config parse(const std::vector<Var>& v) {
     c.dt = find(v, "dt").value * 2 * PI;
     Var lam = find(v, "lambda");
     c.lambda = lam.units == "um" ? lam.value * 1e-4 : lam.value;  // cm
-    if (!(c.lambda > 0)) throw std::runtime_error("lambda must be given");
     Var ne = find(v, "ne");
     c.ne = ne.units == "ncr" ? ne.value * 1.11485e+13 / c.lambda / c.lambda : ne.value;
-    if (!(c.dx > 0 && c.dy > 0 && c.dz > 0 && c.dt > 0))
-        throw std::runtime_error("dx, dy, dz and dt must be given (automatic dt/dx of main.cpp:2603-2615 is not supported)");
+    // lambda in units of the plasma wavelength (main.cpp:2593-2599)
+    if (lam.units == "lambda_p") c.lambda = lam.value * std::sqrt(1.11485e13 / c.ne);
+    if (!(c.lambda > 0)) throw std::runtime_error("lambda must be given");
+    // automatic dt and dx (main.cpp:2600-2615): dt half the critical step of
+    // the plasma of density ne, dx the least dispersive stable step for dt
+    if (c.dt == 0 || c.dx == 0) {
+        if (!(c.ne > 0)) throw std::runtime_error("automatic dt / dx need ne");
+        const double k0 = std::sqrt(1.11485e+13 / c.lambda / c.lambda / c.ne);
+        if (c.dt == 0) {
+            c.dt = 0.5 * k0 * std::sqrt(4.04);
+            c.dx = 0;
+        }
+        if (c.dx == 0) {
+            c.dx = (1 + 1e-4) * c.dt / (1 - 1 / (k0 * k0) * c.dt * c.dt / 4.04);
+            if (c.dx < 0) throw std::runtime_error("Cannot calculate stable dx, reduce dt");
+        }
+    }
+    if (!(c.dx > 0 && c.dy > 0 && c.dz > 0 && c.dt > 0)) throw std::runtime_error("dy and dz must be given");
     auto len_lambda = [&](const char* n) {
         Var x = find(v, n);
         if (x.units == "um") return x.value * 1e-4 / c.lambda * 2 * PI;
@@ -226,6 +255,32 @@ Config parse(const std::vector<Var>& v) {
     c.x0 = length(find(v, "x0"), c.lambda);
     c.y00 = length(find(v, "y0"), c.lambda);
     c.z00 = length(find(v, "z0"), c.lambda);
+    c.x0fout = length(find(v, "x0fout"), c.lambda);
+    if (c.x0fout == 0) c.x0fout = c.xlength / 2;
+    // the amplitude from the power, the intensity or the energy
+    // (main.cpp:2735-2771); a0 given explicitly wins
+    {
+        const Var& P = find(v, "P");
+        double pv = P.value;
+        if (P.units == "PW") pv *= 1e22;
+        if (P.units == "TW") pv *= 1e19;
+        if (pv != 0) c.a0y = 5.27281e+17 * std::sqrt(2 * pv / (PI * 2.42161e+52 * c.ysigma * c.zsigma));
+        const Var& I = find(v, "I");
+        double iv = I.value;
+        if (I.units == "W/cm^2") iv *= 1e7;
+        if (iv != 0) c.a0y = 5.27281e+17 * c.lambda * std::sqrt(iv / (PI * 2.42161e+52));
+        const Var& W = find(v, "W");
+        double wv = W.value;
+        if (W.units == "J") wv *= 1e7;
+        if (wv != 0) {
+            // 3.691e4 = (mc^2)^2/(8 pi^2 e^2)
+            c.a0y = std::sqrt(wv / (3.691e4 * c.lambda * PI * std::sqrt(PI / 2) * c.xsigma * c.ysigma * c.zsigma / 4));
+            if (find(v, "polarization").units == "circular") {
+                c.a0y = c.a0y / std::sqrt(2);
+                c.a0z = c.a0y;
+            }
+        }
+    }
     if (find(v, "a0").value != 0) c.a0y = find(v, "a0").value;
     const Var& pol = find(v, "polarization");
     if (pol.units == "circular") { c.a0z = c.a0y; c.polarization = "circular"; }
@@ -392,9 +447,21 @@ Config parse(const std::vector<Var>& v) {
     }
     if (!find(v, "data_folder").units.empty()) c.data_folder = find(v, "data_folder").units;
     c.binary = find(v, "output_mode").units == "binary";
-    if (!find(v, "e_components_for_output").units.empty()) c.e_out = find(v, "e_components_for_output").units;
-    if (!find(v, "b_components_for_output").units.empty()) c.b_out = find(v, "b_components_for_output").units;
+    // field components written (main.cpp:2959-2978); the reference's default is none
+    c.e_out = find(v, "e_components_for_output").units;
+    c.b_out = find(v, "b_components_for_output").units;
+    if (c.e_out.empty()) c.e_out = "none";
+    if (c.b_out.empty()) c.b_out = "none";
+    {
+        const std::string jc = find(v, "j_components_for_output").units;
+        for (int a = 0; a < 3; a++) c.write_j[a] = jc.find("xyz"[a]) != std::string::npos;
+    }
     if (!find(v, "particles_for_output").units.empty()) c.particles_for_output = find(v, "particles_for_output").units;
+    c.write_p = c.particles_for_output == "ep" || c.particles_for_output == "epph";
+    c.write_ph = c.particles_for_output == "eph" || c.particles_for_output == "epph";
+    if (find(v, "balancing_particle_weight").value != 0 || !find(v, "balancing_particle_weight").units.empty())
+        c.balancing_particle_weight = find(v, "balancing_particle_weight").value;
+    c.ordered_current = find(v, "current_order").units == "reference";
     c.enthp = (int)find(v, "enthp").value; if (c.enthp <= 0) c.enthp = 1;
     c.enthp_p = (int)find(v, "enthp_p").value; if (c.enthp_p == 0) c.enthp_p = c.enthp;
     c.enthp_ph = (int)find(v, "enthp_ph").value; if (c.enthp_ph == 0) c.enthp_ph = c.enthp;
@@ -416,11 +483,23 @@ Config parse(const std::vector<Var>& v) {
     c.xtr1 = length(find(v, "xtr1"), c.lambda); c.ytr1 = length(find(v, "ytr1"), c.lambda); c.ztr1 = length(find(v, "ztr1"), c.lambda);
     c.xtr2 = length(find(v, "xtr2"), c.lambda); c.ytr2 = length(find(v, "ytr2"), c.lambda); c.ztr2 = length(find(v, "ztr2"), c.lambda);
     c.dump_photons = find(v, "dump_photons").units == "on" && c.qed;  // main.cpp:3545-3549
+    // spectra (main.cpp:3337-3373): bin widths in MeV (MeV per nucleon for
+    // ions), bin counts; each falls back to deps / neps
     auto mev = [&](const char* n) { const Var& w = find(v, n); return w.units == "mc^2" ? w.value * 0.511 : w.value; };
+    c.deps = mev("deps");
+    c.deps_p = mev("deps_p");
+    if (c.deps_p == 0) c.deps_p = c.deps;
     c.deps_ph = mev("deps_ph");
-    if (c.deps_ph == 0) c.deps_ph = mev("deps");
+    if (c.deps_ph == 0) c.deps_ph = c.deps;
+    c.deps_i = find(v, "deps_i").value;
+    if (c.deps_i == 0) c.deps_i = c.deps;
+    c.neps = (int)find(v, "neps").value;
+    c.neps_p = (int)find(v, "neps_p").value;
+    if (c.neps_p == 0) c.neps_p = c.neps;
     c.neps_ph = (int)find(v, "neps_ph").value;
-    if (c.neps_ph == 0) c.neps_ph = (int)find(v, "neps").value;
+    if (c.neps_ph == 0) c.neps_ph = c.neps;
+    c.neps_i = (int)find(v, "neps_i").value;
+    if (c.neps_i == 0) c.neps_i = c.neps;
     const std::string pr = find(v, "precision").units;
     if (pr == "mixed") c.precision = QP_PREC_MIXED;
     c.seed = (uint64_t)find(v, "seed").value;
@@ -1033,6 +1112,7 @@ int main(int argc, char** argv) {
     std::vector<double> i_del(icmr.size(), 0.0);
     int i_particle = 0, i_particle_p = 0, i_particle_ph = 0, i_particle_i = 0;
     if (r == QP_OK && c.n_tracks > 0) r = qp_set_tracking(h, 1);
+    if (r == QP_OK && c.ordered_current) r = qp_set_ordered_current(h, 1);
     std::ofstream fED;
     if (r == QP_OK && (c.catching || c.dump_photons)) {
         int64_t total = 0, np = 0;
@@ -1119,7 +1199,9 @@ int main(int argc, char** argv) {
     std::ofstream fN(c.data_folder + "/N"), fE(c.data_folder + "/energy");
     size_t out_i = 0;
     std::vector<double> slices(12 * ((size_t)g.nx * (g.ny + g.nz) + (size_t)g.ny * g.nz));
-    const int ix = (int)((c.xlength - c.xlength / 2) / c.dx);
+    // the yz plane of the field and density files: x = xlength - x0fout
+    // (get_xindex_in_sr, main.cpp:144-147)
+    const int ix = std::min(g.nx - 1, std::max(0, (int)((c.xlength - c.x0fout) / c.dx)));
     // moving window state (main.cpp:122, 2665-2679)
     int nmw = 1;
     const double t_add_mw = c.t_add_mw != 0 ? c.t_add_mw : sch.it.back() * c.dt;
@@ -1383,31 +1465,39 @@ int main(int argc, char** argv) {
             const size_t per = (size_t)g.nx * (g.ny + g.nz) + (size_t)g.ny * g.nz;
             qp_dump_field_slices(h, ix, slices.data());
             const size_t NC = (size_t)g.nc();
-            const char* en[3] = {"ex", "ey", "ez"};
-            const char* bn[3] = {"bx", "by", "bz"};
+            // currents (write_density with scale_j, main.cpp:2346-2349,
+            // 369-415): J scaled by dx / dt, as spatial_region::scale_j does
             for (int a = 0; a < 3; a++) {
-                const char comp = "xyz"[a];
-                if (c.e_out.find(comp) != std::string::npos)
-                    write_values(c.data_folder + "/" + en[a] + sfx, slices.data() + a * per, per, c.binary);
-                if (c.b_out.find(comp) != std::string::npos)
-                    write_values(c.data_folder + "/" + bn[a] + sfx, slices.data() + (3 + a) * per, per, c.binary);
+                if (!c.write_j[a]) continue;
+                std::vector<double> jv(slices.data() + (6 + a) * per, slices.data() + (7 + a) * per);
+                for (double& x2 : jv) x2 *= c.dx / c.dt;
+                write_values(c.data_folder + "/j" + std::string(1, "xyz"[a]) + sfx, jv.data(), per, c.binary);
             }
-            // densities: CIC deposition of every species (rhodeposition,
-            // deposition.cpp:358-429) into rho / rho_p / rho_ph
-            const char* names[3] = {"rho", "rho_p", "rho_ph"};
-            const int sps[3] = {sp_e, sp_pos, sp_ph};
-            for (int w = 0; w < 3; w++) {
-                if (sps[w] < 0) continue;
+            // every species in traversal order (each species' particles in the
+            // order of the reference's cell lists)
+            struct SpDump { std::vector<double> x, y, z, ux, uy, uz, g, q, chi; };
+            auto dump = [&](int si) {
+                SpDump D;
+                if (si < 0) return D;
                 int64_t np = 0;
-                qp_count_particles(h, sps[w], &np);
-                std::vector<double> x(np), y(np), z(np), q(np), rho(NC, 0.0);
-                if (np) qp_dump_particles(h, sps[w], np, x.data(), y.data(), z.data(), nullptr, nullptr, nullptr,
-                                          nullptr, q.data(), nullptr, nullptr);
-                for (int64_t t = 0; t < np; t++) {
-                    const int i = (int)std::floor(x[t]), j = (int)std::floor(y[t]), k = (int)std::floor(z[t]);
+                qp_count_particles(h, si, &np);
+                for (auto* vv : {&D.x, &D.y, &D.z, &D.ux, &D.uy, &D.uz, &D.g, &D.q, &D.chi}) vv->resize(np);
+                if (np) qp_dump_particles(h, si, np, D.x.data(), D.y.data(), D.z.data(), D.ux.data(), D.uy.data(),
+                                          D.uz.data(), D.g.data(), D.q.data(), D.chi.data(), nullptr);
+                return D;
+            };
+            const SpDump De_ = dump(sp_e), Dp_ = dump(c.write_p ? sp_pos : -1), Dph_ = dump(c.write_ph ? sp_ph : -1);
+            std::vector<SpDump> Di_(sp_pop.size());
+            for (size_t m = 0; m < sp_pop.size(); m++) Di_[m] = dump(sp_pop[m]);
+            // densities (compute_rho + rhodeposition, fout.cpp:7-40,
+            // deposition.cpp:358-429): cloud-in-cell charge of the particles
+            // in is_inside cells, in the reference's term order
+            auto cic = [&](const SpDump& D, std::vector<double>& rho) {
+                for (size_t t = 0; t < D.x.size(); t++) {
+                    const int i = (int)std::floor(D.x[t]), j = (int)std::floor(D.y[t]), k = (int)std::floor(D.z[t]);
                     if (!(i > 0 && i < g.nx - 2 && j > 0 && j < g.ny - 2 && k > 0 && k < g.nz - 2)) continue;
-                    const double xa = x[t] - i, xb = 1 - xa, ya = y[t] - j, yb = 1 - ya, za = z[t] - k, zb = 1 - za;
-                    const double qq = q[t];
+                    const double xa = D.x[t] - i, xb = 1 - xa, ya = D.y[t] - j, yb = 1 - ya, za = D.z[t] - k, zb = 1 - za;
+                    const double qq = D.q[t];
                     rho[g.at(i, j, k)] += qq * xb * yb * zb;
                     rho[g.at(i + 1, j, k)] += qq * xa * yb * zb;
                     rho[g.at(i, j + 1, k)] += qq * xb * ya * zb;
@@ -1417,19 +1507,83 @@ int main(int argc, char** argv) {
                     rho[g.at(i, j + 1, k + 1)] += qq * xb * ya * za;
                     rho[g.at(i + 1, j + 1, k + 1)] += qq * xa * ya * za;
                 }
-                write_slice(c.data_folder + "/" + names[w] + sfx, rho.data(), g, ix, c.binary);
-                // phasespace of the species selected by particles_for_output:
-                // q, x, y, z in lambda, ux, uy, uz, g, chi, every enthp-th
-                const char key = "epg"[w];
-                if (c.particles_for_output.find(key) != std::string::npos || (w == 2 && c.particles_for_output.find("ph") != std::string::npos)) {
-                    std::vector<double> ux(np), uy(np), uz(np), gg(np), chi(np);
-                    if (np) qp_dump_particles(h, sps[w], np, x.data(), y.data(), z.data(), ux.data(), uy.data(),
-                                              uz.data(), gg.data(), q.data(), chi.data(), nullptr);
-                    std::ofstream P(c.data_folder + "/phasespace" + std::string(w == 0 ? "" : (w == 1 ? "_p" : "_ph")) + sfx);
-                    for (int64_t t = 0; t < np; t += c.enthp)
-                        P << q[t] << '\n' << x[t] * c.dx / 2 / PI << '\n' << y[t] * c.dy / 2 / PI << '\n'
-                          << z[t] * c.dz / 2 / PI << '\n' << ux[t] << '\n' << uy[t] << '\n' << uz[t] << '\n'
-                          << gg[t] << '\n' << chi[t] << '\n';
+            };
+            {
+                // write_density(true, write_p, write_ph, "rho", "rho_p", "rho_ph", true)
+                const SpDump* ds[3] = {&De_, &Dp_, &Dph_};
+                const bool wr[3] = {true, c.write_p, c.write_ph};
+                const char* names[3] = {"rho", "rho_p", "rho_ph"};
+                for (int w = 0; w < 3; w++) {
+                    if (!wr[w]) continue;
+                    std::vector<double> rho(NC, 0.0);
+                    cic(*ds[w], rho);
+                    write_slice(c.data_folder + "/" + names[w] + sfx, rho.data(), g, ix, c.binary);
+                }
+                // ion densities irho_<cmr>_ (main.cpp:440-470, fout.cpp:662-704)
+                if (c.ions == "on" || c.ions == "positrons")
+                    for (size_t m = 0; m < sp_pop.size(); m++) {
+                        std::vector<double> rho(NC, 0.0);
+                        cic(Di_[m], rho);
+                        char b2[32];
+                        snprintf(b2, sizeof b2, "%g", icmr[m]);
+                        write_slice(c.data_folder + "/irho_" + b2 + "_" + sfx, rho.data(), g, ix, c.binary);
+                    }
+            }
+            // spectra and phase space (write_spectrum_phasespace,
+            // main.cpp:478-743): dN/deps in 1/MeV from the charge per energy
+            // bin; 9 values (q, x y z in lambda, ux uy uz, g, chi) of every
+            // particle after which a class's counter passes its enthp
+            {
+                const double vol = 1.11485e13 * c.lambda * c.dx * c.dy * c.dz / (8 * PI * PI * PI);
+                auto ps_put = [&](std::ofstream& o, const SpDump& D, size_t t) {
+                    o << D.q[t] << "\n" << c.dx * D.x[t] / (2 * PI) << "\n" << c.dy * D.y[t] / (2 * PI) << "\n"
+                      << c.dz * D.z[t] / (2 * PI) << "\n" << D.ux[t] << "\n" << D.uy[t] << "\n" << D.uz[t] << "\n"
+                      << D.g[t] << "\n" << D.chi[t] << "\n";
+                };
+                std::ofstream PSe(c.data_folder + "/phasespace" + sfx), PSp(c.data_folder + "/phasespace_p" + sfx),
+                    PSph(c.data_folder + "/phasespace_ph" + sfx);
+                std::vector<double> spec(std::max(c.neps, 0), 0.0), spec_p(std::max(c.neps_p, 0), 0.0),
+                    spec_ph(std::max(c.neps_ph, 0), 0.0);
+                for (size_t t = 0; t < De_.x.size(); t++) {
+                    const int ie = (int)((De_.g[t] - 1) * 0.511 / c.deps);
+                    if (ie > -1 && ie < c.neps) spec[ie] = spec[ie] - De_.q[t];
+                    if (++i_particle > c.enthp) { i_particle = 0; ps_put(PSe, De_, t); }
+                }
+                for (size_t t = 0; t < Dp_.x.size(); t++) {
+                    const int ie = (int)((Dp_.g[t] - 1) * 0.511 / c.deps_p);
+                    if (ie > -1 && ie < c.neps_p) spec_p[ie] = spec_p[ie] + Dp_.q[t];
+                    if (++i_particle_p > c.enthp_p) { i_particle_p = 0; ps_put(PSp, Dp_, t); }
+                }
+                for (size_t t = 0; t < Dph_.x.size(); t++) {
+                    const int ie = (int)(Dph_.g[t] * 0.511 / c.deps_ph);
+                    if (ie > -1 && ie < c.neps_ph) spec_ph[ie] = spec_ph[ie] + Dph_.q[t];
+                    if (++i_particle_ph > c.enthp_ph) { i_particle_ph = 0; ps_put(PSph, Dph_, t); }
+                }
+                std::vector<std::vector<double>> spec_i(sp_pop.size(), std::vector<double>(std::max(c.neps_i, 0), 0.0));
+                for (size_t m = 0; m < sp_pop.size(); m++) {
+                    char b2[32];
+                    snprintf(b2, sizeof b2, "%g", icmr[m]);
+                    std::ofstream PSi(c.data_folder + "/phasespace_" + b2 + "_" + sfx);
+                    const SpDump& D = Di_[m];
+                    for (size_t t = 0; t < D.x.size(); t++) {
+                        const int ie = (int)((D.g[t] - 1) * 0.511 * PROTON_MASS / c.deps_i);
+                        if (ie > -1 && ie < c.neps_i) spec_i[m][ie] += D.q[t];
+                        if (++i_particle_i > c.enthp_i) { i_particle_i = 0; ps_put(PSi, D, t); }
+                    }
+                }
+                std::ofstream S(c.data_folder + "/spectrum" + sfx), Sp(c.data_folder + "/spectrum_p" + sfx),
+                    Sph(c.data_folder + "/spectrum_ph" + sfx);
+                for (double& x2 : spec) { x2 = x2 * (vol / c.deps); S << x2 << "\n"; }
+                if (c.write_p)
+                    for (double& x2 : spec_p) { x2 = x2 * (vol / c.deps_p); Sp << x2 << "\n"; }
+                if (c.write_ph)
+                    for (double& x2 : spec_ph) { x2 = x2 * (vol / c.deps_ph); Sph << x2 << "\n"; }
+                for (size_t m = 0; m < sp_pop.size(); m++) {
+                    char b2[32];
+                    snprintf(b2, sizeof b2, "%g", icmr[m]);
+                    std::ofstream Si(c.data_folder + "/spectrum_" + b2 + "_" + sfx);
+                    const double norm_i = vol / (icmr[m] * c.deps_i);
+                    for (double& x2 : spec_i[m]) { x2 = x2 * norm_i; Si << x2 << "\n"; }
                 }
             }
             if (c.catching || c.dump_photons) {
@@ -1477,6 +1631,60 @@ int main(int argc, char** argv) {
                     const double norm = 1.11485e13 * c.lambda * c.dx * c.dy * c.dz / (8 * PI * PI * PI) / c.deps_ph;
                     for (double v2 : spec) S << v2 * norm << '\n';
                 }
+            }
+            // layer weights (write_layer_weights, main.cpp:997-1039): ny*nz
+            // plus balancing_particle_weight per particle of the layer
+            {
+                std::vector<int64_t> cnt(g.nx, 0);
+                qp_layer_counts(h, cnt.data());
+                std::ofstream Wt(c.data_folder + "/weights" + sfx);
+                for (int i = 0; i < g.nx; i++) {
+                    double wgt = (double)g.ny * g.nz;
+                    for (int64_t u = 0; u < cnt[i]; u++) wgt += c.balancing_particle_weight;
+                    Wt << wgt << "\n";
+                }
+            }
+            // fields (write_fields, main.cpp:745-995): the chosen E and B
+            // components, then w = E^2 + B^2 and inv = E^2 - B^2 from E and
+            // the B average at the slice nodes (e_to_particle / b_to_particle at
+            // integer positions, fout.cpp:437-561), always as text
+            const char* en[3] = {"ex", "ey", "ez"};
+            const char* bn[3] = {"bx", "by", "bz"};
+            for (int a = 0; a < 3; a++) {
+                const char comp = "xyz"[a];
+                if (c.e_out.find(comp) != std::string::npos)
+                    write_values(c.data_folder + "/" + en[a] + sfx, slices.data() + a * per, per, c.binary);
+                if (c.b_out.find(comp) != std::string::npos)
+                    write_values(c.data_folder + "/" + bn[a] + sfx, slices.data() + (3 + a) * per, per, c.binary);
+            }
+            {
+                // the yz plane of w / inv one layer lower when it is the last
+                std::vector<double> plane_lo;
+                if (ix == g.nx - 1) {
+                    plane_lo.resize(12 * per);
+                    qp_dump_field_slices(h, ix - 1, plane_lo.data());
+                }
+                auto val = [&](const std::vector<double>& src, int comp, size_t at) { return src[comp * per + at]; };
+                const size_t yz0 = (size_t)g.nx * (g.ny + g.nz);
+                std::ofstream Wf(c.data_folder + "/w" + sfx), If(c.data_folder + "/inv" + sfx);
+                auto put = [&](const std::vector<double>& src, size_t at) {
+                    const double ex = val(src, 0, at), ey = val(src, 1, at), ez = val(src, 2, at);
+                    const double bx = val(src, 9, at), by = val(src, 10, at), bz = val(src, 11, at);
+                    Wf << ex * ex + ey * ey + ez * ez + bx * bx + by * by + bz * bz << "\n";
+                    If << ex * ex + ey * ey + ez * ez - bx * bx - by * by - bz * bz << "\n";
+                };
+                for (int i = 0; i < g.nx; i++) {
+                    const int ii = i == g.nx - 1 ? i - 1 : i;  // the last region's last layer
+                    const size_t row = (size_t)ii * (g.ny + g.nz);
+                    for (int j = 0; j < g.ny; j++) put(slices, row + (j == g.ny - 1 ? j - 1 : j));
+                    for (int k = 0; k < g.nz; k++) put(slices, row + g.ny + (k == g.nz - 1 ? k - 1 : k));
+                }
+                const std::vector<double>& src = ix == g.nx - 1 ? plane_lo : slices;
+                for (int j = 0; j < g.ny; j++)
+                    for (int k = 0; k < g.nz; k++) {
+                        const int jj = j == g.ny - 1 ? j - 1 : j, kk = k == g.nz - 1 ? k - 1 : k;
+                        put(src, yz0 + (size_t)jj * g.nz + kk);
+                    }
             }
             out_i++;
         }
