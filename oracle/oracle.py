@@ -116,6 +116,8 @@ def _load(kind: str, flavour: str):
                                _D, _D, _D)
         api["f_init_focused"] = fn("f_init_focused", None, C.c_void_p, _D, _D, _D, _D, _D, _D, I, _D, _D, _D, I, _D,
                                    I, _D, _D, _D, _D)
+        api["set_catching"] = fn("set_catching", None, C.c_void_p, I)
+        api["energy_deleted"] = fn("energy_deleted", None, C.c_void_p, _DP)
     _LIBS[key] = api
     return api
 
@@ -307,6 +309,19 @@ class Region:
         """f_init_focused (init.cpp:212-385)."""
         self.api["f_init_focused"](self.h, a0y, a0z, xsigma, sigma0, x0, x1, int(b_sign), phase, y0, z0,
                                    int(append), phi, int(sscos), K, xtarget, ytarget, ztarget)
+
+    # --- catching (reference only) ----------------------------------------
+    def set_catching(self, on: bool):
+        """catching_enabled: erased particles' energy is summed by the
+        reference's update_energy_deleted (a process-wide flag)."""
+        self.api["set_catching"](self.h, int(bool(on)))
+
+    def energy_deleted(self) -> np.ndarray:
+        """Cumulative deleted energies in Joules: electrons, positrons,
+        photons, then each ion population."""
+        out = np.zeros(3 + self.n_ion)
+        self.api["energy_deleted"](self.h, _dp(out))
+        return out
 
     def layer_counts(self) -> np.ndarray:
         out = np.zeros(self.shape[0], dtype=np.int64)

@@ -457,4 +457,23 @@ double qref_partition_imbalance(const double* weights, int n, const int* part, i
     return calculate_partition_imbalance(wv, p, overlap);
 }
 
+// Catching (catching_enabled, main.cpp:3531-3534): particles erased outside
+// the region are recorded by delete_particle and their energy summed by
+// update_energy_deleted (low-level.cpp:247-313).  The flag is the process's.
+void qref_set_catching(void* h, int on) {
+    (void)h;
+    catching_enabled = on != 0;
+}
+
+// energy_e_deleted, energy_p_deleted, energy_ph_deleted, then
+// ienergy_deleted per ion population (Joules); the record list is dropped.
+void qref_energy_deleted(void* h, double* out) {
+    RefRegion* r = (RefRegion*)h;
+    out[0] = r->sr.energy_e_deleted;
+    out[1] = r->sr.energy_p_deleted;
+    out[2] = r->sr.energy_ph_deleted;
+    for (size_t m = 0; m < r->icmr.size(); m++) out[3 + m] = r->sr.ienergy_deleted[m];
+    r->sr.deleted_particles.clear();
+}
+
 }  // extern "C"

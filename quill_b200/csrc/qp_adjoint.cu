@@ -424,15 +424,16 @@ void record_inputs(State& s, Species& sp, int n, Lam7 rec, double* g_out) {
 // E (planes 0..2) and Bbar (9..11) at the step's start, FP64.
 cudaError_t record_fields(State& s, double* out) {
     const size_t nc = (size_t)s.grid.nc;
-    if (s.fp64) {
-        const double* F = (const double*)s.fields;
-        cudaError_t e = cudaMemcpyAsync(out, F, 3 * nc * 8, cudaMemcpyDeviceToDevice, s.stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out + 3 * nc, F + 9 * nc, 3 * nc * 8, cudaMemcpyDeviceToDevice, s.stream);
-        return e;
+    const int src[6] = {0, 1, 2, 9, 10, 11};
+    for (int a = 0; a < 6; a++) {
+        if (s.fp64) {
+            const cudaError_t e = cudaMemcpyAsync(out + a * nc, s.plane[src[a]], nc * 8, cudaMemcpyDeviceToDevice,
+                                                  s.stream);
+            if (e != cudaSuccess) return e;
+        } else {
+            k_widen<<<nblk(nc, 256), 256, 0, s.stream>>>((const float*)s.plane[src[a]], out + a * nc, nc);
+        }
     }
-    const float* F = (const float*)s.fields;
-    k_widen<<<nblk(3 * nc, 256), 256, 0, s.stream>>>(F, out, 3 * nc);
-    k_widen<<<nblk(3 * nc, 256), 256, 0, s.stream>>>(F + 9 * nc, out + 3 * nc, 3 * nc);
     return cudaGetLastError();
 }
 

@@ -178,7 +178,9 @@ static void free_state(State* s) {
 int snapshot_take(State& s, State::Snap& sn) {
     const size_t nc = (size_t)s.grid.nc;
     if (!sn.fields) QP_CUDA_CHECK(s, cudaMalloc(&sn.fields, 12 * nc * s.field_elem));
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(sn.fields, s.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
+    for (int a = 0; a < 12; a++)
+        QP_CUDA_CHECK(s, cudaMemcpyAsync((char*)sn.fields + a * nc * s.field_elem, s.plane[a], nc * s.field_elem,
+                                         cudaMemcpyDeviceToDevice, s.stream));
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
     for (auto& v : sn.arrays)
         for (void* p : v) cudaFree(p);
@@ -218,7 +220,9 @@ int snapshot_take(State& s, State::Snap& sn) {
 int snapshot_restore(State& s, State::Snap& sn) {
     if (!sn.valid) { s.err = "checkpoint slot is empty"; return QP_ERR_STATE; }
     const size_t nc = (size_t)s.grid.nc;
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(s.fields, sn.fields, 12 * nc * s.field_elem, cudaMemcpyDeviceToDevice, s.stream));
+    for (int a = 0; a < 12; a++)
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(s.plane[a], (char*)sn.fields + a * nc * s.field_elem, nc * s.field_elem,
+                                         cudaMemcpyDeviceToDevice, s.stream));
     for (size_t i = 0; i < s.sp.size(); i++) {
         Species& sp = s.sp[i];
         const int64_t cap = sn.cap[i];
@@ -345,8 +349,15 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;
     const size_t nc = (size_t)s.grid.nc;
-    if (e == cudaSuccess) e = cudaMalloc(&s.fields, 12 * nc * s.field_elem);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s.fields, 0, 12 * nc * s.field_elem, s.stream);
+    // 12 planes, and 6 more for the FDTD step's other E and B
+    const int nplanes = p.solver == QP_SOLVER_FDTD ? 18 : 12;
+    if (e == cudaSuccess) e = cudaMalloc(&s.fields, nplanes * nc * s.field_elem);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.fields, 0, nplanes * nc * s.field_elem, s.stream);
+    if (e == cudaSuccess) {
+        for (int a = 0; a < 12; a++) s.plane[a] = (char*)s.fields + a * nc * s.field_elem;
+        if (nplanes == 18)
+            for (int a = 0; a < 6; a++) s.spare_eb[a] = (char*)s.fields + (12 + a) * nc * s.field_elem;
+    }
     if (e == cudaSuccess) e = cudaMalloc(&s.d_diag, sizeof(DiagAccum));
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_diag, sizeof(DiagAccum), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_count, QP_MAX_SPECIES * sizeof(int32_t), cudaHostAllocDefault);
@@ -482,13 +493,13 @@ int qp_load_fields(qp_handle* h, const double* ex, const double* ey, const doubl
     // host or device planes (unified addressing decides the copy direction)
     if (s.fp64) {
         for (int a = 0; a < 6; a++)
-            QP_CUDA_CHECK(s, cudaMemcpyAsync((double*)s.fields + a * nc, src[a], nc * 8, cudaMemcpyDefault, s.stream));
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(s.plane[a], src[a], nc * 8, cudaMemcpyDefault, s.stream));
     } else {
         double* stage = nullptr;
         QP_CUDA_CHECK(s, cudaMalloc(&stage, nc * 8));
         for (int a = 0; a < 6; a++) {
             QP_CUDA_CHECK(s, cudaMemcpyAsync(stage, src[a], nc * 8, cudaMemcpyDefault, s.stream));
-            launch_f64_to_f32(s, stage, (float*)s.fields + a * nc, nc);
+            launch_f64_to_f32(s, stage, (float*)s.plane[a], nc);
         }
         QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
         cudaFree(stage);
@@ -754,7 +765,7 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
     for (int l = 0; l < nsteps; l++) {
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[0], s.stream));
         // padvance (advance.cpp:90-387): J = 0, push and deposit every species
-        QP_CUDA_CHECK(s, cudaMemsetAsync((char*)s.fields + 6 * nc * s.field_elem, 0, 3 * nc * s.field_elem, s.stream));
+        for (int a = 6; a < 9; a++) QP_CUDA_CHECK(s, cudaMemsetAsync(s.plane[a], 0, nc * s.field_elem, s.stream));
         QP_CUDA_CHECK(s, cudaMemsetAsync(s.d_diag, 0, sizeof(DiagAccum), s.stream));
         if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[1], s.stream));
         std::vector<int> born(s.sp.size(), 0);
@@ -862,15 +873,18 @@ int qp_dump_fields(qp_handle* h, double* out) {
     cudaPointerAttributes at{};
     const bool dev = cudaPointerGetAttributes(&at, out) == cudaSuccess && at.type == cudaMemoryTypeDevice;
     cudaGetLastError();
-    if (s.fp64) {
-        QP_CUDA_CHECK(s, cudaMemcpyAsync(out, s.fields, 12 * nc * 8, cudaMemcpyDefault, s.stream));
-    } else if (dev) {
-        launch_f32_to_f64(s, (const float*)s.fields, out, 12 * nc);
-    } else {
-        std::vector<float> tmp(12 * nc);
-        QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), s.fields, 12 * nc * 4, cudaMemcpyDeviceToHost, s.stream));
-        QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-        for (size_t c = 0; c < 12 * nc; c++) out[c] = tmp[c];
+    for (int a = 0; a < 12; a++) {
+        double* o = out + a * nc;
+        if (s.fp64) {
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(o, s.plane[a], nc * 8, cudaMemcpyDefault, s.stream));
+        } else if (dev) {
+            launch_f32_to_f64(s, (const float*)s.plane[a], o, nc);
+        } else {
+            std::vector<float> tmp(nc);
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(tmp.data(), s.plane[a], nc * 4, cudaMemcpyDeviceToHost, s.stream));
+            QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
+            for (size_t c = 0; c < nc; c++) o[c] = tmp[c];
+        }
     }
     QP_CUDA_CHECK(s, cudaGetLastError());
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));

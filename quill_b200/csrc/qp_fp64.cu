@@ -357,19 +357,11 @@ cudaError_t launch_qed_rates(int n, const double* d_in, double* d_out, double e_
     return cudaGetLastError();
 }
 
-static Fields<double> fields64(State& s) {
-    double* b = (double*)s.fields;
-    const size_t nc = (size_t)s.grid.nc;
-    Fields<double> f;
-    double** p[12] = {&f.ex, &f.ey, &f.ez, &f.bx, &f.by, &f.bz, &f.jx, &f.jy, &f.jz, &f.bex, &f.bey, &f.bez};
-    for (int a = 0; a < 12; a++) *p[a] = b + a * nc;
-    return f;
-}
 
 SolverCoef solver_coef(const qp_params& p);
 
 void launch_fields_fp64(State& s, int phase) {
-    Fields<double> f = fields64(s);
+    Fields<double> f = fields_of<double>(s);
     Coef<double> c(solver_coef(s.prm));
     dim3 blk(32, 8, 1);
     dim3 grd((s.grid.nz + 31) / 32, (s.grid.ny + 7) / 8, s.grid.nx);
@@ -395,7 +387,7 @@ void launch_fields_fp64(State& s, int phase) {
 }
 
 void zero_planes_fp64(State& s, const ZeroPlane* zp, int n) {
-    Fields<double> f = fields64(s);
+    Fields<double> f = fields_of<double>(s);
     for (int a = 0; a < n; a++) {
         int nu = zp[a].axis == 2 ? s.grid.ny : s.grid.nz;
         int nv = zp[a].axis == 0 ? s.grid.ny : s.grid.nx;
@@ -462,7 +454,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
         t1 = t0;
     }
     const int nb = push_blocks(s, sp.n, 2, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
-    Fields<double> f = fields64(s);
+    Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push64_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
     if (sp.kind == KIND_PHOTON) {
@@ -484,7 +476,7 @@ int launch_vacuum_fp64(State& s) {
     const double qv = 8 * PI * PI / dV * 2.818e-13 / p.lambda_cm;  // main.cpp:2324
     QedArgs qa = qed_args(s);
     AppendTarget<PStore64> t0 = target64(s, s.sp_e, false), t1 = target64(s, s.sp_p, false);
-    Fields<double> f = fields64(s);
+    Fields<double> f = fields_of<double>(s);
     const int nb = (s.grid.nc + 255) / 256;
     if (p.pusher == QP_PUSHER_VAY)
         k_vacuum64<QP_PUSHER_VAY><<<nb, 256, 0, s.stream>>>(f, s.grid, qa, p.dt, dV, qv, t0, t1, s.d_status);
@@ -514,7 +506,7 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     const int nb = push_blocks(s, sp.n, s.push_minblocks, &a.resident);
-    Fields<double> f = fields64(s);
+    Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LP(P, K)                                                                                          \
     if (s.push_minblocks == 2)                                                                                \

@@ -128,8 +128,13 @@ struct State {
     int fp64 = 1;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    void* fields = nullptr;       // 12 planes
+    void* fields = nullptr;       // allocation of the 12 planes (18 with the FDTD step's spare E and B)
     size_t field_elem = 8;
+    // the device address of each plane (ex ey ez bx by bz jx jy jz bex bey
+    // bez): the fused FDTD step writes E and B into the other of two plane
+    // sets and swaps these pointers
+    void* plane[12] = {nullptr};
+    void* spare_eb[6] = {nullptr};  // the other E and B planes (FDTD), nullptr otherwise
     std::vector<Species> sp;
     DiagAccum* d_diag = nullptr;  // device accumulators
     DiagAccum* h_diag = nullptr;  // pinned host copy
@@ -205,6 +210,26 @@ struct State {
         int64_t step_index = 0;
     } snap[4];
 };
+
+// The 12 field planes of the current step as typed device pointers.
+template <typename T>
+inline Fields<T> fields_of(const State& s) {
+    Fields<T> f;
+    T** p[12] = {&f.ex, &f.ey, &f.ez, &f.bx, &f.by, &f.bz, &f.jx, &f.jy, &f.jz, &f.bex, &f.bey, &f.bez};
+    for (int a = 0; a < 12; a++) *p[a] = (T*)s.plane[a];
+    return f;
+}
+// The same as an array (plane a = component a of ex .. bez).
+template <typename T>
+struct Planes {
+    T* p[12];
+};
+template <typename T>
+inline Planes<T> planes_of(const State& s) {
+    Planes<T> q;
+    for (int a = 0; a < 12; a++) q.p[a] = (T*)s.plane[a];
+    return q;
+}
 
 // Blocks of 256 threads for a push over n particles in block-sized chunks
 // (chunk_range): up to push_waves groups of `resident` blocks (the blocks

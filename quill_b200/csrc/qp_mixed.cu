@@ -373,19 +373,11 @@ __global__ void __launch_bounds__(256) k_vacuum32(Fields<float> f, Grid g, QedAr
     }
 }
 
-static Fields<float> fields32(State& s) {
-    float* b = (float*)s.fields;
-    const size_t nc = (size_t)s.grid.nc;
-    Fields<float> f;
-    float** p[12] = {&f.ex, &f.ey, &f.ez, &f.bx, &f.by, &f.bz, &f.jx, &f.jy, &f.jz, &f.bex, &f.bey, &f.bez};
-    for (int a = 0; a < 12; a++) *p[a] = b + a * nc;
-    return f;
-}
 
 SolverCoef solver_coef(const qp_params& p);
 
 void launch_fields_mixed(State& s, int phase) {
-    Fields<float> f = fields32(s);
+    Fields<float> f = fields_of<float>(s);
     Coef<float> c(solver_coef(s.prm));
     dim3 blk(32, 8, 1);
     constexpr int CPT = FieldCells<float>::value;
@@ -412,7 +404,7 @@ void launch_fields_mixed(State& s, int phase) {
 }
 
 void zero_planes_mixed(State& s, const ZeroPlane* zp, int n) {
-    Fields<float> f = fields32(s);
+    Fields<float> f = fields_of<float>(s);
     for (int a = 0; a < n; a++) {
         int nu = zp[a].axis == 2 ? s.grid.ny : s.grid.nz;
         int nv = zp[a].axis == 0 ? s.grid.ny : s.grid.nx;
@@ -450,7 +442,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     const int nb = push_blocks(s, sp.n, s.push_minblocks_mixed, &a.resident);
-    Fields<float> f = fields32(s);
+    Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LP(P, K)                                                                                          \
     if (s.push_minblocks_mixed == 4)                                                                          \
@@ -523,7 +515,7 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
         t1 = t0;
     }
     const int nb = push_blocks(s, sp.n, 2, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
-    Fields<float> f = fields32(s);
+    Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push32_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
     if (sp.kind == KIND_PHOTON) {
@@ -545,7 +537,7 @@ int launch_vacuum_mixed(State& s) {
     const double qv = 8 * PI * PI / dV * 2.818e-13 / p.lambda_cm;  // main.cpp:2324
     QedArgs qa = qed_args32(s);
     AppendTarget<PStore32> t0 = target32(s, s.sp_e, false), t1 = target32(s, s.sp_p, false);
-    Fields<float> f = fields32(s);
+    Fields<float> f = fields_of<float>(s);
     const int nb = (s.grid.nc + 255) / 256;
     if (p.pusher == QP_PUSHER_VAY)
         k_vacuum32<QP_PUSHER_VAY><<<nb, 256, 0, s.stream>>>(f, s.grid, qa, (float)p.dt, p.dt * dV, (float)qv, t0, t1,

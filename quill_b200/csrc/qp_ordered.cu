@@ -160,11 +160,12 @@ __global__ void __launch_bounds__(256) k_entries_scatter(int64_t n_particles, co
 // Each target's bucket ordered by key (insertion sort: buckets hold the
 // terms of the particles of the neighbouring cells, tens of entries) and
 // summed from zero in that order, as cj = cj + term does.
-__global__ void __launch_bounds__(256) k_entries_sum(int n_targets, const int32_t* __restrict__ start,
+__global__ void __launch_bounds__(256) k_entries_sum(int nc, const int32_t* __restrict__ start,
                                                      int64_t* __restrict__ skey, double* __restrict__ sval,
-                                                     double* __restrict__ J) {
+                                                     double* __restrict__ jx, double* __restrict__ jy,
+                                                     double* __restrict__ jz) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_targets) return;
+    if (t >= 3 * nc) return;
     const int b = start[t], e = start[t + 1];
     for (int i = b + 1; i < e; i++) {
         const int64_t k = skey[i];
@@ -180,7 +181,8 @@ __global__ void __launch_bounds__(256) k_entries_sum(int n_targets, const int32_
     }
     double acc = 0.0;
     for (int i = b; i < e; i++) acc = acc + sval[i];
-    J[t] = acc;
+    const int comp = t / nc;
+    (comp == 0 ? jx : (comp == 1 ? jy : jz))[t - comp * nc] = acc;
 }
 
 struct SpeciesOrder {
@@ -252,14 +254,6 @@ static PStore64 store64_of(Species& sp, int b) {
     return st;
 }
 
-static Fields<double> fields_of(State& s) {
-    double* b = (double*)s.fields;
-    const size_t nc = (size_t)s.grid.nc;
-    Fields<double> f;
-    double** p[12] = {&f.ex, &f.ey, &f.ez, &f.bx, &f.by, &f.bz, &f.jx, &f.jy, &f.jz, &f.bex, &f.bey, &f.bez};
-    for (int a = 0; a < 12; a++) *p[a] = b + a * nc;
-    return f;
-}
 
 void ordered_release(State& s) {
     State::Ordered& o = s.ord;
@@ -345,7 +339,7 @@ int ordered_push_all(State& s, double external_bz) {
     if (r != QP_OK) return r;
     State::Ordered& o = s.ord;
     const int ns = (int)s.sp.size();
-    Fields<double> f = fields_of(s);
+    Fields<double> f = fields_of<double>(s);
     int64_t base = 0;
     for (int si = 0; si < ns; si++) {
         Species& sp = s.sp[si];
@@ -390,7 +384,7 @@ int ordered_push_all(State& s, double external_bz) {
         const int64_t ne = base * ENT_PER_PARTICLE;
         k_entries_scatter<<<(int)((ne + 255) / 256), 256, 0, s.stream>>>(base, o.nent, o.tgt, o.key, o.val,
                                                                          o.jcount, o.skey, o.sval);
-        k_entries_sum<<<(nc3 + 255) / 256, 256, 0, s.stream>>>(nc3, o.jstart, o.skey, o.sval, f.jx);
+        k_entries_sum<<<(nc3 + 255) / 256, 256, 0, s.stream>>>(s.grid.nc, o.jstart, o.skey, o.sval, f.jx, f.jy, f.jz);
         s.launches += 2;
     }
     QP_CUDA_CHECK(s, cudaGetLastError());

@@ -95,32 +95,32 @@ extern "C" int qp_set_diag_range(qp_handle* h, int i_lo, int i_hi) {
 
 // 12 planes of the slab <-> 12 consecutive blocks of m doubles (device).
 template <typename T>
-__global__ void k_field_slab_out(const T* __restrict__ fields, size_t nc, size_t off, size_t m, double* __restrict__ out) {
+__global__ void k_field_slab_out(qp::Planes<T> f, size_t off, size_t m, double* __restrict__ out) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 12 * m) return;
     const size_t a = t / m, c = t - a * m;
-    out[t] = (double)fields[a * nc + off + c];
+    out[t] = (double)f.p[a][off + c];
 }
 
 template <typename T>
-__global__ void k_field_slab_in(const double* __restrict__ in, size_t nc, size_t off, size_t m, T* __restrict__ fields) {
+__global__ void k_field_slab_in(const double* __restrict__ in, size_t off, size_t m, qp::Planes<T> f) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 12 * m) return;
     const size_t a = t / m, c = t - a * m;
-    fields[a * nc + off + c] = (T)in[t];
+    f.p[a][off + c] = (T)in[t];
 }
 
 // Host or device buffers (the copies are cudaMemcpyDefault).
 extern "C" int qp_get_field_slab(qp_handle* h, int i0, int width, double* out12) {
     QP_SLAB_ENTRY(h, s);
     if (!slab_ok(s, i0, width) || !out12) return QP_ERR_ARG;
-    const size_t nc = (size_t)s.grid.nc, m = (size_t)width * s.grid.nynz, off = (size_t)i0 * s.grid.nynz;
+    const size_t m = (size_t)width * s.grid.nynz, off = (size_t)i0 * s.grid.nynz;
     if (m == 0) return QP_OK;
     double* d = nullptr;
     QP_CUDA_CHECK(s, cudaMalloc(&d, 12 * m * sizeof(double)));
     const unsigned nb = (unsigned)((12 * m + 255) / 256);
-    if (s.fp64) k_field_slab_out<double><<<nb, 256, 0, s.stream>>>((const double*)s.fields, nc, off, m, d);
-    else k_field_slab_out<float><<<nb, 256, 0, s.stream>>>((const float*)s.fields, nc, off, m, d);
+    if (s.fp64) k_field_slab_out<double><<<nb, 256, 0, s.stream>>>(qp::planes_of<double>(s), off, m, d);
+    else k_field_slab_out<float><<<nb, 256, 0, s.stream>>>(qp::planes_of<float>(s), off, m, d);
     s.launches++;
     const cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) cudaMemcpyAsync(out12, d, 12 * m * sizeof(double), cudaMemcpyDefault, s.stream);
@@ -133,15 +133,15 @@ extern "C" int qp_get_field_slab(qp_handle* h, int i0, int width, double* out12)
 extern "C" int qp_set_field_slab(qp_handle* h, int i0, int width, const double* in12) {
     QP_SLAB_ENTRY(h, s);
     if (!slab_ok(s, i0, width) || !in12) return QP_ERR_ARG;
-    const size_t nc = (size_t)s.grid.nc, m = (size_t)width * s.grid.nynz, off = (size_t)i0 * s.grid.nynz;
+    const size_t m = (size_t)width * s.grid.nynz, off = (size_t)i0 * s.grid.nynz;
     if (m == 0) return QP_OK;
     double* d = nullptr;
     QP_CUDA_CHECK(s, cudaMalloc(&d, 12 * m * sizeof(double)));
     cudaError_t e = cudaMemcpyAsync(d, in12, 12 * m * sizeof(double), cudaMemcpyDefault, s.stream);
     const unsigned nb = (unsigned)((12 * m + 255) / 256);
     if (e == cudaSuccess) {
-        if (s.fp64) k_field_slab_in<double><<<nb, 256, 0, s.stream>>>(d, nc, off, m, (double*)s.fields);
-        else k_field_slab_in<float><<<nb, 256, 0, s.stream>>>(d, nc, off, m, (float*)s.fields);
+        if (s.fp64) k_field_slab_in<double><<<nb, 256, 0, s.stream>>>(d, off, m, qp::planes_of<double>(s));
+        else k_field_slab_in<float><<<nb, 256, 0, s.stream>>>(d, off, m, qp::planes_of<float>(s));
         s.launches++;
         e = cudaGetLastError();
     }
@@ -177,20 +177,8 @@ extern "C" int qp_max_w(qp_handle* h, int i0, int i1, double* out) {
     unsigned long long* d = nullptr;
     QP_CUDA_CHECK(s, cudaMalloc(&d, sizeof(unsigned long long)));
     QP_CUDA_CHECK(s, cudaMemsetAsync(d, 0, sizeof(unsigned long long), s.stream));
-    const size_t nc = (size_t)s.grid.nc;
-    if (s.fp64) {
-        const double* b = (const double*)s.fields;
-        qp::Fields<double> f{};
-        f.ex = const_cast<double*>(b); f.ey = f.ex + nc; f.ez = f.ey + nc;
-        f.bx = f.ez + nc; f.by = f.bx + nc; f.bz = f.by + nc;
-        k_max_w<double><<<148 * 4, 256, 0, s.stream>>>(f, off, m, d);
-    } else {
-        const float* b = (const float*)s.fields;
-        qp::Fields<float> f{};
-        f.ex = const_cast<float*>(b); f.ey = f.ex + nc; f.ez = f.ey + nc;
-        f.bx = f.ez + nc; f.by = f.bx + nc; f.bz = f.by + nc;
-        k_max_w<float><<<148 * 4, 256, 0, s.stream>>>(f, off, m, d);
-    }
+    if (s.fp64) k_max_w<double><<<148 * 4, 256, 0, s.stream>>>(qp::fields_of<double>(s), off, m, d);
+    else k_max_w<float><<<148 * 4, 256, 0, s.stream>>>(qp::fields_of<float>(s), off, m, d);
     s.launches++;
     unsigned long long v = 0;
     cudaError_t e = cudaGetLastError();
@@ -206,7 +194,7 @@ extern "C" int qp_max_w(qp_handle* h, int i0, int i1, double* out) {
 // per component, for each i the line along y at k = nz/2 and the line along
 // z at j = ny/2, then the plane i = ix.
 template <typename T>
-__global__ void k_field_slices(const T* __restrict__ fields, int nx, int ny, int nz, int ix, size_t per,
+__global__ void k_field_slices(qp::Planes<T> f, int nx, int ny, int nz, int ix, size_t per,
                                double* __restrict__ out) {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 12 * per) return;
@@ -222,7 +210,7 @@ __global__ void k_field_slices(const T* __restrict__ fields, int nx, int ny, int
         const int j = (int)(v / nz), k = (int)(v - (size_t)j * nz);
         cell = ((long)ix * ny + j) * nz + k;
     }
-    out[t] = (double)fields[(size_t)a * nx * ny * nz + cell];
+    out[t] = (double)f.p[a][cell];
 }
 
 extern "C" int qp_dump_field_slices(qp_handle* h, int ix, double* out) {
@@ -233,8 +221,8 @@ extern "C" int qp_dump_field_slices(qp_handle* h, int ix, double* out) {
     double* d = nullptr;
     QP_CUDA_CHECK(s, cudaMalloc(&d, 12 * per * sizeof(double)));
     const unsigned nb = (unsigned)((12 * per + 255) / 256);
-    if (s.fp64) k_field_slices<double><<<nb, 256, 0, s.stream>>>((const double*)s.fields, nx, ny, nz, ix, per, d);
-    else k_field_slices<float><<<nb, 256, 0, s.stream>>>((const float*)s.fields, nx, ny, nz, ix, per, d);
+    if (s.fp64) k_field_slices<double><<<nb, 256, 0, s.stream>>>(qp::planes_of<double>(s), nx, ny, nz, ix, per, d);
+    else k_field_slices<float><<<nb, 256, 0, s.stream>>>(qp::planes_of<float>(s), nx, ny, nz, ix, per, d);
     s.launches++;
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 12 * per * sizeof(double), cudaMemcpyDefault, s.stream);

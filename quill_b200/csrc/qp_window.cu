@@ -61,7 +61,7 @@ int moving_window(State& s) {
     const int planes[9] = {0, 1, 2, 3, 4, 5, 9, 10, 11};
     const int nb = (int)((nc + 255) / 256);
     for (int a = 0; a < 9; a++) {
-        char* plane = (char*)s.fields + (size_t)planes[a] * nc * elem;
+        char* plane = (char*)s.plane[planes[a]];
         QP_CUDA_CHECK(s, cudaMemcpyAsync(s.window_scratch, plane + ynz * elem, keep * elem, cudaMemcpyDeviceToDevice,
                                          s.stream));
         if (s.fp64)

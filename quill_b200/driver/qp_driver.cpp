@@ -717,6 +717,15 @@ struct Parts {
         x.push_back(X); y.push_back(Y); z.push_back(Z);
         ux.push_back(UX); uy.push_back(UY); uz.push_back(UZ); g.push_back(G); q.push_back(Q);
     }
+    // The order place() leaves the particles in: each is inserted at the head
+    // of its cell's list (plist.cpp:22-39), so within a cell the last one
+    // created comes first.  qp_load_particles keeps the given order within
+    // a cell, so the particles are handed over last first.
+    Parts head_order() const {
+        Parts r = *this;
+        for (auto* v : {&r.x, &r.y, &r.z, &r.ux, &r.uy, &r.uz, &r.g, &r.q}) std::reverse(v->begin(), v->end());
+        return r;
+    }
 };
 
 // fill_cell_by_particles (init.cpp:402-478): a regular in-cell lattice of
@@ -1087,8 +1096,9 @@ int main(int argc, char** argv) {
         film(c, g, c.films[f], E, pi >= 0 ? &I[pi] : nullptr, pi >= 0 ? icmr[pi] : 0,
              c.ions == "positrons" ? &Pz : nullptr, rng, 0, false, profiled);
     }
-    auto load = [&](int s, Parts& P) {
-        if (r != QP_OK || P.x.empty()) return;
+    auto load = [&](int s, const Parts& P0) {
+        if (r != QP_OK || P0.x.empty()) return;
+        const Parts P = P0.head_order();
         r = qp_load_particles(h, s, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
                               P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
     };
@@ -1235,10 +1245,11 @@ int main(int argc, char** argv) {
                  c.ions == "positrons" ? &Pm : nullptr, rng, nmw * c.dx, true);
         }
         int rr = QP_OK;
-        auto put = [&](int sp, Parts& P) {
-            if (rr == QP_OK && !P.x.empty())
-                rr = qp_load_particles(h, sp, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
-                                       P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
+        auto put = [&](int sp, const Parts& P0) {
+            if (rr != QP_OK || P0.x.empty()) return;
+            const Parts P = P0.head_order();
+            rr = qp_load_particles(h, sp, (int64_t)P.x.size(), P.x.data(), P.y.data(), P.z.data(), P.ux.data(),
+                                   P.uy.data(), P.uz.data(), P.g.data(), P.q.data(), nullptr);
         };
         put(sp_e, Em);
         for (size_t k = 0; k < mcrs.size(); k++) put(sp_pop[k], Im[k]);
@@ -1377,7 +1388,7 @@ int main(int argc, char** argv) {
                 }
                 return Q;
             };
-            Parts Eq = keep_inside(Ef), Iq = keep_inside(If);
+            const Parts Eq = keep_inside(Ef).head_order(), Iq = keep_inside(If).head_order();
             if (!Eq.x.empty())
                 rr = qp_load_particles(h, sp_e, (int64_t)Eq.x.size(), Eq.x.data(), Eq.y.data(), Eq.z.data(),
                                        Eq.ux.data(), Eq.uy.data(), Eq.uz.data(), Eq.g.data(), Eq.q.data(), nullptr);
@@ -1638,10 +1649,13 @@ int main(int argc, char** argv) {
                 std::vector<int64_t> cnt(g.nx, 0);
                 qp_layer_counts(h, cnt.data());
                 std::ofstream Wt(c.data_folder + "/weights" + sfx);
+                // the reference gathers region 0's layers up to nx - nx_ich/2
+                // whatever n_sr is (main.cpp:1005-1008): with one region its
+                // last 4 layers stay 0
                 for (int i = 0; i < g.nx; i++) {
                     double wgt = (double)g.ny * g.nz;
                     for (int64_t u = 0; u < cnt[i]; u++) wgt += c.balancing_particle_weight;
-                    Wt << wgt << "\n";
+                    Wt << (i < g.nx - 4 ? wgt : 0.0) << "\n";
                 }
             }
             // fields (write_fields, main.cpp:745-995): the chosen E and B

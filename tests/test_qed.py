@@ -1,7 +1,9 @@
 """QED: device rate functions against the reference's (mc.cpp:26-116), the
 counter-based random numbers against the published Philox4x32-10 answers,
 and photon-emission / pair-creation statistics of whole steps against the
-reference run with 16 seeds (agreement within 3 sigma)."""
+reference run with 16 seeds (agreement within 3 sigma): photon, electron
+and positron counts and energies, and their energy spectra bin by bin with
+the reference's spectrum normalisation."""
 import numpy as np
 import pytest
 
@@ -79,9 +81,29 @@ def _sort(p):
     return {k: v[o] for k, v in p.items()}
 
 
+# energy bins of the spectra, as write_spectrum_phasespace bins them
+# (main.cpp:535-600): photons by g * 0.511 / deps_ph, leptons by
+# (g - 1) * 0.511 / deps, weight q (its magnitude), normalised to dN/deps in
+# 1/MeV with the reference's factor (main.cpp:683-700)
+DEPS_PH, NEPS_PH = 100.0, 24      # MeV: the 2.04 GeV pair photons and the emitted ones below 511 MeV
+DEPS_L, NEPS_L = 100.0, 24        # MeV: electrons from 511 MeV down, pairs up to 2 GeV
+LAMBDA_CM = 1e-4
+SPEC_NORM = 1.11485e13 * LAMBDA_CM * DX * DX * DX / (8 * np.pi ** 3)
+
+
+def _spectrum(p, photon, deps, neps):
+    e = (p["g"] if photon else p["g"] - 1) * 0.511 / deps
+    i = e.astype(int)
+    keep = (i > -1) & (i < neps)
+    return np.bincount(i[keep], weights=np.abs(p["q"][keep]), minlength=neps) * SPEC_NORM / deps
+
+
 def _stats_from(parts_e, parts_p, parts_ph):
     return {"n_ph": parts_ph["x"].size, "e_ph": parts_ph["g"].sum(), "n_p": parts_p["x"].size,
-            "e_e": parts_e["g"].sum()}
+            "e_e": parts_e["g"].sum(),
+            "spec_ph": _spectrum(parts_ph, True, DEPS_PH, NEPS_PH),
+            "spec_e": _spectrum(parts_e, False, DEPS_L, NEPS_L),
+            "spec_p": _spectrum(parts_p, False, DEPS_L, NEPS_L)}
 
 
 def _ref_stats(seed):
@@ -136,6 +158,28 @@ def test_qed_step_statistics_vs_reference(precision):
         sig = np.sqrt(r.var(ddof=1) / r.size + v.var(ddof=1) / v.size)
         assert abs(v.mean() - r.mean()) <= 3 * sig + 1e-12 * abs(r.mean()), (key, v.mean(), r.mean(), sig)
         assert r.mean() > 0
+    # spectra, bin by bin (photons, electrons, positrons): the difference of
+    # the 16-seed means within 3 sigma of that difference; with about 70
+    # populated bins tested at 3 sigma, one exceedance is allowed (its
+    # expected number by chance is about 0.2), none beyond 4 sigma.  Bins that
+    # are empty in both runs are skipped.
+    over3 = []
+    tested = 0
+    for key in ("spec_ph", "spec_e", "spec_p"):
+        r = np.array([x[key] for x in ref])
+        v = np.array([x[key] for x in gpu])
+        assert r.sum() > 0, key
+        for b in range(r.shape[1]):
+            if not (r[:, b].any() or v[:, b].any()):
+                continue
+            tested += 1
+            sig = np.sqrt(r[:, b].var(ddof=1) / r.shape[0] + v[:, b].var(ddof=1) / v.shape[0])
+            dev = abs(v[:, b].mean() - r[:, b].mean())
+            assert dev <= 4 * sig + 1e-12 * abs(r[:, b].mean()), (key, b, v[:, b].mean(), r[:, b].mean(), sig)
+            if dev > 3 * sig + 1e-12 * abs(r[:, b].mean()):
+                over3.append((key, b))
+    assert tested >= 20
+    assert len(over3) <= 1, over3
 
 
 # Schwinger pairs from a uniform Ex of 0.073 e_s: about 1e-2 pairs per
