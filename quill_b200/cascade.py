@@ -2,6 +2,7 @@
 
     python -m quill_b200.cascade [--grid 256 256 256] [--steps 600]
                                  [--precision fp64|mixed] [--seed 0] [--every 50]
+                                 [--crpc 1.5]
 
 Five-point solver, Vay pusher, QED on (photon emission, Breit-Wheeler pairs,
 vacuum pairs): two counter-propagating circularly polarised pulses (a0 =
@@ -12,10 +13,20 @@ of electrons and protons, dx = lambda/32, dt = 0.3 dx (the five-point scheme
 needs dt below about 0.35 dx on cubic cells).  The state is generated on the
 GPU (seeded); positrons and photons start empty.
 
+The cascade multiplies the particles about tenfold every 50 steps at this
+field; as the reference does in such runs, particle merging bounds them:
+after a step in which a species holds more than crpc macro-particles per
+cell, that species is thinned by the reference's "nl" merging
+(evaluate_merging_condition / pmerging, main.cpp:1691-1748, mc.cpp:198-462:
+deletion probability (n - crpc cells) / n weighted by the particle's charge,
+survivors' weights raised so that the species' charge is kept) before the
+next step.
+
 Prints, every `--every` steps, the macro-particles per species and the
-elapsed device time, and at the end one JSON line: particle-steps/s over the
-whole run (the particles pushed in each step, summed, over the CUDA-event
-time of all steps), the final counts, and the peak particle count.
+elapsed time (CUDA events on the stream, host work between steps included),
+and at the end one JSON line: particle-steps/s over the whole run (the
+particles pushed in each step, summed, over that time, merging included),
+the final counts, and the peak particle count.
 """
 from __future__ import annotations
 
@@ -24,7 +35,7 @@ import json
 import time
 
 
-def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, device=0, quiet=False):
+def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crpc=1.5, device=0, quiet=False):
     import torch
 
     from . import workloads as W
@@ -60,31 +71,38 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, dev
     n0 = sum(counts)
     if not quiet:
         print(f"{case.nx}x{case.ny}x{case.nz} cells, {precision}, start: {counts} (e, p+, e+, photons)", flush=True)
-    pushed, peak, ms_total = 0, n0, 0.0
+    pushed, peak, ms_total, merges = 0, n0, 0.0, 0
     history = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    done = 0
+    crnp = crpc * case.nx * case.ny * case.nz
     t_wall = time.perf_counter()
-    while done < steps:
-        k = min(every, steps - done)
-        n_start = sum(reg.count(i) for i in range(len(species)))
-        e0.record(stream)
-        d = reg.step(k)
-        e1.record(stream)
-        e1.synchronize()
-        ms_total += e0.elapsed_time(e1)
-        pushed += n_start + sum(sum(x.n_macro[i] for i in range(len(species))) for x in d[:-1])
-        done += k
-        counts = [reg.count(i) for i in range(len(species))]
+    counts = [reg.count(i) for i in range(len(species))]
+    e0.record(stream)
+    for step in range(1, steps + 1):
+        pushed += sum(counts)
+        d = reg.step(1)[0]
+        counts = [int(d.n_macro[i]) for i in range(len(species))]
         peak = max(peak, sum(counts))
-        history.append({"step": done, "counts": counts, "ms": ms_total})
-        if not quiet:
-            print(f"step {done}: {counts}, {sum(counts):.3e} particles, {ms_total / 1e3:.2f} s device", flush=True)
+        # the nl merging condition per species (main.cpp:1691-1748)
+        ppd = [(n - crnp) / n if n > crnp else 0.0 for n in counts]
+        if any(v > 0 for v in ppd):
+            reg.pmerging("nl", ppd)
+            merges += 1
+            counts = [reg.count(i) for i in range(len(species))]
+        if step % every == 0 or step == steps:
+            e1.record(stream)
+            e1.synchronize()
+            ms_total = e0.elapsed_time(e1)
+            history.append({"step": step, "counts": counts, "ms": ms_total, "merges": merges})
+            if not quiet:
+                print(f"step {step}: {counts}, {sum(counts):.3e} particles, {ms_total / 1e3:.2f} s, "
+                      f"{merges} merging passes", flush=True)
     reg.close()
     return {"metric": "QED particle-steps/s", "value": pushed / (ms_total * 1e-3), "unit": "particle-steps/s",
             "precision": precision, "grid": list(grid), "steps": steps, "seconds_device": ms_total / 1e3,
             "seconds_wall": time.perf_counter() - t_wall, "particles_start": n0, "particles_end": sum(counts),
-            "particles_peak": peak, "counts_end": counts, "history": history}
+            "particles_peak": peak, "counts_end": counts, "merging_passes": merges, "crpc": crpc,
+            "history": history}
 
 
 def _main():
@@ -94,8 +112,10 @@ def _main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--every", type=int, default=50)
+    ap.add_argument("--crpc", type=float, default=1.5,
+                    help="macro-particles per cell above which a species is merged")
     a = ap.parse_args()
-    r = run(tuple(a.grid), a.steps, a.precision, a.seed, a.every)
+    r = run(tuple(a.grid), a.steps, a.precision, a.seed, a.every, a.crpc)
     print(json.dumps(r), flush=True)
 
 

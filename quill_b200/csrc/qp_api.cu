@@ -161,8 +161,6 @@ static void free_state(State* s) {
     cudaFreeHost(s->h_count);
     cudaFree(s->d_status);
     cudaFree(s->long_list);
-    cudaFree(s->crowd_bits);
-    s->crowd_bits = nullptr;
     cudaFree(s->window_scratch);
     catch_release(*s);
     ordered_release(*s);
@@ -349,15 +347,10 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     s.own_stream = true;
     const size_t nc = (size_t)s.grid.nc;
-    // 12 planes, and 6 more for the FDTD step's other E and B
-    const int nplanes = p.solver == QP_SOLVER_FDTD ? 18 : 12;
-    if (e == cudaSuccess) e = cudaMalloc(&s.fields, nplanes * nc * s.field_elem);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s.fields, 0, nplanes * nc * s.field_elem, s.stream);
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess) e = cudaMalloc(&s.fields, 12 * nc * s.field_elem);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s.fields, 0, 12 * nc * s.field_elem, s.stream);
+    if (e == cudaSuccess)
         for (int a = 0; a < 12; a++) s.plane[a] = (char*)s.fields + a * nc * s.field_elem;
-        if (nplanes == 18)
-            for (int a = 0; a < 6; a++) s.spare_eb[a] = (char*)s.fields + (12 + a) * nc * s.field_elem;
-    }
     if (e == cudaSuccess) e = cudaMalloc(&s.d_diag, sizeof(DiagAccum));
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_diag, sizeof(DiagAccum), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&s.h_count, QP_MAX_SPECIES * sizeof(int32_t), cudaHostAllocDefault);
@@ -365,7 +358,6 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     if (e == cudaSuccess) e = cudaMemsetAsync(s.d_status, 0, sizeof(unsigned int), s.stream);
     s.scan_tmp_bytes = ((nc + 4095) / 4096 + 2) * sizeof(int32_t);
     if (e == cudaSuccess) e = cudaMalloc(&s.scan_tmp, s.scan_tmp_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&s.crowd_bits, (nc + 31) / 32 * sizeof(uint32_t));
     int ion = 0;
     s.sp.resize(p.n_species);
     for (int i = 0; i < p.n_species && e == cudaSuccess; i++) {

@@ -128,13 +128,10 @@ struct State {
     int fp64 = 1;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    void* fields = nullptr;       // allocation of the 12 planes (18 with the FDTD step's spare E and B)
+    void* fields = nullptr;       // allocation of the 12 planes
     size_t field_elem = 8;
-    // the device address of each plane (ex ey ez bx by bz jx jy jz bex bey
-    // bez): the fused FDTD step writes E and B into the other of two plane
-    // sets and swaps these pointers
+    // the device address of each plane (ex ey ez bx by bz jx jy jz bex bey bez)
     void* plane[12] = {nullptr};
-    void* spare_eb[6] = {nullptr};  // the other E and B planes (FDTD), nullptr otherwise
     std::vector<Species> sp;
     DiagAccum* d_diag = nullptr;  // device accumulators
     DiagAccum* h_diag = nullptr;  // pinned host copy
@@ -178,9 +175,6 @@ struct State {
     // rebin: entry 0 counts them, entries 1.. list them
     int32_t* long_list = nullptr;
     int64_t long_cap = 0;
-    // one bit per cell: the rebin's front part of the cell has two entries or
-    // more (the front order's work)
-    uint32_t* crowd_bits = nullptr;
     // bumped by every change of the particle layout other than a step's
     // rebin, merging and the moving window (loads, restores, slab
     // replacements): the reference-order deposition then rebuilds its keys

@@ -92,6 +92,10 @@ __device__ __forceinline__ T qed_w(T g, T& r, T chi, T e_s) {
         scale = r_max;
     }
     const T d = r / ((T(1) - r) * chi);
+    // FP32 (denormals flushed): (1 - r) chi can underflow to 0 where FP64
+    // keeps it; d is then infinite and the formula 0 * NaN.  The rate of
+    // that limit is 0.
+    if (sizeof(T) == 4 && !(d <= T(3.0e38))) return T(0);
     const T a = pow(d, T(1) / T(3));
     const T kappa = a * a;
     const T k3 = (kappa + T(0.80049)) * (kappa + T(0.80049)) * (kappa + T(0.80049));
@@ -106,6 +110,7 @@ template <typename T>
 __device__ __forceinline__ T qed_tilde_w(T g, T r, T chi, T e_s) {
     if (chi == T(0) || r * g < T(1) || (T(1) - r) * g < T(1)) return T(0);
     const T d = T(1) / (r * (T(1) - r) * chi);
+    if (sizeof(T) == 4 && !(d <= T(3.0e38))) return T(0);  // as qed_w
     const T a = pow(d, T(1) / T(3));
     const T kappa = a * a;
     const T k3 = (kappa + T(0.80049)) * (kappa + T(0.80049)) * (kappa + T(0.80049));

@@ -24,13 +24,9 @@ namespace qp {
 //     scan), so the stayers land in ascending order with no atomics; an
 //     arrival or a born particle (t >= n) claims the next slot from the front
 //     of the range (one atomic per run of equal cells in the warp);
-//     the claim that brings a cell's front part to two entries marks the
-//     cell in a bitmap;
-//  2. front order (thread per cell): the claimed front part of a marked cell
-//     is put in list order, born ascending then arrivals DESCENDING by old
-//     position; it is short (the arrivals of one step), long parts go to a
-//     block each.  Parts of 0 or 1 entry need no ordering: their cells read
-//     one bitmap word per warp and nothing else.
+//  2. front order (thread per cell): the claimed front part is put in list
+//     order, born ascending then arrivals DESCENDING by old position; it is
+//     short (the arrivals of one step), long parts go to a block each.
 
 __device__ __forceinline__ long long front_key(int x, int n_old) {
     if (x >= n_old) return (long long)x;                       // born
@@ -52,11 +48,11 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
                                                        const int32_t* __restrict__ cs,
                                                        const int32_t* __restrict__ start,
                                                        int32_t* __restrict__ cursor, int32_t* __restrict__ perm,
-                                                       uint32_t* __restrict__ crowd, unsigned int* status) {
+                                                       unsigned int* status) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32 * REBIN_CHUNKS;
-    int key[REBIN_CHUNKS], e[REBIN_CHUNKS], end[REBIN_CHUNKS], b[REBIN_CHUNKS], sb[REBIN_CHUNKS];
+    int key[REBIN_CHUNKS], e[REBIN_CHUNKS], end[REBIN_CHUNKS], b[REBIN_CHUNKS];
 #pragma unroll
     for (int h = 0; h < REBIN_CHUNKS; h++) {
         const int t = w0 + 32 * h + lane;
@@ -66,11 +62,10 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
     for (int h = 0; h < REBIN_CHUNKS; h++) {
         // independent loads, issued together: the old range of the new cell
         // and the end of its new range (used if the particle stayed)
-        b[h] = 0; e[h] = 0; end[h] = 0; sb[h] = 0;
+        b[h] = 0; e[h] = 0; end[h] = 0;
         if (key[h] >= 0) {
             b[h] = __ldg(cs + key[h]);
             e[h] = __ldg(cs + key[h] + 1);
-            sb[h] = __ldg(start + key[h]);
             end[h] = __ldg(start + key[h] + 1);
         }
     }
@@ -103,14 +98,7 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
         const unsigned above = heads & ~upto;
         const int next = above ? __ffs(above) - 1 : 32;   // first lane of the next run
         base[h] = 0;
-        if (head && akey[h] >= 0) {
-            base[h] = atomicAdd(cursor + akey[h], next - lane);
-            // the claim that brings the cell's front part to two entries
-            // marks the cell for the front order (parts of 0 or 1 entry are
-            // in order already)
-            const int before = base[h] - sb[h];
-            if (before < 2 && before + next - lane >= 2) atomicOr(crowd + (akey[h] >> 5), 1u << (akey[h] & 31));
-        }
+        if (head && akey[h] >= 0) base[h] = atomicAdd(cursor + akey[h], next - lane);
     }
 #pragma unroll
     for (int h = 0; h < REBIN_CHUNKS; h++) {
@@ -123,20 +111,17 @@ __global__ void __launch_bounds__(256) k_rebin_scatter(const int32_t* __restrict
     }
 }
 
-// Front part [start[c], cursor[c]) of cell c into list order, in place, if
-// the scatter marked the cell (a front part of two entries or more; lanes of
-// unmarked cells take part in the warp's collectives only).  The part holds
-// one step's arrivals: up to 8 entries are sorted in registers, up to
-// REBIN_LONG_SEG by insertion sort in place, longer parts are queued for
-// k_rebin_front_long.
-__global__ void __launch_bounds__(256) k_rebin_front(int ncell, const uint32_t* __restrict__ crowd,
-                                                     const int32_t* __restrict__ start,
+// Front part [start[c], cursor[c]) of each cell into list order, in place.
+// The part holds one step's arrivals: up to 8 entries are sorted in
+// registers, up to REBIN_LONG_SEG by insertion sort in place, longer parts
+// are queued for k_rebin_front_long.
+__global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* __restrict__ start,
                                                      const int32_t* __restrict__ cursor, int n_old, int total,
                                                      int32_t* __restrict__ perm, int32_t* __restrict__ long_list,
                                                      int* __restrict__ n_long, unsigned int* status) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     int b = 0, f = 0;
-    if (c < ncell && ((__ldg(crowd + (c >> 5)) >> (c & 31)) & 1u)) {
+    if (c < ncell) {
         b = __ldg(start + c);
         f = __ldg(cursor + c) - b;
         if (f >= 2 && (b < 0 || b + f > total)) {  // counts inconsistent with the cells
@@ -352,17 +337,16 @@ void rebin(State& s, int si, int64_t born, bool counted) {
     }
     // cell_next = exclusive scan of the counts; count becomes the claim cursor
     exclusive_scan_i32(s, sp.count, sp.cell_next, g.nc, sp.count);
-    cudaMemsetAsync(s.crowd_bits, 0, (size_t)((g.nc + 31) / 32) * sizeof(uint32_t), s.stream);
     if (total > 0) {
         const int per_block = 256 * REBIN_CHUNKS;
         k_rebin_scatter<<<(total + per_block - 1) / per_block, 256, 0, s.stream>>>(
-            sp.newcell, total, sp.cell_start, sp.cell_next, sp.count, sp.perm, s.crowd_bits, s.d_status);
+            sp.newcell, total, sp.cell_start, sp.cell_next, sp.count, sp.perm, s.d_status);
         s.launches++;
     }
     int* n_long = (int*)s.long_list;  // entry 0: count; cells from entry 1
     cudaMemsetAsync(n_long, 0, sizeof(int), s.stream);
-    k_rebin_front<<<(g.nc + 255) / 256, 256, 0, s.stream>>>(g.nc, s.crowd_bits, sp.cell_next, sp.count, n, total,
-                                                             sp.perm, s.long_list + 1, n_long, s.d_status);
+    k_rebin_front<<<(g.nc + 255) / 256, 256, 0, s.stream>>>(g.nc, sp.cell_next, sp.count, n, total, sp.perm,
+                                                             s.long_list + 1, n_long, s.d_status);
     k_rebin_front_long<<<2 * 148, 256, 0, s.stream>>>(sp.cell_next, sp.count, n, sp.perm, sp.newcell,
                                                       s.long_list + 1, n_long);
     s.launches += 2;

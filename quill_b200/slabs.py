@@ -270,12 +270,15 @@ class TorchComm:
             metas_out[p] = m.to(self.device)
             metas_in[p] = torch.zeros(MAXA, dtype=torch.int64, device=self.device)
         self._exchange({p: metas_out[p] for p in nbrs}, metas_in)
+        # the received lengths size the receive buffers: one copy to the host
+        # for both neighbours
+        host = torch.stack([metas_in[p] for p in nbrs]).cpu() if nbrs else None
         data_out, data_in, lens_in = {}, {}, {}
-        for p in nbrs:
+        for q, p in enumerate(nbrs):
             arrs = out.get((me, p), [])
             flat = [self._t(a) for a in arrs]
             data_out[p] = torch.cat(flat) if flat else torch.zeros(0, dtype=torch.float64, device=self.device)
-            mi = metas_in[p].cpu()
+            mi = host[q]
             lens = [int(v) for v in mi[1:1 + int(mi[0])]]
             lens_in[p] = lens
             data_in[p] = torch.empty(sum(lens), dtype=torch.float64, device=self.device)

@@ -245,10 +245,14 @@ def build(case: Case):
 # streams differ from numpy's.
 # ---------------------------------------------------------------------------
 
-def make_fields_torch(case: Case, device="cuda"):
+def make_fields_torch(case: Case, device="cuda", i0: int = 0, nxr: int | None = None):
+    """make_fields on the device; with i0 / nxr only the x-layers
+    [i0, i0 + nxr) of the box (an x-slab region)."""
     import torch
     nx, ny, nz = case.nx, case.ny, case.nz
-    z0 = lambda: torch.zeros((nx, ny, nz), dtype=torch.float64, device=device)
+    if nxr is None:
+        nxr = nx
+    z0 = lambda: torch.zeros((nxr, ny, nz), dtype=torch.float64, device=device)
     f = {k: z0() for k in ("ex", "ey", "ez", "bx", "by", "bz")}
     L = case.laser
     if L is None:
@@ -258,7 +262,7 @@ def make_fields_torch(case: Case, device="cuda"):
     xs = min(xs, 0.45 * nx * dx)
     w = L.waist_lambda * TWO_PI
     xc = xs
-    i = torch.arange(nx, dtype=torch.float64, device=device)
+    i = torch.arange(i0, i0 + nxr, dtype=torch.float64, device=device)
     j = torch.arange(ny, dtype=torch.float64, device=device)
     k = torch.arange(nz, dtype=torch.float64, device=device)
 
@@ -282,14 +286,18 @@ def make_fields_torch(case: Case, device="cuda"):
         f["ez"] = pol[1] * wave(i, -0.5 * math.pi)[:, None, None] * t_ez[None]
         f["by"] = -pol[1] * wave(i + 0.5, -0.5 * math.pi)[:, None, None] * t_ez[None]
     if L.counter:
+        if nxr != nx:
+            raise ValueError("counter-propagating pulse: whole box only")
         for key, sgn in (("ey", 1), ("ez", 1), ("by", -1), ("bz", -1)):
             f[key] = f[key] + sgn * torch.flip(f[key], dims=(0,))
     return {kk: v.contiguous() for kk, v in f.items()}
 
 
-def particle_chunks_torch(case: Case, sp: SpeciesSpec, planes_per_chunk=32, device="cuda", seed=0):
+def particle_chunks_torch(case: Case, sp: SpeciesSpec, planes_per_chunk=32, device="cuda", seed=0, i_range=None):
     """Yield particle dicts (torch float64 tensors on the device) for groups
-    of x-planes, in traversal order, ppc per occupied cell."""
+    of x-planes, in traversal order, ppc per occupied cell; with i_range =
+    (a, b) only the x-layers [a, b), positions in the frame of layer a (an
+    x-slab region starting there)."""
     import torch
     nx, ny, nz = case.nx, case.ny, case.nz
     gen = torch.Generator(device=device)
@@ -297,8 +305,10 @@ def particle_chunks_torch(case: Case, sp: SpeciesSpec, planes_per_chunk=32, devi
     jj, kk = torch.meshgrid(torch.arange(1, ny - 2, device=device), torch.arange(1, nz - 2, device=device),
                             indexing="ij")
     jj, kk = jj.reshape(-1), kk.reshape(-1)
-    for i0 in range(1, nx - 2, planes_per_chunk):
-        i1 = min(i0 + planes_per_chunk, nx - 2)
+    lo, hi = (1, nx - 2) if i_range is None else (max(1, i_range[0]), min(nx - 2, i_range[1]))
+    shift = 0 if i_range is None else i_range[0]
+    for i0 in range(lo, hi, planes_per_chunk):
+        i1 = min(i0 + planes_per_chunk, hi)
         ii = torch.arange(i0, i1, device=device).repeat_interleave(jj.numel())
         cj = jj.repeat(i1 - i0)
         ck = kk.repeat(i1 - i0)
@@ -311,7 +321,7 @@ def particle_chunks_torch(case: Case, sp: SpeciesSpec, planes_per_chunk=32, devi
         if m == 0:
             continue
         rep = lambda t: t.repeat_interleave(sp.ppc).to(torch.float64)
-        x = rep(ii) + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
+        x = rep(ii) - shift + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
         y = rep(cj) + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
         z = rep(ck) + torch.rand(m, generator=gen, device=device, dtype=torch.float64)
         if sp.theta > 0:
