@@ -398,6 +398,109 @@ def pinned_host_state(case, device_index):
     return {"f": hf, "p": hp, "out": out}
 
 
+def slab_main(args, case, rank, world, local):
+    """One box of world x local_regions x-slab regions, each the size of the
+    benchmark box along x (weak scaling), stepped with the neighbour exchange
+    of synchronize_regions (main.cpp:1493-1506) after every step."""
+    import datetime
+    import torch
+    from quill_b200 import workloads as W
+    from quill_b200.api import Region
+    from quill_b200.slabs import NM, LocalComm, SlabBox, SlabLayout, TorchComm
+    dist = None
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    dev = f"cuda:{local}"
+    nreg = world * args.local_regions
+    gcase = W.scaled(case, case.nx * nreg, case.ny, case.nz)
+    gcase.seed = 1234
+    layout = SlabLayout.even(gcase.nx, nreg)
+    if world > 1:
+        if args.local_regions != 1:
+            raise SystemExit("--local-regions needs a single process")
+        comm = TorchComm(device=dev)
+    else:
+        comm = LocalComm(device=dev)
+    prec = "fp64"
+    species = tuple(sp.cmr for sp in gcase.species)
+
+    def make_region(r, nxl):
+        reg = Region(nxl, gcase.ny, gcase.nz, gcase.dx, gcase.dx, gcase.dx, gcase.dt, species_cmr=species,
+                     solver=gcase.solver, pusher=gcase.pusher, precision=prec, device=local)
+        reg.set_stream(stream.cuda_stream)
+        return reg
+
+    box = SlabBox(layout, make_region, comm)
+    keys = ("x", "y", "z", "ux", "uy", "uz", "g", "q")
+    for r in box.local:
+        reg, x0, nxl = box.regions[r], layout.x0[r], layout.nx[r]
+        f = W.make_fields_torch(gcase, device=dev, i0=x0, nxr=nxl)
+        torch.cuda.synchronize()
+        reg._check(reg.lib.qp_load_fields(reg.h, *[_tp(f[k]) for k in ("ex", "ey", "ez", "bx", "by", "bz")]))
+        del f
+        for si, sp in enumerate(gcase.species):
+            for ch in W.particle_chunks_torch(gcase, sp, 48, device=dev, seed=gcase.seed + 17 * si + 1000 * r,
+                                              i_range=(x0, x0 + nxl)):
+                _load_torch(reg, si, ch)
+                del ch
+    box.init_boundaries()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    def count(row):  # N_qp_e + N_qp_p + N_qp_g + ions
+        return float(row[3] + row[4] + row[5] + sum(row[10 + 2 * m] for m in range((len(row) - 10) // 2)))
+
+    rows = box.step(args.warmup) if args.warmup else []
+    last = count(rows[-1]) if len(rows) else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    ev[0].record(stream)
+    pushed = 0.0
+    for k in range(args.steps):
+        acc = None
+        for r in box.local:
+            d = box.regions[r].step(1)[0].as_array()
+            acc = d if acc is None else acc + d
+        ev[2 * k + 1].record(stream)
+        row = comm.allsum(acc)
+        box.synchronize(NM, NM)
+        ev[2 * k + 2].record(stream)
+        pushed += last if last is not None else count(row)
+        last = count(row)
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[-1])
+    exch = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps))
+    if dist:
+        t = torch.tensor([ms, exch], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, exch = float(t[0]), float(t[1])
+        dist.barrier()
+        for reg in box.regions.values():
+            reg.close()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": pushed / (ms * 1e-3), "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, generated on the GPU)",
+        "cell_updates_per_s": gcase.nx * gcase.ny * gcase.nz * args.steps / (ms * 1e-3),
+        "config": workload_config(case),
+        "parallelism": f"one box of {nreg} x-slab regions of {case.nx} cells along x ({gcase.nx}x{gcase.ny}x"
+                       f"{gcase.nz} cells), {world} GPU(s); neighbours exchange field halos and particles after "
+                       f"every step ({'NCCL point to point' if world > 1 else 'device copies in one process'})",
+        "exchange_ms_per_step": exch / args.steps,
+        "regions_per_gpu": args.local_regions,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,6 +515,12 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-regions", type=int, default=0,
                     help="x-slab regions of the reference runs (default: the host's core count)")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "slabs"],
+                    help="replicas: one independent box per GPU; slabs: one box cut into x-slab regions, one "
+                         "region per GPU (the reference's decomposition), neighbours exchanging halos and "
+                         "particles every step over NCCL")
+    ap.add_argument("--local-regions", type=int, default=1,
+                    help="slabs mode: regions per process (several on one GPU measure the exchange without NVLink)")
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="also run this many untimed steps per precision and report the relative drift of the "
                          "total energy (field + particles) over them")
@@ -459,6 +568,10 @@ def main():
                     "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line), flush=True)
+        return
+
+    if args.mode == "slabs":
+        slab_main(args, case, rank, world, local)
         return
 
     import torch

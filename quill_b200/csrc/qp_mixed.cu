@@ -223,7 +223,11 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                 const float g_prev = gm, chi_prev = chi;
                 chi = qed_chi(E, B, ui, gm, e_s);
                 const float am = 0.5f * (chi + chi_prev);
-                const bool pair = !(r2 >= (double)(qed_tilde_w(g_prev, r, am, e_s) * g_prev * a.dt));
+                // tilde_w's range check (r g >= 1 and (1 - r) g >= 1, mc.cpp:76-97)
+                // on the FP64 draw: in FP32, 1 - r rounds to 1 for draws below
+                // 2^-24 and the check would let them through
+                const bool room = rd * (double)g_prev >= 1.0 && (1.0 - rd) * (double)g_prev >= 1.0;
+                const bool pair = room && !(r2 >= (double)(qed_tilde_w(g_prev, r, am, e_s) * g_prev * a.dt));
                 if (!pair) {
                     const float tt = a.dt / gm;
                     o[0] += ux * tt * a.idx; o[1] += uy * tt * a.idy; o[2] += uz * tt * a.idz;
@@ -245,7 +249,10 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                 const float ui[3] = {0.5f * (ux + up[0]), 0.5f * (uy + up[1]), 0.5f * (uz + up[2])};
                 chi = qed_chi(E, B, ui, 0.5f * (gm + g_prev), e_s);
                 const float am = 0.5f * (chi + chi_prev);
-                const bool emit = !(r2 >= (double)(qed_w(g_prev, r, am, e_s) * g_prev * a.dt));
+                // w's range check ((1 - r) g >= 1, r > 0, mc.cpp:40-74) on the
+                // FP64 draw, as for tilde_w: a resting lepton cannot emit
+                const bool room = rd > 0.0 && (1.0 - rd) * (double)g_prev >= 1.0;
+                const bool emit = room && !(r2 >= (double)(qed_w(g_prev, r, am, e_s) * g_prev * a.dt));
                 if (!emit) {
                     const float tt = a.dt / gm;
                     const float d[3] = {ux * tt * a.idx, uy * tt * a.idy, uz * tt * a.idz};
