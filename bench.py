@@ -72,8 +72,8 @@ BYTES = {"fp64": (120, 168), "mixed": (68, 84)}
 # (15,250,622 particles, about 2.5 GB on the device).  At fixed ppc the
 # traffic grows in proportion to the particle count, so the per-particle
 # figure is scaled by Np for the grid being measured.
-TRAFFIC_PER_PARTICLE = {"fp64": (2.472e9 + 1.296e9) / 15250622,
-                        "mixed": (0.935e9 + 0.670e9) / 15250622}
+TRAFFIC_PER_PARTICLE = {"fp64": (1.361e9 + 1.120e9) / 15250622,
+                        "mixed": (0.783e9 + 0.645e9) / 15250622}
 TRAFFIC_SOURCE = "ncu capture of one launch at 160^3 (same physics), per particle x Np"
 
 

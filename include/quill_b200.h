@@ -188,6 +188,14 @@ int qp_set_timing(qp_handle* h, int enable);
  * diagnostics; *steps = timed steps (nullable). */
 int qp_get_timing(qp_handle* h, double* ms4, int64_t* steps);
 
+/* QED steps since qp_set_timing(h, 1), in milliseconds, each part of [0] of
+ * qp_get_timing: [0] preparation (room for the particles a push can create,
+ * the vacuum-pair kernel, the merge of its pairs into the cell lists, and
+ * the host synchronisation that reads their count), [1] the push kernels,
+ * [2] the read-back of the born-particle counts after them; *steps = timed
+ * QED steps (nullable). */
+int qp_get_qed_timing(qp_handle* h, double* ms3, int64_t* steps);
+
 /* Reference-order current deposition (parity switch; FP64, QED off): each
  * step sums every J element's terms from zero in the order the reference's
  * padvance adds them (cells lexicographic, each cell's list of all species

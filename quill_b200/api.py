@@ -113,6 +113,7 @@ def load_library(path: str | None = None):
         "qp_eval_qed_rates": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_eval_qed_rates_noalloc": (C.c_int, [C.c_int, D, I64, DP, DP]),
         "qp_get_timing": (C.c_int, [VP, DP, I64P]),
+        "qp_get_qed_timing": (C.c_int, [VP, DP, I64P]),
         "qp_set_erased_tracking": (C.c_int, [VP, C.c_int]),
         "qp_set_ordered_current": (C.c_int, [VP, C.c_int]),
         "qp_pmerging": (C.c_int, [VP, C.c_int, DP]),
@@ -438,6 +439,14 @@ class Region:
         ms = np.zeros(4)
         n = C.c_int64()
         self._check(self.lib.qp_get_timing(self.h, _dp(ms), C.byref(n)))
+        return ms, n.value
+
+    def get_qed_timing(self):
+        """(ms [preparation incl. vacuum pairs and one host sync, push
+        kernels, born-count read-back], QED steps timed)."""
+        ms = np.zeros(3)
+        n = C.c_int64()
+        self._check(self.lib.qp_get_qed_timing(self.h, _dp(ms), C.byref(n)))
         return ms, n.value
 
     def adjoint_energy(self, nsteps: int, every: int = 32, external_bz: float = 0.0):

@@ -26,7 +26,10 @@ Prints, every `--every` steps, the macro-particles per species and the
 elapsed time (CUDA events on the stream, host work between steps included),
 and at the end one JSON line: particle-steps/s over the whole run (the
 particles pushed in each step, summed, over that time, merging included),
-the final counts, and the peak particle count.
+the final counts, the peak particle count, and the mean time per step of
+each phase (`ms_per_step`; push_deposit contains qed_prepare, the push
+kernels and the born-count read-back, which are also given apart; merging
+is averaged over all steps).
 """
 from __future__ import annotations
 
@@ -54,6 +57,7 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crp
                  solver=case.solver, pusher=case.pusher, qed=True, precision=precision, seed=seed,
                  device=device)
     reg.set_stream(stream.cuda_stream)
+    reg.set_timing(True)
     f = W.make_fields_torch(case, device=dev)
     torch.cuda.synchronize()
     import ctypes as C
@@ -72,6 +76,7 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crp
     if not quiet:
         print(f"{case.nx}x{case.ny}x{case.nz} cells, {precision}, start: {counts} (e, p+, e+, photons)", flush=True)
     pushed, peak, ms_total, merges = 0, n0, 0.0, 0
+    merge_events = []
     history = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     crnp = crpc * case.nx * case.ny * case.nz
@@ -86,7 +91,11 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crp
         # the nl merging condition per species (main.cpp:1691-1748)
         ppd = [(n - crnp) / n if n > crnp else 0.0 for n in counts]
         if any(v > 0 for v in ppd):
+            m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
             reg.pmerging("nl", ppd)
+            m1.record(stream)
+            merge_events.append((m0, m1))
             merges += 1
             counts = [reg.count(i) for i in range(len(species))]
         if step % every == 0 or step == steps:
@@ -97,11 +106,19 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crp
             if not quiet:
                 print(f"step {step}: {counts}, {sum(counts):.3e} particles, {ms_total / 1e3:.2f} s, "
                       f"{merges} merging passes", flush=True)
+    phase, nph = reg.get_timing()
+    merge_ms = sum(a.elapsed_time(b) for a, b in merge_events)
+    qed, nq = reg.get_qed_timing()
     reg.close()
+    per = lambda v, n: float(v) / max(n, 1)
     return {"metric": "QED particle-steps/s", "value": pushed / (ms_total * 1e-3), "unit": "particle-steps/s",
             "precision": precision, "grid": list(grid), "steps": steps, "seconds_device": ms_total / 1e3,
             "seconds_wall": time.perf_counter() - t_wall, "particles_start": n0, "particles_end": sum(counts),
             "particles_peak": peak, "counts_end": counts, "merging_passes": merges, "crpc": crpc,
+            "ms_per_step": {"push_deposit": per(phase[0], nph), "rebin": per(phase[1], nph),
+                            "fields": per(phase[2], nph), "diag": per(phase[3], nph),
+                            "qed_prepare": per(qed[0], nq), "push_kernels": per(qed[1], nq),
+                            "born_readback": per(qed[2], nq), "merging": merge_ms / max(steps, 1)},
             "history": history}
 
 

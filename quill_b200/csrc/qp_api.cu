@@ -54,19 +54,18 @@ static int n_arrays(const State& s) { return s.fp64 ? 9 : 10; }
 static int merge_sorted_slots(State& s, int si, int64_t slot0, int64_t n_new, const int32_t* d_cells) {
     Species& sp = s.sp[si];
     const Grid gr = s.grid;
+    // the merged permutation goes to sp.newcell (free between steps; d_cells
+    // is never a part of it), which then becomes sp.perm
     int32_t* nstart = nullptr;
-    int32_t* d_perm = nullptr;
-    QP_CUDA_CHECK(s, cudaMalloc(&nstart, (size_t)(gr.nc + 1) * sizeof(int32_t)));
-    QP_CUDA_CHECK(s, cudaMalloc(&d_perm, sp.cap * sizeof(int32_t)));
+    QP_CUDA_CHECK(s, scratch_alloc(s, (void**)&nstart, (size_t)(gr.nc + 1) * sizeof(int32_t)));
     launch_histogram(s, d_cells, (int)n_new, sp.count);
     exclusive_scan_i32(s, sp.count, nstart, gr.nc);
     if (sp.trn[sp.cur]) QP_CUDA_CHECK(s, cudaMemsetAsync(sp.trn[sp.cur] + slot0, 0, n_new * sizeof(int32_t), s.stream));
-    load_merge(s, si, slot0, nstart, d_perm);
+    load_merge(s, si, slot0, nstart, sp.newcell);
+    scratch_free(s, nstart);
     QP_CUDA_CHECK(s, cudaGetLastError());
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    cudaFree(sp.perm);
-    sp.perm = d_perm;
-    cudaFree(nstart);
+    std::swap(sp.perm, sp.newcell);
     sp.n += n_new;
     sp.slots = slot0 + n_new;
     s.layout_epoch++;
@@ -75,7 +74,29 @@ static int merge_sorted_slots(State& s, int si, int64_t slot0, int64_t n_new, co
 static size_t arr_elem(const State& s, int a) { return s.fp64 ? 8 : 4; }
 
 // Allocate (or grow, keeping contents) the particle arrays of a species.
-static int ensure_capacity(State& s, int si, int64_t need) {
+cudaError_t scratch_alloc(State& s, void** p, size_t bytes) {
+    if (!s.pool) {
+        cudaMemPoolProps pr = {};
+        pr.allocType = cudaMemAllocationTypePinned;
+        pr.location.type = cudaMemLocationTypeDevice;
+        pr.location.id = s.prm.device;
+        cudaError_t e = cudaMemPoolCreate(&s.pool, &pr);
+        if (e != cudaSuccess) {
+            s.pool = nullptr;
+            return e;
+        }
+        unsigned long long keep = ~0ull;
+        e = cudaMemPoolSetAttribute(s.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaMallocFromPoolAsync(p, bytes, s.pool, s.stream);
+}
+
+void scratch_free(State& s, void* p) {
+    if (p) cudaFreeAsync(p, s.stream);
+}
+
+int ensure_capacity(State& s, int si, int64_t need) {
     Species& sp = s.sp[si];
     if (need <= sp.cap) return QP_OK;
     if (need >= (int64_t)INT32_MAX) {
@@ -85,6 +106,9 @@ static int ensure_capacity(State& s, int si, int64_t need) {
     int64_t cap = std::max<int64_t>(need, sp.cap + sp.cap / 2);
     cap = std::min<int64_t>(cap, (int64_t)INT32_MAX - 1);
     const int na = n_arrays(s);
+    // Every caller runs between steps: the live particles are slots
+    // [0, sp.slots) of buf[cur] (perm: positions [0, n)); buf[1 - cur] is
+    // the next push's output and holds nothing to keep.
     for (int b = 0; b < 2; b++)
         for (int a = 0; a < na; a++) {
             if (s.fp64 && a == 8 && !s.prm.qed) continue;   // chi only with QED
@@ -92,7 +116,8 @@ static int ensure_capacity(State& s, int si, int64_t need) {
             void* p = nullptr;
             QP_CUDA_CHECK(s, cudaMalloc(&p, cap * arr_elem(s, a)));
             if (sp.buf[b][a]) {
-                QP_CUDA_CHECK(s, cudaMemcpyAsync(p, sp.buf[b][a], sp.cap * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
+                if (b == sp.cur && sp.slots > 0)
+                    QP_CUDA_CHECK(s, cudaMemcpyAsync(p, sp.buf[b][a], sp.slots * arr_elem(s, a), cudaMemcpyDeviceToDevice, s.stream));
                 QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
                 cudaFree(sp.buf[b][a]);
             }
@@ -101,7 +126,8 @@ static int ensure_capacity(State& s, int si, int64_t need) {
     int32_t* np = nullptr;
     QP_CUDA_CHECK(s, cudaMalloc(&np, cap * sizeof(int32_t)));
     if (sp.perm) {
-        QP_CUDA_CHECK(s, cudaMemcpyAsync(np, sp.perm, sp.cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream));
+        if (sp.n > 0)
+            QP_CUDA_CHECK(s, cudaMemcpyAsync(np, sp.perm, sp.n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream));
         QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
         cudaFree(sp.perm);
     }
@@ -114,7 +140,8 @@ static int ensure_capacity(State& s, int si, int64_t need) {
             QP_CUDA_CHECK(s, cudaMalloc(&t, cap * sizeof(int32_t)));
             QP_CUDA_CHECK(s, cudaMemsetAsync(t, 0, cap * sizeof(int32_t), s.stream));
             if (sp.trn[b]) {
-                QP_CUDA_CHECK(s, cudaMemcpyAsync(t, sp.trn[b], sp.cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream));
+                if (b == sp.cur && sp.slots > 0)
+                    QP_CUDA_CHECK(s, cudaMemcpyAsync(t, sp.trn[b], sp.slots * sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream));
                 QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
                 cudaFree(sp.trn[b]);
             }
@@ -171,6 +198,8 @@ static void free_state(State* s) {
         if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     s->stream = nullptr;
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    s->pool = nullptr;
 }
 
 int snapshot_take(State& s, State::Snap& sn) {
@@ -459,6 +488,15 @@ int qp_set_timing(qp_handle* h, int enable) {
     s.timing = enable != 0;
     for (double& v : s.phase_ms) v = 0;
     s.phase_steps = 0;
+    for (double& v : s.qed_ms) v = 0;
+    s.qed_steps = 0;
+    return QP_OK;
+}
+
+int qp_get_qed_timing(qp_handle* h, double* ms3, int64_t* steps) {
+    if (!h || !ms3) return QP_ERR_ARG;
+    for (int i = 0; i < 3; i++) ms3[i] = h->st.qed_ms[i];
+    if (steps) *steps = h->st.qed_steps;
     return QP_OK;
 }
 
@@ -537,6 +575,60 @@ int qp_init_boundaries(qp_handle* h) {
 // load again in sorted order.
 static int load_unsorted(qp_handle* h, int si, int64_t n, const double* const* src);
 
+}  // extern "C"
+
+// Copy n particles into slots [sp.slots, sp.slots + n) of the current
+// buffer (FP64 straight into the slots, mixed precision through an FP64
+// stage), write their cells into `cells` and flag invalid ones (LD_INVALID
+// into *flags, the first bad index into *first_bad).  Stream-ordered; the
+// caller synchronises before reading the flags.
+int qp::stage_particles(State& s, int si, int64_t n, const double* const* src, int32_t* cells,
+                        unsigned int* flags, int* first_bad) {
+    Species& sp = s.sp[si];
+    const int64_t slot0 = sp.slots;
+    const int cur = sp.cur;
+    if (s.fp64) {
+        for (int a = 0; a < 9; a++) {
+            if (!sp.buf[cur][a]) continue;
+            double* dst = (double*)sp.buf[cur][a] + slot0;
+            if (src[a]) QP_CUDA_CHECK(s, cudaMemcpyAsync(dst, src[a], n * 8, cudaMemcpyDefault, s.stream));
+            else QP_CUDA_CHECK(s, cudaMemsetAsync(dst, 0, n * 8, s.stream));
+        }
+        const double* st[8];
+        for (int a = 0; a < 8; a++) st[a] = (const double*)sp.buf[cur][a] + slot0;
+        launch_load_cells(s, st, (int)n, cells, flags, first_bad, 0);
+        return QP_OK;
+    }
+    const int64_t CH = std::min<int64_t>(n, 1 << 24);
+    double* stage = nullptr;
+    QP_CUDA_CHECK(s, scratch_alloc(s, (void**)&stage, CH * 9 * sizeof(double)));
+    PStore32 dst;
+    dst.cell = (int32_t*)sp.buf[cur][0];
+    float** pd[9] = {&dst.ox, &dst.oy, &dst.oz, &dst.ux, &dst.uy, &dst.uz, &dst.g, &dst.q, &dst.chi};
+    for (int a = 0; a < 9; a++) *pd[a] = (float*)sp.buf[cur][1 + a];
+    for (int64_t c0 = 0; c0 < n; c0 += CH) {
+        const int64_t m = std::min<int64_t>(CH, n - c0);
+        const double* st[9];
+        for (int a = 0; a < 9; a++) {
+            double* d = stage + a * CH;
+            cudaError_t e = src[a] ? cudaMemcpyAsync(d, src[a] + c0, m * 8, cudaMemcpyDefault, s.stream)
+                                   : cudaMemsetAsync(d, 0, m * 8, s.stream);
+            if (e != cudaSuccess) {
+                scratch_free(s, stage);
+                s.err = cudaGetErrorString(e);
+                return QP_ERR_CUDA;
+            }
+            st[a] = d;
+        }
+        launch_load_cells(s, st, (int)m, cells, flags, first_bad, (int)c0);
+        launch_to_mixed(s, st, (int)m, dst, (int)(slot0 + c0));
+    }
+    scratch_free(s, stage);
+    return QP_OK;
+}
+
+extern "C" {
+
 int qp_load_particles(qp_handle* h, int si, int64_t n, const double* x, const double* y, const double* z,
                       const double* ux, const double* uy, const double* uz, const double* g, const double* q,
                       const double* chi) {
@@ -552,55 +644,30 @@ int qp_load_particles(qp_handle* h, int si, int64_t n, const double* x, const do
     int r = ensure_capacity(s, si, slot0 + n);
     if (r != QP_OK) return r;
     const double* src[9] = {x, y, z, ux, uy, uz, g, q, chi};
-    const int cur = sp.cur;
     // scratch: cells (n), flags, first bad index, per-cell counts and starts
     int32_t* cells = nullptr;
     unsigned int* flags = nullptr;
     int* first_bad = nullptr;
-    QP_CUDA_CHECK(s, cudaMalloc(&cells, n * sizeof(int32_t)));
-    QP_CUDA_CHECK(s, cudaMalloc(&flags, sizeof(unsigned int) + sizeof(int)));
+    QP_CUDA_CHECK(s, scratch_alloc(s, (void**)&cells, n * sizeof(int32_t)));
+    if (cudaError_t e = scratch_alloc(s, (void**)&flags, sizeof(unsigned int) + sizeof(int)); e != cudaSuccess) {
+        scratch_free(s, cells);
+        s.err = cudaGetErrorString(e);
+        return QP_ERR_CUDA;
+    }
     first_bad = (int*)(flags + 1);
     QP_CUDA_CHECK(s, cudaMemsetAsync(flags, 0, sizeof(unsigned int), s.stream));
     QP_CUDA_CHECK(s, cudaMemsetAsync(first_bad, 0x7f, sizeof(int), s.stream));
-    double* stage = nullptr;
-    if (s.fp64) {
-        // copy straight into the free slots, then validate in place
-        for (int a = 0; a < 9; a++) {
-            if (!sp.buf[cur][a]) continue;
-            double* dst = (double*)sp.buf[cur][a] + slot0;
-            if (src[a]) QP_CUDA_CHECK(s, cudaMemcpyAsync(dst, src[a], n * 8, cudaMemcpyDefault, s.stream));
-            else QP_CUDA_CHECK(s, cudaMemsetAsync(dst, 0, n * 8, s.stream));
-        }
-        const double* st[8];
-        for (int a = 0; a < 8; a++) st[a] = (const double*)sp.buf[cur][a] + slot0;
-        launch_load_cells(s, st, (int)n, cells, flags, first_bad, 0);
-    } else {
-        const int64_t CH = std::min<int64_t>(n, 1 << 24);
-        QP_CUDA_CHECK(s, cudaMalloc(&stage, CH * 9 * sizeof(double)));
-        PStore32 dst;
-        dst.cell = (int32_t*)sp.buf[cur][0];
-        float** pd[9] = {&dst.ox, &dst.oy, &dst.oz, &dst.ux, &dst.uy, &dst.uz, &dst.g, &dst.q, &dst.chi};
-        for (int a = 0; a < 9; a++) *pd[a] = (float*)sp.buf[cur][1 + a];
-        for (int64_t c0 = 0; c0 < n; c0 += CH) {
-            const int64_t m = std::min<int64_t>(CH, n - c0);
-            const double* st[9];
-            for (int a = 0; a < 9; a++) {
-                double* d = stage + a * CH;
-                if (src[a]) QP_CUDA_CHECK(s, cudaMemcpyAsync(d, src[a] + c0, m * 8, cudaMemcpyDefault, s.stream));
-                else QP_CUDA_CHECK(s, cudaMemsetAsync(d, 0, m * 8, s.stream));
-                st[a] = d;
-            }
-            launch_load_cells(s, st, (int)m, cells, flags, first_bad, (int)c0);
-            launch_to_mixed(s, st, (int)m, dst, (int)(slot0 + c0));
-        }
+    if ((r = stage_particles(s, si, n, src, cells, flags, first_bad)) != QP_OK) {
+        scratch_free(s, cells);
+        scratch_free(s, flags);
+        return r;
     }
     launch_check_sorted(s, cells, (int)n, flags);
     unsigned int hf[2] = {0, 0};
     QP_CUDA_CHECK(s, cudaMemcpyAsync(hf, flags, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s.stream));
     QP_CUDA_CHECK(s, cudaGetLastError());
     QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    if (stage) cudaFree(stage);
-    auto release = [&]() { cudaFree(cells); cudaFree(flags); };
+    auto release = [&]() { scratch_free(s, cells); scratch_free(s, flags); };
     if (hf[0] & 1) {
         release();
         char b[160];
@@ -692,10 +759,10 @@ static int qed_prepare(State& s) {
         std::vector<int32_t> sc(k);
         for (int64_t t = 0; t < k; t++) sc[t] = cells[order[t]];
         int32_t* dc = nullptr;
-        QP_CUDA_CHECK(s, cudaMalloc(&dc, k * 4));
-        QP_CUDA_CHECK(s, cudaMemcpy(dc, sc.data(), k * 4, cudaMemcpyHostToDevice));
+        QP_CUDA_CHECK(s, scratch_alloc(s, (void**)&dc, k * 4));
+        QP_CUDA_CHECK(s, cudaMemcpyAsync(dc, sc.data(), k * 4, cudaMemcpyHostToDevice, s.stream));
         r = merge_sorted_slots(s, who[w], slot0, k, dc);
-        cudaFree(dc);
+        scratch_free(s, dc);
         if (r != QP_OK) return r;
     }
     // room for a photon from every lepton, the vacuum pairs included
@@ -764,6 +831,7 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
         if (s.prm.qed) {
             int r = qed_prepare(s);
             if (r != QP_OK) return r;
+            if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[5], s.stream));
             for (auto& sp : s.sp)  // particles born in this push: untracked
                 if (sp.trn[1 - sp.cur] && sp.cap > sp.n)
                     QP_CUDA_CHECK(s, cudaMemsetAsync(sp.trn[1 - sp.cur] + sp.n, 0, (sp.cap - sp.n) * sizeof(int32_t), s.stream));
@@ -772,6 +840,7 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
                 else launch_push_mixed_qed(s, (int)i, external_bz);
             }
             QP_CUDA_CHECK(s, cudaGetLastError());
+            if (s.timing) QP_CUDA_CHECK(s, cudaEventRecord(s.ev[6], s.stream));
             for (size_t i = 0; i < s.sp.size(); i++)
                 QP_CUDA_CHECK(s, cudaMemcpyAsync(&born[i], s.sp[i].d_counter, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
             QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
@@ -834,6 +903,16 @@ int qp_step(qp_handle* h, int nsteps, double external_bz, qp_diag* diag) {
             s.phase_ms[2] += t4e;
             s.phase_ms[3] += t01 + t34;
             s.phase_steps++;
+            if (s.prm.qed) {
+                float q0, q1, q2;
+                cudaEventElapsedTime(&q0, s.ev[1], s.ev[5]);
+                cudaEventElapsedTime(&q1, s.ev[5], s.ev[6]);
+                cudaEventElapsedTime(&q2, s.ev[6], s.ev[2]);
+                s.qed_ms[0] += q0;
+                s.qed_ms[1] += q1;
+                s.qed_ms[2] += q2;
+                s.qed_steps++;
+            }
         }
         fill_diag(s, &s.last_diag);
         s.last_diag.status = st ? (st & ST_NAN ? QP_ERR_NAN : (st & ST_CAPACITY ? QP_ERR_CAPACITY : QP_ERR_CONFIG)) : QP_OK;

@@ -127,6 +127,7 @@ struct State {
     Grid grid;
     int fp64 = 1;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;  // scratch (scratch_alloc), created on first use
     bool own_stream = false;
     void* fields = nullptr;       // allocation of the 12 planes
     size_t field_elem = 8;
@@ -168,9 +169,13 @@ struct State {
     bool catch_erasures = false;     // qp_set_catching: erasures go to the buffer
     bool dump_photons = false;       // qp_set_dump_photons: emitted photons go to the buffer
     CatchBuf* d_cat = nullptr;       // its device copy, passed to the push kernels
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     double phase_ms[4] = {0, 0, 0, 0};
     int64_t phase_steps = 0;
+    // QED steps: preparation (capacity, vacuum pairs and their merge), push
+    // kernels, read-back of the born counts (qp_get_qed_timing)
+    double qed_ms[3] = {0, 0, 0};
+    int64_t qed_steps = 0;
     // cells whose new range is too long for the per-thread ordering of the
     // rebin: entry 0 counts them, entries 1.. list them
     int32_t* long_list = nullptr;
@@ -294,6 +299,18 @@ void launch_to_mixed(State& s, const double* const* a, int n, PStore32 dst, int 
 void launch_f64_to_f32(State& s, const double* a, float* b, size_t n);
 void launch_f32_to_f64(State& s, const float* a, double* b, size_t n);
 void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n, int32_t* copy = nullptr);
+// Particle store (qp_api.cu): grow the arrays of a species to `need` slots,
+// keeping their contents; copy n particles (9 FP64 arrays, host or device,
+// chi may be null) into slots [sp.slots, sp.slots + n) with their cells and
+// validity flags (stream-ordered, nothing synchronised).
+int ensure_capacity(State& s, int si, int64_t need);
+// Per-call scratch, stream-ordered on s.stream, from a memory pool the region
+// owns.  The pool keeps the memory it has mapped (unlimited release
+// threshold), so repeated calls cost no mapping; it goes with the region.
+cudaError_t scratch_alloc(State& s, void** p, size_t bytes);
+void scratch_free(State& s, void* p);
+int stage_particles(State& s, int si, int64_t n, const double* const* src, int32_t* cells, unsigned int* flags,
+                    int* first_bad);
 
 }  // namespace qp
 

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "qp_kernels.cuh"
 #include "qp_qed.cuh"
@@ -45,10 +46,12 @@ __global__ void __launch_bounds__(256) k_merge_sum(const int32_t* __restrict__ p
 }
 
 // Draw, decide, (nl) rescale the survivors, flag, and sum: the deleted
-// signed charge (ti) or the survivors' new signed charge (nl) into acc.
+// signed charge (ti) or the survivors' new signed charge (nl) into acc[1].
+// acc[0] holds the species' signed charge a (k_merge_sum); the mean weight
+// a / n is taken here, so the host does not wait for it.
 template <typename QT>
 __global__ void __launch_bounds__(256) k_merge_mark(const int32_t* __restrict__ perm, int n, QT* __restrict__ q,
-                                                    int mode, double ppd, double sgn, double av_q, uint32_t sp,
+                                                    int mode, double ppd, double sgn, uint32_t sp,
                                                     uint32_t step, uint32_t key0, uint32_t key1,
                                                     int32_t* __restrict__ keep, double* acc) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -56,6 +59,7 @@ __global__ void __launch_bounds__(256) k_merge_mark(const int32_t* __restrict__ 
     if (s < n) {
         const int p = perm[s];
         const double qq = (double)q[p];
+        const double av_q = acc[0] / n;
         const double pdel = mode == QP_MERGE_TI ? ppd : ppd * merge_ppd(sgn * qq, av_q);
         double r, r2;
         uniform2(philox4x32_10((uint32_t)s, sp, RNG_MERGE, step, key0, key1), r, r2);
@@ -69,19 +73,25 @@ __global__ void __launch_bounds__(256) k_merge_mark(const int32_t* __restrict__ 
             v = sgn * (double)(QT)qn;
         }
     }
-    block_sum(acc, v);
+    block_sum(acc + 1, v);
 }
 
 // Survivors: weight times f, moved to their new traversal position.
 // keep was scanned in place: survivor flag = scan[s+1] - scan[s].
+// f restores the species' charge a = acc[0]: a / (a - deleted) for ti
+// (mc.cpp:280-283), a / (new sum) for nl (mc.cpp:431-436).
 template <typename QT>
 __global__ void __launch_bounds__(256) k_merge_compact(const int32_t* __restrict__ perm, int n,
-                                                       const int32_t* __restrict__ scan, QT* __restrict__ q, double f,
-                                                       int32_t* __restrict__ perm_new) {
+                                                       const int32_t* __restrict__ scan, QT* __restrict__ q, int mode,
+                                                       const double* __restrict__ acc, int32_t* __restrict__ perm_new) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int pos = scan[s];
     if (scan[s + 1] == pos) return;  // deleted
+    const double a = acc[0], h = acc[1];
+    double f;
+    if (mode == QP_MERGE_TI) f = (a - h != 0) ? a / (a - h) : a;
+    else f = h != 0 ? a / h : 0.0;
     const int p = perm[s];
     q[p] = (QT)(f * (double)q[p]);
     perm_new[pos] = p;
@@ -93,41 +103,29 @@ __global__ void k_merge_starts(int ncell, const int32_t* __restrict__ cs, const 
     if (c <= ncell) cs_new[c] = scan[cs[c]];
 }
 
+// Stream-ordered; the species' new count goes to s.h_count[si] (pinned),
+// read by the caller after its synchronisation.  acc: two doubles of
+// device scratch.
 template <typename QT>
-int merge_species(State& s, int si, int mode, double ppd, int32_t* scratch) {
+int merge_species(State& s, int si, int mode, double ppd, int32_t* scratch, double* acc) {
     Species& sp = s.sp[si];
     const int n = (int)sp.n;
-    if (n == 0 || ppd <= 0.0) return QP_OK;
     const double sgn = sp.cmr == -1 ? -1.0 : 1.0;
     QT* q = (QT*)sp.buf[sp.cur][s.fp64 ? 7 : 8];
-    double* acc = &s.d_diag->sum_q[0];  // scratch: the accumulators are reset by every step
     const int nb = (n + 255) / 256;
-    double h[2];
     QP_CUDA_CHECK(s, cudaMemsetAsync(acc, 0, 2 * sizeof(double), s.stream));
     k_merge_sum<QT><<<nb, 256, 0, s.stream>>>(sp.perm, n, q, sgn, acc);
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(h, acc, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    const double a = h[0];
-    const double av_q = a / n;
     const uint32_t key0 = (uint32_t)(s.prm.seed & 0xffffffffu), key1 = (uint32_t)(s.prm.seed >> 32);
-    k_merge_mark<QT><<<nb, 256, 0, s.stream>>>(sp.perm, n, q, mode, ppd, sgn, av_q, (uint32_t)si,
-                                               (uint32_t)s.step_index, key0, key1, scratch, acc + 1);
+    k_merge_mark<QT><<<nb, 256, 0, s.stream>>>(sp.perm, n, q, mode, ppd, sgn, (uint32_t)si, (uint32_t)s.step_index,
+                                               key0, key1, scratch, acc);
     exclusive_scan_i32(s, scratch, scratch, n);
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(h + 1, acc + 1, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
-    double f;
-    if (mode == QP_MERGE_TI) f = (a - h[1] != 0) ? a / (a - h[1]) : a;  // mc.cpp:280-283
-    else f = h[1] != 0 ? a / h[1] : 0.0;                                  // mc.cpp:431-436
-    k_merge_compact<QT><<<nb, 256, 0, s.stream>>>(sp.perm, n, scratch, q, f, sp.newcell);
+    k_merge_compact<QT><<<nb, 256, 0, s.stream>>>(sp.perm, n, scratch, q, mode, acc, sp.newcell);
     k_merge_starts<<<(s.grid.nc + 1 + 255) / 256, 256, 0, s.stream>>>(s.grid.nc, sp.cell_start, scratch, sp.cell_next);
     s.launches += 4;
-    int32_t total = 0;
-    QP_CUDA_CHECK(s, cudaMemcpyAsync(&total, scratch + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream));
-    QP_CUDA_CHECK(s, cudaStreamSynchronize(s.stream));
     QP_CUDA_CHECK(s, cudaGetLastError());
+    QP_CUDA_CHECK(s, cudaMemcpyAsync(s.h_count + si, scratch + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s.stream));
     std::swap(sp.perm, sp.newcell);
     std::swap(sp.cell_start, sp.cell_next);
-    sp.n = total;
     return QP_OK;
 }
 
@@ -158,15 +156,25 @@ extern "C" int qp_pmerging(qp_handle* h, int mode, const double* ppd) {
         s.scan_tmp = t;
         s.scan_tmp_bytes = tiles;
     }
-    int32_t* scratch = nullptr;  // keep flags, scanned in place (n + 1)
-    e = cudaMalloc(&scratch, (size_t)(nmax + 1) * sizeof(int32_t));
+    // keep flags, scanned in place (n + 1), then two doubles of sums
+    const size_t keep_b = ((size_t)(nmax + 1) * sizeof(int32_t) + 15) / 16 * 16;
+    char* scratch = nullptr;
+    e = qp::scratch_alloc(s, (void**)&scratch, keep_b + 2 * sizeof(double));
     if (e != cudaSuccess) { s.err = std::string("qp_pmerging: ") + cudaGetErrorString(e); return QP_ERR_CUDA; }
+    std::vector<char> merged(ns, 0);
     int r = QP_OK;
     for (int i = 0; i < ns && r == QP_OK; i++) {
         const double p = mode == QP_MERGE_TI ? ppd[0] : ppd[i];
-        r = s.fp64 ? qp::merge_species<double>(s, i, mode, p, scratch)
-                   : qp::merge_species<float>(s, i, mode, p, scratch);
+        if (s.sp[i].n == 0 || p <= 0.0) continue;
+        merged[i] = 1;
+        r = s.fp64 ? qp::merge_species<double>(s, i, mode, p, (int32_t*)scratch, (double*)(scratch + keep_b))
+                   : qp::merge_species<float>(s, i, mode, p, (int32_t*)scratch, (double*)(scratch + keep_b));
     }
-    cudaFree(scratch);
-    return r;
+    qp::scratch_free(s, scratch);
+    e = cudaStreamSynchronize(s.stream);
+    if (r == QP_OK && e != cudaSuccess) { s.err = std::string("qp_pmerging: ") + cudaGetErrorString(e); r = QP_ERR_CUDA; }
+    if (r != QP_OK) return r;
+    for (int i = 0; i < ns; i++)
+        if (merged[i]) s.sp[i].n = s.h_count[i];
+    return QP_OK;
 }

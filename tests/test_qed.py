@@ -231,3 +231,35 @@ def test_vacuum_pairs_vs_reference(precision):
             r, v = ref[:, step, sp], gpu[:, step, sp]
             sig = np.sqrt(r.var(ddof=1) / r.size + v.var(ddof=1) / v.size)
             assert abs(v.mean() - r.mean()) <= 3 * sig, (step, sp, v.mean(), r.mean(), sig)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_resting_leptons_do_not_emit(precision):
+    """A lepton at rest (g = 1) cannot emit: w's range check (1 - r) g >= 1
+    rejects every draw (mc.cpp:40-74).  In FP32, 1 - r rounds to 1 for draws
+    below 2^-24, so the mixed path takes the check on the FP64 draw; without
+    it a resting electron in a strong field emitted a photon along an
+    undefined direction (NaN).  Cold electrons in a field of 1500 m c omega /
+    e over 2 steps: no NaN, and no photon from the first step."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    from quill_b200.api import Region
+    n = 16
+    rng = np.random.default_rng(3)
+    m = 200000
+    p = {"x": rng.uniform(3, 12, m), "y": rng.uniform(3, 12, m), "z": rng.uniform(3, 12, m),
+         "ux": np.zeros(m), "uy": np.zeros(m), "uz": np.zeros(m), "g": np.ones(m), "q": np.full(m, -1e-3)}
+    z = np.zeros((n, n, n))
+    g = Region(n, n, n, DX, DX, DX, DT, species_cmr=(-1.0, 1.0, 0.0), solver="fdtd", pusher="vay", qed=True,
+               seed=7, precision=precision)
+    g.set_fields(z, np.full((n, n, n), 1500.0), z, z, z, np.full((n, n, n), 1500.0))
+    g.init_boundaries()
+    g.add_particles(0, _sort(p))
+    g.step(1)
+    assert g.count(2) == 0
+    g.step(1)  # the electrons now move; emission may start, but nothing is NaN
+    for s in range(3):
+        q = g.get_particles(s)
+        for k in ("x", "ux", "g"):
+            assert np.isfinite(q[k]).all(), (s, k)

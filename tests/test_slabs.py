@@ -301,3 +301,60 @@ def test_gpu_mixed_slabs_match_one_region():
     assert np.abs(f1 - f3).max() <= 1e-4 * np.abs(f1).max()
     one.close()
     three.close()
+
+
+def _cell_sorted(rng, m, lo, hi, ny, nz):
+    """m particles with x in [lo, hi), sorted by cell, random order inside a
+    cell kept (stable sort)."""
+    p = {"x": rng.uniform(lo, hi, m), "y": rng.uniform(0, ny, m), "z": rng.uniform(0, nz, m),
+         "ux": rng.normal(0, 0.1, m), "uy": rng.normal(0, 0.1, m), "uz": rng.normal(0, 0.1, m), "q": rng.uniform(-2, -1, m)}
+    p["g"] = np.sqrt(1 + p["ux"] ** 2 + p["uy"] ** 2 + p["uz"] ** 2)
+    cell = (p["x"].astype(int) * ny + p["y"].astype(int)) * nz + p["z"].astype(int)
+    o = np.argsort(cell, kind="stable")
+    return {k: v[o] for k, v in p.items()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("device_payload", [False, True])
+@pytest.mark.parametrize("end", ["low", "high"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_end_slab_replacement_follows_the_list_rule(precision, end, device_payload):
+    """Replacing the particles of a slab at either x end (the halo update of
+    the exchange) empties the slab's cells and puts the given particles in
+    them in the given order: the traversal becomes new + kept (low end) or
+    kept + new (high end).  The same holds when an input particle lies
+    outside the slab (it then joins the head of its cell, as a load does)."""
+    if not gpu_available():
+        pytest.skip("needs a CUDA device")
+    import torch
+    from quill_b200.api import Region
+    nx, ny, nz, w = 20, 6, 5, 3
+    rng = np.random.default_rng(11)
+    reg = Region(nx, ny, nz, 0.1, 0.1, 0.1, 0.05, species_cmr=(-1.0,), solver="fdtd", pusher="boris",
+                 precision=precision)
+    reg.add_particles(0, _cell_sorted(rng, 4000, 0, nx, ny, nz))
+    before = reg.get_particles(0)
+    i0 = 0 if end == "low" else nx - w
+    new = _cell_sorted(rng, 700, i0, i0 + w, ny, nz)
+    payload = {k: torch.from_numpy(v).cuda() for k, v in new.items()} if device_payload else new
+    reg.replace_particle_slab(0, i0, w, payload)
+    after = reg.get_particles(0)
+    inside = (before["x"] >= i0) & (before["x"] < i0 + w)
+    kept = {k: before[k][~inside] for k in ("x", "y", "z", "ux", "uy", "uz", "g", "q")}
+    want = {k: (np.concatenate([new[k], kept[k]]) if end == "low" else np.concatenate([kept[k], new[k]]))
+            for k in kept}
+    assert after["x"].size == want["x"].size
+    tol = 0 if precision == "fp64" else 2e-6
+    for k in want:
+        np.testing.assert_allclose(after[k], want[k], rtol=tol, atol=tol * nx, err_msg=k)
+    # a particle outside the slab: loaded into its own cell, at its head
+    stray = _cell_sorted(rng, 5, i0, i0 + w, ny, nz)
+    stray["x"][-1] = 10.5
+    before = reg.get_particles(0)
+    reg.replace_particle_slab(0, i0, w, stray)
+    after = reg.get_particles(0)
+    assert after["x"].size == before["x"].size - 700 + 5
+    assert np.isclose(after["x"], 10.5, rtol=0, atol=tol * nx + 1e-12).sum() == 1
+    reg.step(1)  # the new layout steps (layers 0, n-2, n-1 are erased first)
+    assert 0 < reg.count(0) <= after["x"].size
+    reg.close()
