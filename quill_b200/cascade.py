@@ -38,7 +38,22 @@ import json
 import time
 
 
-def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crpc=1.5, device=0, quiet=False):
+def reservation(nc: int, crpc: float, n_ions: int) -> list[int]:
+    """Particle slots to reserve per species (electrons, protons, positrons,
+    photons) so that the cascade never grows a store mid-run.
+
+    Merging keeps each species near crpc * nc macro-particles between steps.
+    Before each QED push the library needs, in the worst case, one new pair
+    per photon in each lepton store and one new photon per lepton in the
+    photon store; the photons are bounded by the same merging.  Four times
+    the merging bound per lepton store and six times for the photons covers
+    both with room for a step's growth above the bound."""
+    crnp = int(crpc * nc)
+    return [4 * crnp, n_ions + 1024, 4 * crnp, 6 * crnp]
+
+
+def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crpc=1.5, device=0, quiet=False,
+        reserve=True):
     import torch
 
     from . import workloads as W
@@ -53,9 +68,12 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crp
     stream = torch.cuda.Stream(device=device)
     torch.cuda.set_stream(stream)
     species = (-1.0, W.PROTON_CMR, 1.0, 0.0)  # electrons, protons, positrons, photons
+    n_ions = sum(ch["x"].numel() for ch in W.particle_chunks_torch(case, case.species[1], 32, device=dev,
+                                                                     seed=seed + 17))
+    capacity = reservation(case.nx * case.ny * case.nz, crpc, n_ions) if reserve else None
     reg = Region(case.nx, case.ny, case.nz, case.dx, case.dx, case.dx, case.dt, species_cmr=species,
                  solver=case.solver, pusher=case.pusher, qed=True, precision=precision, seed=seed,
-                 device=device)
+                 capacity=capacity, device=device)
     reg.set_stream(stream.cuda_stream)
     reg.set_timing(True)
     f = W.make_fields_torch(case, device=dev)
@@ -115,6 +133,7 @@ def run(grid=(256, 256, 256), steps=600, precision="fp64", seed=0, every=50, crp
             "precision": precision, "grid": list(grid), "steps": steps, "seconds_device": ms_total / 1e3,
             "seconds_wall": time.perf_counter() - t_wall, "particles_start": n0, "particles_end": sum(counts),
             "particles_peak": peak, "counts_end": counts, "merging_passes": merges, "crpc": crpc,
+            "reserved_slots": capacity,
             "ms_per_step": {"push_deposit": per(phase[0], nph), "rebin": per(phase[1], nph),
                             "fields": per(phase[2], nph), "diag": per(phase[3], nph),
                             "qed_prepare": per(qed[0], nq), "push_kernels": per(qed[1], nq),
@@ -131,8 +150,10 @@ def _main():
     ap.add_argument("--every", type=int, default=50)
     ap.add_argument("--crpc", type=float, default=1.5,
                     help="macro-particles per cell above which a species is merged")
+    ap.add_argument("--no-reserve", action="store_true",
+                    help="let the stores grow on demand instead of reserving them up front")
     a = ap.parse_args()
-    r = run(tuple(a.grid), a.steps, a.precision, a.seed, a.every, a.crpc)
+    r = run(tuple(a.grid), a.steps, a.precision, a.seed, a.every, a.crpc, reserve=not a.no_reserve)
     print(json.dumps(r), flush=True)
 
 

@@ -364,8 +364,14 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.diag_hi = p.nx;
     s.grid.div_nynz.init((uint32_t)(p.ny * p.nz));
     s.field_elem = s.fp64 ? 8 : 4;
-    if (const char* mb = getenv("QP_PUSH_MINBLOCKS")) s.push_minblocks = atoi(mb) == 2 ? 2 : (atoi(mb) == 4 ? 4 : 3);
-    if (const char* mb = getenv("QP_PUSH_MINBLOCKS_MIXED")) s.push_minblocks_mixed = atoi(mb) == 4 ? 4 : 3;
+    if (const char* v = getenv("QP_PUSH_SHAPE")) {
+        const int i = atoi(v);
+        if (i >= 0 && i < n_push_shapes64) s.push_shape = i;
+    }
+    if (const char* v = getenv("QP_PUSH_SHAPE_MIXED")) {
+        const int i = atoi(v);
+        if (i >= 0 && i < n_push_shapes32) s.push_shape_mixed = i;
+    }
     if (const char* w = getenv("QP_PUSH_WAVES")) s.push_waves = atoi(w) > 0 ? atoi(w) : 0;
     {
         int sms = 0;

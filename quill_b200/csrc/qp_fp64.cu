@@ -13,8 +13,8 @@ namespace qp {
 // buffer.  The current goes through the warp's segment-slot run reduction
 // (deposit_runs).  newcell (-1 = erased, place(), plist.cpp:7-39) and the
 // particles-per-new-cell histogram (count) feed the rebin.
-template <int PUSHER, int KIND, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
+template <int PUSHER, int KIND, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs a) {
     // the grid (a few waves) strides over the particles in block-sized
@@ -453,7 +453,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
         t0 = target64(s, s.sp_ph, true);
         t1 = t0;
     }
-    const int nb = push_blocks(s, sp.n, 2, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
+    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
     Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push64_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
@@ -505,20 +505,26 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
-    const int nb = push_blocks(s, sp.n, s.push_minblocks, &a.resident);
+    const PushShape sh = push_shapes64[s.push_shape];
+    const int nb = push_blocks(s, sp.n, sh, &a.resident);
     Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LP(P, K)                                                                                          \
-    if (s.push_minblocks == 2)                                                                                \
-        k_push64<P, K, 2><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
-    else if (s.push_minblocks == 4)                                                                           \
-        k_push64<P, K, 4><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
-    else                                                                                                      \
-        k_push64<P, K, 3><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+#define QP_LS(P, K, BS, MB) \
+    k_push64<P, K, BS, MB><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+#define QP_LP(P, K)                              \
+    do { switch (s.push_shape) {                 \
+        case 1: QP_LS(P, K, 256, 3); break;      \
+        case 2: QP_LS(P, K, 192, 3); break;      \
+        case 3: QP_LS(P, K, 128, 5); break;      \
+        case 4: QP_LS(P, K, 128, 4); break;      \
+        case 5: QP_LS(P, K, 64, 8); break;       \
+        default: QP_LS(P, K, 256, 2); break;     \
+    } } while (0)
     if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
     else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
 #undef QP_LP
+#undef QP_LS
     s.launches++;
 }
 

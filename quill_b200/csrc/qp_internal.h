@@ -146,12 +146,11 @@ struct State {
     int64_t step_index = 0;
     bool boundaries_done = false;
     int sp_e = -1, sp_p = -1, sp_ph = -1;  // QED species (cmr -1, +1, 0)
-    // CTAs per SM the FP64 push's register budget targets (2, 3 or 4; more
-    // CTAs, fewer registers per thread); QP_PUSH_MINBLOCKS selects.  2: the
-    // grid-stride kernel needs 128 registers to run without spills
-    int push_minblocks = 2;
-    // the same for the mixed push (3 or 4; QP_PUSH_MINBLOCKS_MIXED)
-    int push_minblocks_mixed = 3;
+    // launch shape of the non-QED pushes: threads per block and the CTAs per
+    // SM its register budget targets (push_shapes64 / push_shapes32 below;
+    // QP_PUSH_SHAPE and QP_PUSH_SHAPE_MIXED select by index)
+    int push_shape = 0;
+    int push_shape_mixed = 2;
     // grid of the non-QED pushes: at most push_waves x (SMs x CTAs per SM)
     // blocks striding over the particles (QP_PUSH_WAVES; 0: one thread per
     // particle)
@@ -234,8 +233,22 @@ inline Planes<T> planes_of(const State& s) {
 // (chunk_range): up to push_waves groups of `resident` blocks (the blocks
 // resident at once: SMs x CTAs per SM); one chunk per block if push_waves is
 // 0 or the chunks are fewer than the resident blocks.
-inline int push_blocks(const State& s, int64_t n, int minb, int* resident) {
-    const int64_t nch = (n + 255) / 256;
+// Launch shapes of the pushes: {threads per block, CTAs per SM}; a block
+// takes chunks of `threads` particles.  FP64: 128 registers per thread run
+// the loop without spills (256 x 2, the default); the smaller budgets trade
+// spills for resident warps and measured 0-25 % slower at 512^3.  Mixed:
+// 80 registers (256 x 3) run without spills; 72 (128 x 7, the default, 28
+// warps per SM, a few spills) measured 5 % faster, 64 (32 warps) slower.
+struct PushShape {
+    int threads, minb;
+};
+constexpr PushShape push_shapes64[] = {{256, 2}, {256, 3}, {192, 3}, {128, 5}, {128, 4}, {64, 8}};
+constexpr PushShape push_shapes32[] = {{256, 3}, {256, 4}, {128, 7}, {128, 6}, {128, 8}, {64, 14}};
+constexpr int n_push_shapes64 = 6, n_push_shapes32 = 6;
+
+inline int push_blocks(const State& s, int64_t n, PushShape sh, int* resident) {
+    const int64_t nch = (n + sh.threads - 1) / sh.threads;
+    const int minb = sh.minb;
     const int64_t r = (int64_t)s.sm_count * minb;
     if (s.push_waves <= 0 || nch <= r) {
         *resident = (int)(nch > 0 ? nch : 1);

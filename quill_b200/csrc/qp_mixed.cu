@@ -37,8 +37,8 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
 // waves striding over block-sized chunks, diagnostics reduced once).  The
 // move runs in the particle's cell frame (offsets in [0, 1)), the current
 // through the warp's segment-slot run reduction (deposit_runs).
-template <int PUSHER, int KIND, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
+template <int PUSHER, int KIND, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs32 a) {
     double dq = 0.0, de = 0.0, er = 0.0;
@@ -448,18 +448,26 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.trn_src = sp.trn[sp.cur];
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
-    const int nb = push_blocks(s, sp.n, s.push_minblocks_mixed, &a.resident);
+    const PushShape sh = push_shapes32[s.push_shape_mixed];
+    const int nb = push_blocks(s, sp.n, sh, &a.resident);
     Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
-#define QP_LP(P, K)                                                                                          \
-    if (s.push_minblocks_mixed == 4)                                                                          \
-        k_push32<P, K, 4><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a);   \
-    else                                                                                                      \
-        k_push32<P, K, 3><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+#define QP_LS(P, K, BS, MB) \
+    k_push32<P, K, BS, MB><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+#define QP_LP(P, K)                              \
+    do { switch (s.push_shape_mixed) {                 \
+        case 0: QP_LS(P, K, 256, 3); break;      \
+        case 2: QP_LS(P, K, 128, 7); break;      \
+        case 3: QP_LS(P, K, 128, 6); break;      \
+        case 4: QP_LS(P, K, 128, 8); break;      \
+        case 5: QP_LS(P, K, 64, 14); break;      \
+        default: QP_LS(P, K, 256, 4); break;     \
+    } } while (0)
     if (sp.kind == KIND_PHOTON) QP_LP(QP_PUSHER_BORIS, KIND_PHOTON);
     else if (vay) QP_LP(QP_PUSHER_VAY, KIND_LEPTON);
     else QP_LP(QP_PUSHER_BORIS, KIND_LEPTON);
 #undef QP_LP
+#undef QP_LS
     s.launches++;
 }
 
@@ -521,7 +529,7 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
         t0 = target32(s, s.sp_ph, true);
         t1 = t0;
     }
-    const int nb = push_blocks(s, sp.n, 2, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
+    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
     Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push32_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)

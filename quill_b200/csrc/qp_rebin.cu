@@ -231,8 +231,14 @@ __global__ void __launch_bounds__(256) k_rebin_front_long(const int32_t* __restr
 }
 
 // ---------------------------------------------------------------- scan ----
-constexpr int SCAN_THREADS = 1024;
-constexpr int SCAN_ITEMS = 4;
+// Reduce-then-scan over tiles of SCAN_TILE items: k_scan_reduce sums each
+// tile, k_scan_sums scans the tile sums in one block, k_scan_down scans each
+// tile from its offset and writes the result (and the copy).  The input is
+// read twice and the output written once: 3 (4 with the copy) passes of
+// 4 bytes per item.  Items are loaded and stored four at a time when the
+// arrays are 16-byte aligned.
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 
 __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
@@ -264,33 +270,55 @@ __device__ __forceinline__ int block_excl_scan(int v, int* sh, int& total) {
     return r;
 }
 
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(const int32_t* in, int32_t* out, int n,
-                                                             int32_t* tile_sums) {
+// The SCAN_ITEMS items of this thread (consecutive), zero past n.
+template <bool VEC>
+__device__ __forceinline__ void scan_load(const int32_t* in, int n, int base, int v[SCAN_ITEMS]) {
+    if (VEC && base + SCAN_ITEMS <= n) {
+#pragma unroll
+        for (int q = 0; q < SCAN_ITEMS / 4; q++) {
+            const int4 w = *reinterpret_cast<const int4*>(in + base + 4 * q);
+            v[4 * q] = w.x; v[4 * q + 1] = w.y; v[4 * q + 2] = w.z; v[4 * q + 3] = w.w;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < SCAN_ITEMS; t++) v[t] = base + t < n ? in[base + t] : 0;
+    }
+}
+
+template <bool VEC>
+__device__ __forceinline__ void scan_store(int32_t* out, int n, int base, const int v[SCAN_ITEMS]) {
+    if (VEC && base + SCAN_ITEMS <= n) {
+#pragma unroll
+        for (int q = 0; q < SCAN_ITEMS / 4; q++)
+            *reinterpret_cast<int4*>(out + base + 4 * q) = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int t = 0; t < SCAN_ITEMS; t++)
+            if (base + t < n) out[base + t] = v[t];
+    }
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_reduce(const int32_t* __restrict__ in, int n,
+                                                              int32_t* __restrict__ tile_sums) {
     __shared__ int sh[33];
     const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
     int v[SCAN_ITEMS];
+    scan_load<VEC>(in, n, base, v);
     int sum = 0;
 #pragma unroll
-    for (int t = 0; t < SCAN_ITEMS; t++) {
-        v[t] = (base + t < n) ? in[base + t] : 0;
-        sum += v[t];
-    }
+    for (int t = 0; t < SCAN_ITEMS; t++) sum += v[t];
     int total;
-    int off = block_excl_scan(sum, sh, total);
-#pragma unroll
-    for (int t = 0; t < SCAN_ITEMS; t++) {
-        if (base + t < n) out[base + t] = off;
-        off += v[t];
-    }
+    block_excl_scan(sum, sh, total);
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
 // Exclusive scan of the tile sums in one block; writes the grand total to
 // tile_sums[nt] (nt tiles).
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int32_t* tile_sums, int nt) {
+__global__ void __launch_bounds__(1024) k_scan_sums(int32_t* tile_sums, int nt) {
     __shared__ int sh[33];
     int carry = 0;
-    for (int b = 0; b < nt; b += SCAN_THREADS) {
+    for (int b = 0; b < nt; b += blockDim.x) {
         const int idx = b + threadIdx.x;
         const int v = idx < nt ? tile_sums[idx] : 0;
         int total;
@@ -301,25 +329,48 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_sums(int32_t* tile_sums, 
     if (threadIdx.x == 0) tile_sums[nt] = carry;
 }
 
-__global__ void __launch_bounds__(256) k_scan_add(int32_t* out, int n, const int32_t* tile_sums, int nt,
-                                                  int32_t* copy) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x < n) {
-        const int v = out[x] + tile_sums[x / SCAN_TILE];
-        out[x] = v;
-        if (copy) copy[x] = v;
+// in may alias out or copy: every thread reads its items before writing them.
+template <bool VEC>
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_down(const int32_t* in, int32_t* out, int n,
+                                                            const int32_t* __restrict__ tile_sums, int nt,
+                                                            int32_t* copy) {
+    __shared__ int sh[33];
+    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    scan_load<VEC>(in, n, base, v);
+    int sum = 0;
+#pragma unroll
+    for (int t = 0; t < SCAN_ITEMS; t++) sum += v[t];
+    int total;
+    int off = block_excl_scan(sum, sh, total) + tile_sums[blockIdx.x];
+#pragma unroll
+    for (int t = 0; t < SCAN_ITEMS; t++) {
+        const int x = v[t];
+        v[t] = off;
+        off += x;
     }
-    if (x == 0) out[n] = tile_sums[nt];
+    scan_store<VEC>(out, n, base, v);
+    if (copy) scan_store<VEC>(copy, n, base, v);
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_sums[nt];
 }
 
 // out[0..n] = exclusive scan of in[0..n), out[n] = total; copy[0..n) (if
-// given, may alias in) receives out[0..n) as well.
+// given, may alias in) receives out[0..n) as well.  in may alias out.
 void exclusive_scan_i32(State& s, const int32_t* in, int32_t* out, int n, int32_t* copy) {
     const int nt = (n + SCAN_TILE - 1) / SCAN_TILE;
     int32_t* sums = (int32_t*)s.scan_tmp;
-    k_scan_tiles<<<nt, SCAN_THREADS, 0, s.stream>>>(in, out, n, sums);
-    k_scan_sums<<<1, SCAN_THREADS, 0, s.stream>>>(sums, nt);
-    k_scan_add<<<(n + 255) / 256, 256, 0, s.stream>>>(out, n, sums, nt, copy);
+    const bool vec = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0) && ((uintptr_t)copy % 16 == 0);
+    if (nt > 0) {
+        if (vec) k_scan_reduce<true><<<nt, SCAN_THREADS, 0, s.stream>>>(in, n, sums);
+        else k_scan_reduce<false><<<nt, SCAN_THREADS, 0, s.stream>>>(in, n, sums);
+    }
+    k_scan_sums<<<1, 1024, 0, s.stream>>>(sums, nt);
+    if (nt > 0) {
+        if (vec) k_scan_down<true><<<nt, SCAN_THREADS, 0, s.stream>>>(in, out, n, sums, nt, copy);
+        else k_scan_down<false><<<nt, SCAN_THREADS, 0, s.stream>>>(in, out, n, sums, nt, copy);
+    } else {
+        cudaMemcpyAsync(out, sums, sizeof(int32_t), cudaMemcpyDeviceToDevice, s.stream);  // out[0] = 0
+    }
     s.launches += 3;
 }
 
