@@ -28,9 +28,11 @@ namespace qp {
 //     order, born ascending then arrivals DESCENDING by old position; it is
 //     short (the arrivals of one step), long parts go to a block each.
 
-__device__ __forceinline__ long long front_key(int x, int n_old) {
-    if (x >= n_old) return (long long)x;                       // born
-    return (1ll << 32) | (long long)(0x7fffffff - x);          // arrival
+// Sort key of a front entry: born (x >= n_old) ascending first, then
+// arrivals (x < n_old) by DESCENDING old position; both fit 32 bits.
+__device__ __forceinline__ unsigned front_key(int x, int n_old) {
+    if (x >= n_old) return (unsigned)(x - n_old);               // born: [0, 2^31)
+    return 0x80000000u + (unsigned)(n_old - 1 - x);             // arrival: [2^31, 2^32)
 }
 
 // Particles per new cell (entries < 0 skipped), one atomic per run.
@@ -150,16 +152,16 @@ __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* _
     if (fmax <= 4) {
         if (f < 2) return;
         int x[4];
-        long long k[4];
+        unsigned k[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             x[u] = u < f ? perm[b + u] : 0;
-            k[u] = u < f ? front_key(x[u], n_old) : 0x7fffffffffffffffll;
+            k[u] = u < f ? front_key(x[u], n_old) : 0xffffffffu;
         }
         // optimal 4-input network: (0,1) (2,3) (0,2) (1,3) (1,2)
         auto cx = [&](int i, int j) {
             if (k[i] > k[j]) {
-                const long long tk = k[i]; k[i] = k[j]; k[j] = tk;
+                const unsigned tk = k[i]; k[i] = k[j]; k[j] = tk;
                 const int tx = x[i]; x[i] = x[j]; x[j] = tx;
             }
         };
@@ -173,18 +175,18 @@ __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* _
     if (f <= 8) {
         // in registers: all loads issued together, odd-even transposition sort
         int x[8];
-        long long k[8];
+        unsigned k[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             x[u] = u < f ? perm[b + u] : 0;
-            k[u] = u < f ? front_key(x[u], n_old) : 0x7fffffffffffffffll;
+            k[u] = u < f ? front_key(x[u], n_old) : 0xffffffffu;
         }
 #pragma unroll
         for (int r = 0; r < 8; r++) {
 #pragma unroll
             for (int u = r & 1; u + 1 < 8; u += 2) {
                 if (k[u] > k[u + 1]) {
-                    const long long tk = k[u]; k[u] = k[u + 1]; k[u + 1] = tk;
+                    const unsigned tk = k[u]; k[u] = k[u + 1]; k[u + 1] = tk;
                     const int tx = x[u]; x[u] = x[u + 1]; x[u + 1] = tx;
                 }
             }
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(256) k_rebin_front(int ncell, const int32_t* _
     }
     for (int u = b + 1; u < b + f; u++) {
         const int x = perm[u];
-        const long long kx = front_key(x, n_old);
+        const unsigned kx = front_key(x, n_old);
         int v = u - 1;
         while (v >= b && front_key(perm[v], n_old) > kx) {
             perm[v + 1] = perm[v];
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(256) k_rebin_front_long(const int32_t* __restr
         __syncthreads();
         for (int u = b + (int)threadIdx.x; u < e; u += blockDim.x) {
             const int x = scratch[u];
-            const long long kx = front_key(x, n_old);
+            const unsigned kx = front_key(x, n_old);
             int r = 0;
             for (int v = b; v < e; v++) r += front_key(scratch[v], n_old) < kx;
             perm[b + r] = x;
