@@ -364,6 +364,7 @@ int qp_create(const qp_params* prm, qp_handle** out) {
     s.diag_hi = p.nx;
     s.grid.div_nynz.init((uint32_t)(p.ny * p.nz));
     s.field_elem = s.fp64 ? 8 : 4;
+    if (const char* v = getenv("QP_PREFETCH")) s.prefetch = atoi(v) != 0;
     if (const char* v = getenv("QP_PUSH_SHAPE")) {
         const int i = atoi(v);
         if (i >= 0 && i < n_push_shapes64) s.push_shape = i;

@@ -13,7 +13,7 @@ namespace qp {
 // buffer.  The current goes through the warp's segment-slot run reduction
 // (deposit_runs).  newcell (-1 = erased, place(), plist.cpp:7-39) and the
 // particles-per-new-cell histogram (count) feed the rebin.
-template <int PUSHER, int KIND, int BS, int MINB>
+template <int PUSHER, int KIND, int BS, int MINB, bool PF>
 __global__ void __launch_bounds__(BS, MINB) k_push64(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs a) {
@@ -24,16 +24,33 @@ __global__ void __launch_bounds__(BS, MINB) k_push64(Fields<double> f, Grid g, P
     double dq = 0.0, de = 0.0, er = 0.0;
     unsigned long long dc = 0;
     const ChunkRange cr = chunk_range(a.n, a.resident);
+    // software pipeline over the thread's chunks: the slot and position of
+    // the next chunk's particle are loaded during this chunk, so that the
+    // loads of a particle's momenta and of its fields issue together
+    int p_nx = 0;
+    double x_nx = 0.0, y_nx = 0.0, z_nx = 0.0;
+    if (PF) {
+        const int s0 = cr.first * blockDim.x + threadIdx.x;
+        if (cr.first < cr.end && s0 < a.n) {
+            p_nx = perm[s0];
+            x_nx = src.x[p_nx]; y_nx = src.y[p_nx]; z_nx = src.z[p_nx];
+        }
+    }
     for (int ch = cr.first; ch < cr.end; ch += cr.step) {
     const int s = ch * blockDim.x + threadIdx.x;
-    int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+    const int s_nx = (ch + cr.step) * blockDim.x + threadIdx.x;
+    const bool has_nx = PF && ch + cr.step < cr.end && s_nx < a.n;
+    int nc = -1, p = p_nx, i0 = 0, j0 = 0, k0 = 0;
     bool nc_owned = true;
     bool live = false, active = false;
-    double pos[3] = {0.0, 0.0, 0.0}, d[3] = {0.0, 0.0, 0.0};
+    double pos[3] = {x_nx, y_nx, z_nx}, d[3] = {0.0, 0.0, 0.0};
     double ux = 0.0, uy = 0.0, uz = 0.0, gm = 1.0, q = 0.0;
-    if (s < a.n) {
+    if (!PF && s < a.n) {
         p = perm[s];
         pos[0] = src.x[p]; pos[1] = src.y[p]; pos[2] = src.z[p];
+    }
+    if (has_nx) p_nx = perm[s_nx];
+    if (s < a.n) {
         ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
         q = src.q[p];
         i0 = (int)pos[0]; j0 = (int)pos[1]; k0 = (int)pos[2];
@@ -57,6 +74,9 @@ __global__ void __launch_bounds__(BS, MINB) k_push64(Fields<double> f, Grid g, P
             }
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
         }
+    }
+    if (has_nx) {
+        x_nx = src.x[p_nx]; y_nx = src.y[p_nx]; z_nx = src.z[p_nx];
     }
     deposit_runs(f, g, pos, d, q, 0, 0, 0, active, a.status);
     if (s < a.n) {
@@ -510,7 +530,8 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LS(P, K, BS, MB) \
-    k_push64<P, K, BS, MB><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+    do { if (s.prefetch) k_push64<P, K, BS, MB, true><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a); \
+         else k_push64<P, K, BS, MB, false><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a); } while (0)
 #define QP_LP(P, K)                              \
     do { switch (s.push_shape) {                 \
         case 1: QP_LS(P, K, 256, 3); break;      \

@@ -149,8 +149,9 @@ struct State {
     // launch shape of the non-QED pushes: threads per block and the CTAs per
     // SM its register budget targets (push_shapes64 / push_shapes32 below;
     // QP_PUSH_SHAPE and QP_PUSH_SHAPE_MIXED select by index)
+    bool prefetch = true;  // pushes: next chunk's slot and cell (FP64: position) loaded a chunk ahead (QP_PREFETCH)
     int push_shape = 0;
-    int push_shape_mixed = 2;
+    int push_shape_mixed = 3;
     // grid of the non-QED pushes: at most push_waves x (SMs x CTAs per SM)
     // blocks striding over the particles (QP_PUSH_WAVES; 0: one thread per
     // particle)
@@ -237,8 +238,9 @@ inline Planes<T> planes_of(const State& s) {
 // takes chunks of `threads` particles.  FP64: 128 registers per thread run
 // the loop without spills (256 x 2, the default); the smaller budgets trade
 // spills for resident warps and measured 0-25 % slower at 512^3.  Mixed:
-// 80 registers (256 x 3) run without spills; 72 (128 x 7, the default, 28
-// warps per SM, a few spills) measured 5 % faster, 64 (32 warps) slower.
+// 80 registers run without spills; on 128-thread blocks (128 x 6, the
+// default) with the next chunk's slot and cell loaded a chunk ahead this
+// measured fastest; 72 registers (128 x 7) spill under the prefetch.
 struct PushShape {
     int threads, minb;
 };

@@ -37,23 +37,40 @@ __device__ __forceinline__ float wrap_offset(float o, int& shift) {
 // waves striding over block-sized chunks, diagnostics reduced once).  The
 // move runs in the particle's cell frame (offsets in [0, 1)), the current
 // through the warp's segment-slot run reduction (deposit_runs).
-template <int PUSHER, int KIND, int BS, int MINB>
+template <int PUSHER, int KIND, int BS, int MINB, bool PF>
 __global__ void __launch_bounds__(BS, MINB) k_push32(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                    const int32_t* __restrict__ perm, int32_t* __restrict__ newcell,
                                                    int32_t* __restrict__ count, PushArgs32 a) {
     double dq = 0.0, de = 0.0, er = 0.0;
     unsigned long long dc = 0;
     const ChunkRange cr = chunk_range(a.n, a.resident);
+    // software pipeline over the thread's chunks: the slot and cell of the
+    // next chunk's particle are loaded during this chunk, so that the loads
+    // of a particle's state and of its fields issue together at the top
+    int p_nx = 0, c_nx = 0;
+    if (PF) {
+        const int s0 = cr.first * blockDim.x + threadIdx.x;
+        if (cr.first < cr.end && s0 < a.n) {
+            p_nx = perm[s0];
+            c_nx = src.cell[p_nx];
+        }
+    }
     for (int ch = cr.first; ch < cr.end; ch += cr.step) {
         const int s = ch * blockDim.x + threadIdx.x;
-        int nc = -1, p = 0, i0 = 0, j0 = 0, k0 = 0;
+        const int s_nx = (ch + cr.step) * blockDim.x + threadIdx.x;
+        const bool has_nx = PF && ch + cr.step < cr.end && s_nx < a.n;
+        int nc = -1, p = p_nx, i0 = 0, j0 = 0, k0 = 0;
+        int c0 = c_nx;
+        if (!PF && s < a.n) {
+            p = perm[s];
+            c0 = src.cell[p];
+        }
+        if (has_nx) p_nx = perm[s_nx];
         bool nc_owned = true;
         bool live = false, active = false;
         float o[3] = {0.f, 0.f, 0.f}, d[3] = {0.f, 0.f, 0.f};
         float ux = 0.f, uy = 0.f, uz = 0.f, gm = 1.f, q = 0.f;
         if (s < a.n) {
-            p = perm[s];
-            const int c0 = src.cell[p];
             i0 = g.div_nynz.div(c0);
             const int r0 = c0 - i0 * g.nynz;
             j0 = g.div_nz.div(r0);
@@ -77,6 +94,7 @@ __global__ void __launch_bounds__(BS, MINB) k_push32(Fields<float> f, Grid g, PS
                 if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
             }
         }
+        if (has_nx) c_nx = src.cell[p_nx];
         deposit_runs(f, g, o, d, q, i0, j0, k0, active, a.status);
         if (s < a.n) {
             int i1 = i0, j1 = j0, k1 = k0;
@@ -453,7 +471,8 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LS(P, K, BS, MB) \
-    k_push32<P, K, BS, MB><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a)
+    do { if (s.prefetch) k_push32<P, K, BS, MB, true><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a); \
+         else k_push32<P, K, BS, MB, false><<<nb, BS, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, sp.count, a); } while (0)
 #define QP_LP(P, K)                              \
     do { switch (s.push_shape_mixed) {                 \
         case 0: QP_LS(P, K, 256, 3); break;      \
