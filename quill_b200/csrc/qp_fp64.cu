@@ -187,10 +187,19 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
     // block-sized chunks with the grid striding over them, diagnostics
     // reduced once per block (as in the pushes without QED)
     const ChunkRange cr = chunk_range(a.n, a.resident);
+    // the next chunk's slot loaded a chunk ahead, its position once the
+    // slot has arrived (as in k_push64)
+    int p_nx = 0;
+    {
+        const int s0 = cr.first * blockDim.x + threadIdx.x;
+        if (cr.first < cr.end && s0 < a.n) p_nx = perm[s0];
+    }
     for (int ch = cr.first; ch < cr.end; ch += cr.step) {
     const int s = ch * blockDim.x + threadIdx.x;
+    const int s_nx = (ch + cr.step) * blockDim.x + threadIdx.x;
+    const int p = p_nx;
+    if (ch + cr.step < cr.end && s_nx < a.n) p_nx = perm[s_nx];
     if (s < a.n) {
-        const int p = perm[s];
         double pos[3] = {src.x[p], src.y[p], src.z[p]};
         double ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
         const double q = src.q[p];

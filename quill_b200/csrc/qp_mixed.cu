@@ -212,10 +212,18 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
     // block-sized chunks with the grid striding over them, diagnostics
     // reduced once per block (as in the pushes without QED)
     const ChunkRange cr = chunk_range(a.n, a.resident);
+    // the next chunk's slot loaded a chunk ahead (as in k_push32)
+    int p_nx = 0;
+    {
+        const int s0 = cr.first * blockDim.x + threadIdx.x;
+        if (cr.first < cr.end && s0 < a.n) p_nx = perm[s0];
+    }
     for (int ch = cr.first; ch < cr.end; ch += cr.step) {
     const int s = ch * blockDim.x + threadIdx.x;
+    const int s_nx = (ch + cr.step) * blockDim.x + threadIdx.x;
+    const int p = p_nx;
+    if (ch + cr.step < cr.end && s_nx < a.n) p_nx = perm[s_nx];
     if (s < a.n) {
-        const int p = perm[s];
         const int c0 = src.cell[p];
         const int i0 = g.div_nynz.div(c0);
         const int r0 = c0 - i0 * g.nynz;
