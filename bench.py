@@ -46,7 +46,8 @@ def workload_config(case):
     """The `config` of both arms' lines: the workload, nothing that differs
     between them."""
     sp = case.species[0]
-    ppc = sum(x.ppc for x in case.species)
+    # particles per cell: one figure for one species, per species for several
+    ppc = " + ".join(str(x.ppc) for x in case.species)
     return {"workload": f"{case.name}: {case.nx}x{case.ny}x{case.nz} cells, dx=lambda/{round(1 / case.dx_lambda)}, "
                         f"dt={case.dt_over_dx:g}dx, {case.solver.upper()} + {case.pusher}, "
                         f"QED {'on' if case.qed else 'off'}, {ppc} ppc at {sp.n0:g} n_cr, "
