@@ -5,7 +5,7 @@
 
 Workload: the 512^3-cell, 4-ppc configuration (dx = lambda/20, dt = dx/2,
 FDTD solver, Boris pusher, QED off, uniform 0.05 n_cr electron plasma with
-10 keV Maxwellian momenta, linearly polarised a0 = 20 laser pulse): 5.4e8
+10 keV Maxwellian momenta, linearly polarised a0 = 20 laser pulse): 5.25e8
 electrons, 1.34e8 cells.  Synthetic, seeded, generated on the GPU.
 
 A step is one full timestep of main.cpp:2321-2331 (push + deposition +
@@ -18,8 +18,9 @@ host, dump of the fields to the host).  Inputs (tens of GB) are far larger
 than L2, so no flush is needed between steps.
 
 `--impl reference` times the reference's own CPU build (oracle/_ref) on the
-host cores: one process per core, each stepping a 64^3 sub-box of the same
-plasma (the reference's own parallelism is one x-slab per MPI rank).
+host cores, stepping the same box: cut into x-slab regions as the reference
+cuts it for its MPI ranks, one host process per region and core (the
+exchange between the regions is left out: no MPI on the host).
 """
 from __future__ import annotations
 
