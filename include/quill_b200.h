@@ -152,7 +152,11 @@ int qp_restore(qp_handle* h, int slot);
 /* Wait for all work of the handle's stream. */
 int qp_synchronize(qp_handle* h);
 
-/* Run all work of h on the given cudaStream_t (NULL = the handle's own). */
+/* Run all work of h on the given cudaStream_t.  NULL keeps the handle's own
+ * stream, which is created non-blocking: it is not ordered with the legacy
+ * default stream, so a caller that works on the default stream orders the
+ * two itself (qp_synchronize before reusing memory the handle reads or
+ * writes, or hand the handle a stream of its own here). */
 int qp_set_stream(qp_handle* h, void* cuda_stream);
 
 /* Number of this library's kernel launches issued since the handle was
