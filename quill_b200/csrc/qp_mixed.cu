@@ -556,9 +556,9 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
         t0 = target32(s, s.sp_ph, true);
         t1 = t0;
     }
-    // chunked grid: groups of the blocks resident at once (80 registers: 3 per SM)
-    static const int qmb = getenv("QP_QED_MINB") ? atoi(getenv("QP_QED_MINB")) : 2;
-    const int nb = push_blocks(s, sp.n, PushShape{256, qmb == 3 ? 3 : 2}, &a.resident);
+    // chunked grid in groups of two blocks per SM (three, as the 80 registers
+    // would allow, measured the same in the cascade)
+    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, &a.resident);
     Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push32_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
