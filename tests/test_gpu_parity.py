@@ -150,14 +150,17 @@ def test_rebin_front_orders_crowded_cell(crowd):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("waves", ["1", "0"])
-def test_push_chunks_per_block(monkeypatch, precision, waves):
+@pytest.mark.parametrize("prefetch", ["1", "0"])
+def test_push_chunks_per_block(monkeypatch, precision, waves, prefetch):
     """The pushes take block-sized chunks of the traversal, several per block
     when the grid is smaller than the particle count (QP_PUSH_WAVES = 1: one
     resident wave of blocks, here about ten chunks each) and one per block
-    with QP_PUSH_WAVES = 0; the diagnostics summed per thread over its chunks
-    and the particles equal the reference's (FP64 to 1e-12; mixed to its
-    tolerances)."""
+    with QP_PUSH_WAVES = 0, with the next chunk's slot and cell loaded a
+    chunk ahead (QP_PREFETCH = 1, the default) or not; the diagnostics summed
+    per thread over its chunks and the particles equal the reference's (FP64
+    to 1e-12; mixed to its tolerances)."""
     monkeypatch.setenv("QP_PUSH_WAVES", waves)
+    monkeypatch.setenv("QP_PREFETCH", prefetch)
     species = (-1.0,)
     case, fields, parts = small_case("fdtd", "boris", n=(48, 48, 48), ppc=8, species=species)
     assert parts[0]["x"].size > 600000
