@@ -178,7 +178,7 @@ __device__ __forceinline__ void born_lepton64(const Fields<double>& f, const Gri
 // position, species, tag, step) -> (r, acceptance draw).
 // t0: photons (lepton kernel) or electrons (photon kernel); t1: positrons.
 template <int PUSHER, int KIND>
-__global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
+__global__ void __launch_bounds__(256, 2) k_push64_qed(Fields<double> f, Grid g, PStore64 src, PStore64 dst,
                                                     const int32_t* __restrict__ perm,
                                                     int32_t* __restrict__ newcell, PushArgs a, QedArgs qa,
                                                     AppendTarget<PStore64> t0, AppendTarget<PStore64> t1) {
@@ -199,14 +199,21 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
     const int s_nx = (ch + cr.step) * blockDim.x + threadIdx.x;
     const int p = p_nx;
     if (ch + cr.step < cr.end && s_nx < a.n) p_nx = perm[s_nx];
+    // the lepton's own move without emission (the common case) deposits its
+    // current after the branches, through the warp's run sums (deposit_runs:
+    // every lane of the warp takes part); the rare moves after an emission
+    // deposit directly
+    double pos[3] = {0.0, 0.0, 0.0}, dmove[3] = {0.0, 0.0, 0.0};
+    double ux = 0.0, uy = 0.0, uz = 0.0, gm = 1.0, q = 0.0, chi = 0.0;
+    int i0 = 0, j0 = 0, k0 = 0, nc = -1;
+    bool converted = false;  // a photon that became a pair is not an erasure
+    bool deferred = false;   // the move's current and cell wait for deposit_runs
     if (s < a.n) {
-        double pos[3] = {src.x[p], src.y[p], src.z[p]};
-        double ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
-        const double q = src.q[p];
-        double chi = src.chi[p];
-        const int i0 = (int)pos[0], j0 = (int)pos[1], k0 = (int)pos[2];
-        int nc = -1;
-        bool converted = false;  // a photon that became a pair is not an erasure
+        pos[0] = src.x[p]; pos[1] = src.y[p]; pos[2] = src.z[p];
+        ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
+        q = src.q[p];
+        chi = src.chi[p];
+        i0 = (int)pos[0]; j0 = (int)pos[1]; k0 = (int)pos[2];
         if (!kill_layer(g, i0, j0, k0)) {
             double E[3], B[3];
             gather(f, g, i0, j0, k0, pos[0] - i0, pos[1] - j0, pos[2] - k0, E, B);
@@ -244,12 +251,9 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
                 const bool emit = !(r2 >= qed_w(g_prev, r, am, qa.e_s) * g_prev * a.dt);
                 if (!emit) {
                     const double t = a.dt / gm;
-                    double d[3] = {ux * t, uy * t, uz * t};
-                    d[0] = d[0] / a.dx; d[1] = d[1] / a.dy; d[2] = d[2] / a.dz;
-                    jdeposition(f, g, pos, d, q, 0, 0, 0, a.status);
-                    const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
-                    const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
-                    if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
+                    dmove[0] = ux * t; dmove[1] = uy * t; dmove[2] = uz * t;
+                    dmove[0] = dmove[0] / a.dx; dmove[1] = dmove[1] / a.dy; dmove[2] = dmove[2] / a.dz;
+                    deferred = true;
                 } else {
                     // photon born at the lepton's t_n position, then moved
                     // to t_{n+3/2} (advance.cpp:294-306)
@@ -303,6 +307,14 @@ __global__ void __launch_bounds__(256) k_push64_qed(Fields<double> f, Grid g, PS
                 }
             }
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+        }
+    }
+    if (KIND != KIND_PHOTON) deposit_runs(f, g, pos, dmove, q, 0, 0, 0, deferred, a.status);
+    if (s < a.n) {
+        if (deferred) {
+            const int i1 = (int)pos[0], j1 = (int)pos[1], k1 = (int)pos[2];
+            const bool moved = (i1 != i0) || (j1 != j0) || (k1 != k0);
+            if (!moved || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
         newcell[s] = nc;
         const bool erased = nc < 0 && !converted && (int)pos[0] >= a.dlo && (int)pos[0] < a.dhi;

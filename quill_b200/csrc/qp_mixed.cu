@@ -203,7 +203,7 @@ __device__ __forceinline__ void born_lepton32(const Fields<float>& f, const Grid
 }
 
 template <int PUSHER, int KIND>
-__global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
+__global__ void __launch_bounds__(256, 2) k_push32_qed(Fields<float> f, Grid g, PStore32 src, PStore32 dst,
                                                     const int32_t* __restrict__ perm,
                                                     int32_t* __restrict__ newcell, PushArgs32 a, QedArgs qa,
                                                     AppendTarget<PStore32> t0, AppendTarget<PStore32> t1) {
@@ -223,20 +223,29 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
     const int s_nx = (ch + cr.step) * blockDim.x + threadIdx.x;
     const int p = p_nx;
     if (ch + cr.step < cr.end && s_nx < a.n) p_nx = perm[s_nx];
+    // the lepton's own move without emission (the common case) deposits its
+    // current after the branches, through the warp's run sums (deposit_runs:
+    // every lane of the warp takes part); the rare moves after an emission
+    // deposit directly
+    float o[3] = {0.f, 0.f, 0.f}, dmove[3] = {0.f, 0.f, 0.f};
+    float ux = 0.f, uy = 0.f, uz = 0.f, gm = 1.f, q = 0.f, chi = 0.f;
+    int i0 = 0, j0 = 0, k0 = 0, nc = -1, i1 = 0, j1 = 0, k1 = 0;
+    bool converted = false;  // a photon that became a pair is not an erasure
+    bool live = false;
+    bool deferred = false;   // the move's current and cell wait for deposit_runs
     if (s < a.n) {
         const int c0 = src.cell[p];
-        const int i0 = g.div_nynz.div(c0);
+        i0 = g.div_nynz.div(c0);
         const int r0 = c0 - i0 * g.nynz;
-        const int j0 = g.div_nz.div(r0);
-        const int k0 = r0 - j0 * g.nz;
-        float o[3] = {src.ox[p], src.oy[p], src.oz[p]};
-        float ux = src.ux[p], uy = src.uy[p], uz = src.uz[p], gm = src.g[p];
-        const float q = src.q[p];
-        float chi = src.chi[p];
+        j0 = g.div_nz.div(r0);
+        k0 = r0 - j0 * g.nz;
+        o[0] = src.ox[p]; o[1] = src.oy[p]; o[2] = src.oz[p];
+        ux = src.ux[p]; uy = src.uy[p]; uz = src.uz[p]; gm = src.g[p];
+        q = src.q[p];
+        chi = src.chi[p];
         const float e_s = (float)qa.e_s;
-        int nc = -1, i1 = i0, j1 = j0, k1 = k0;
-        bool converted = false;  // a photon that became a pair is not an erasure
-        const bool live = !kill_layer(g, i0, j0, k0);
+        i1 = i0; j1 = j0; k1 = k0;
+        live = !kill_layer(g, i0, j0, k0);
         if (live) {
             float E[3], B[3];
             gather(f, g, i0, j0, k0, o[0], o[1], o[2], E, B);
@@ -281,12 +290,8 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                 const bool emit = room && !(r2 >= (double)(qed_w(g_prev, r, am, e_s) * g_prev * a.dt));
                 if (!emit) {
                     const float tt = a.dt / gm;
-                    const float d[3] = {ux * tt * a.idx, uy * tt * a.idy, uz * tt * a.idz};
-                    jdeposition(f, g, o, d, q, i0, j0, k0, a.status);
-                    int si, sj, sk;
-                    o[0] = wrap_offset(o[0], si); o[1] = wrap_offset(o[1], sj); o[2] = wrap_offset(o[2], sk);
-                    i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
-                    if (!(si | sj | sk) || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
+                    dmove[0] = ux * tt * a.idx; dmove[1] = uy * tt * a.idy; dmove[2] = uz * tt * a.idz;
+                    deferred = true;
                 } else {
                     // photon born at the lepton's t_n position, then moved to
                     // t_{n+3/2} (advance.cpp:294-306)
@@ -344,6 +349,15 @@ __global__ void __launch_bounds__(256) k_push32_qed(Fields<float> f, Grid g, PSt
                 }
             }
             if (!isfinite(gm)) atomicOr(a.status, (unsigned int)ST_NAN);
+        }
+    }
+    if (KIND != KIND_PHOTON) deposit_runs(f, g, o, dmove, q, i0, j0, k0, deferred, a.status);
+    if (s < a.n) {
+        if (deferred) {
+            int si, sj, sk;
+            o[0] = wrap_offset(o[0], si); o[1] = wrap_offset(o[1], sj); o[2] = wrap_offset(o[2], sk);
+            i1 = i0 + si; j1 = j0 + sj; k1 = k0 + sk;
+            if (!(si | sj | sk) || inside(g, i1, j1, k1)) nc = cidx(g, i1, j1, k1);
         }
         newcell[s] = nc;
         const bool erased = nc < 0 && !converted && i1 >= a.dlo && i1 < a.dhi;
