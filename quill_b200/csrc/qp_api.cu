@@ -373,7 +373,8 @@ int qp_create(const qp_params* prm, qp_handle** out) {
         const int i = atoi(v);
         if (i >= 0 && i < n_push_shapes32) s.push_shape_mixed = i;
     }
-    if (const char* w = getenv("QP_PUSH_WAVES")) s.push_waves = atoi(w) > 0 ? atoi(w) : 0;
+    if (const char* w = getenv("QP_PUSH_WAVES"))
+        s.push_waves = s.push_waves_mixed = s.push_waves_qed = atoi(w) > 0 ? atoi(w) : 0;
     {
         int sms = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device) == cudaSuccess && sms > 0)

@@ -494,7 +494,7 @@ int launch_push_fp64_qed(State& s, int si, double external_bz) {
         t0 = target64(s, s.sp_ph, true);
         t1 = t0;
     }
-    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
+    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, s.push_waves_qed, &a.resident);  // chunked grid (2 resident blocks per SM assumed)
     Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push64_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
@@ -547,7 +547,7 @@ void launch_push_fp64(State& s, int si, double external_bz) {
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     const PushShape sh = push_shapes64[s.push_shape];
-    const int nb = push_blocks(s, sp.n, sh, &a.resident);
+    const int nb = push_blocks(s, sp.n, sh, s.push_waves, &a.resident);
     Fields<double> f = fields_of<double>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LS(P, K, BS, MB) \

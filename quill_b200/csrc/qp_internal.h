@@ -152,10 +152,11 @@ struct State {
     bool prefetch = true;  // pushes: next chunk's slot and cell (FP64: position) loaded a chunk ahead (QP_PREFETCH)
     int push_shape = 0;
     int push_shape_mixed = 3;
-    // grid of the non-QED pushes: at most push_waves x (SMs x CTAs per SM)
-    // blocks striding over the particles (QP_PUSH_WAVES; 0: one thread per
-    // particle)
-    int push_waves = 128;
+    // grid of the pushes: at most push_waves x (SMs x CTAs per SM) blocks
+    // striding over the particles; per push (FP64 256 groups measured 1 %
+    // faster than 128, mixed 128 1 % faster than 256); QP_PUSH_WAVES sets
+    // all three (0: one thread per particle)
+    int push_waves = 256, push_waves_mixed = 128, push_waves_qed = 128;
     int sm_count = 148;
     std::string err;
     // optional per-phase CUDA-event timing of qp_step (push, rebin, fields,
@@ -230,10 +231,10 @@ inline Planes<T> planes_of(const State& s) {
     return q;
 }
 
-// Blocks of 256 threads for a push over n particles in block-sized chunks
-// (chunk_range): up to push_waves groups of `resident` blocks (the blocks
-// resident at once: SMs x CTAs per SM); one chunk per block if push_waves is
-// 0 or the chunks are fewer than the resident blocks.
+// Blocks for a push over n particles in block-sized chunks (chunk_range): up
+// to `waves` groups of `resident` blocks (the blocks resident at once: SMs x
+// CTAs per SM); one chunk per block if waves is 0 or the chunks are fewer
+// than the resident blocks.
 // Launch shapes of the pushes: {threads per block, CTAs per SM}; a block
 // takes chunks of `threads` particles.  FP64: 128 registers per thread run
 // the loop without spills (256 x 2, the default); the smaller budgets trade
@@ -248,15 +249,15 @@ constexpr PushShape push_shapes64[] = {{256, 2}, {256, 3}, {192, 3}, {128, 5}, {
 constexpr PushShape push_shapes32[] = {{256, 3}, {256, 4}, {128, 7}, {128, 6}, {128, 8}, {64, 14}};
 constexpr int n_push_shapes64 = 6, n_push_shapes32 = 6;
 
-inline int push_blocks(const State& s, int64_t n, PushShape sh, int* resident) {
+inline int push_blocks(const State& s, int64_t n, PushShape sh, int waves, int* resident) {
     const int64_t nch = (n + sh.threads - 1) / sh.threads;
     const int minb = sh.minb;
     const int64_t r = (int64_t)s.sm_count * minb;
-    if (s.push_waves <= 0 || nch <= r) {
+    if (waves <= 0 || nch <= r) {
         *resident = (int)(nch > 0 ? nch : 1);
         return (int)nch;
     }
-    const int64_t w = std::min<int64_t>(s.push_waves, (nch + r - 1) / r);
+    const int64_t w = std::min<int64_t>(waves, (nch + r - 1) / r);
     *resident = (int)r;
     return (int)(r * w);
 }

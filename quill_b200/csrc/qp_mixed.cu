@@ -489,7 +489,7 @@ void launch_push_mixed(State& s, int si, double external_bz) {
     a.trn_dst = sp.trn[1 - sp.cur];
     a.dlo = s.diag_lo; a.dhi = s.diag_hi;
     const PushShape sh = push_shapes32[s.push_shape_mixed];
-    const int nb = push_blocks(s, sp.n, sh, &a.resident);
+    const int nb = push_blocks(s, sp.n, sh, s.push_waves_mixed, &a.resident);
     Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LS(P, K, BS, MB) \
@@ -572,7 +572,7 @@ int launch_push_mixed_qed(State& s, int si, double external_bz) {
     }
     // chunked grid in groups of two blocks per SM (three, as the 80 registers
     // would allow, measured the same in the cascade)
-    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, &a.resident);
+    const int nb = push_blocks(s, sp.n, PushShape{256, 2}, s.push_waves_qed, &a.resident);
     Fields<float> f = fields_of<float>(s);
     const bool vay = s.prm.pusher == QP_PUSHER_VAY;
 #define QP_LQ(P, K) k_push32_qed<P, K><<<nb, 256, 0, s.stream>>>(f, s.grid, src, dst, sp.perm, sp.newcell, a, qa, t0, t1)
